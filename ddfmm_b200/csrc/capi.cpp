@@ -1,0 +1,193 @@
+// extern "C" entry points (include/ddfmm.h).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <new>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/ddfmm.h"
+#include "session.hpp"
+
+struct ddfmm_session {
+    ddfmm::Session* impl;
+};
+
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return DDFMM_OK;
+    } catch (const std::bad_alloc&) {
+        return fail(DDFMM_ENOMEM, "host out of memory");
+    } catch (const std::runtime_error& e) {
+        std::string m = e.what();
+        if (m.rfind("CUDA error", 0) == 0) {
+            if (m.find("out of memory") != std::string::npos) return fail(DDFMM_ENOMEM, m);
+            return fail(DDFMM_ECUDA, m);
+        }
+        return fail(DDFMM_ESETUP, m);
+    } catch (const std::exception& e) {
+        return fail(DDFMM_ESETUP, e.what());
+    }
+}
+}  // namespace
+
+extern "C" {
+
+const char* ddfmm_last_error(void) { return g_err.c_str(); }
+
+int ddfmm_session_create(const double* pos3n, int n, int kernel, int accu, int npq, double K, const double* ctr3,
+                         int ptsmax, int maxlevel, int ncell, const char* ld_path, const char* hd_path, int device,
+                         ddfmm_session** out) {
+    if (!out) return fail(DDFMM_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!pos3n || n <= 0) return fail(DDFMM_EINVAL, "need n > 0 points");
+    if (kernel != DDFMM_KERNEL_HELM && kernel != DDFMM_KERNEL_EXPR) return fail(DDFMM_EINVAL, "unknown kernel type");
+    if (accu < 1 || accu > 3) return fail(DDFMM_EINVAL, "ACCU must be 1, 2 or 3");
+    if (npq <= 0 || npq % 2) return fail(DDFMM_EINVAL, "NPQ must be a positive even number");
+    if (!(K >= 1) || !std::isfinite(K)) return fail(DDFMM_EINVAL, "K must be >= 1");
+    if (ncell < 1 || (ncell & (ncell - 1)) || K / ncell < 1 - 1e-12)
+        return fail(DDFMM_EINVAL, "ncell must be a power of two with K/ncell >= 1");
+    if (ptsmax < 1 || maxlevel < 1) return fail(DDFMM_EINVAL, "ptsmax and maxlevel must be positive");
+    if (!ld_path || !hd_path) return fail(DDFMM_EINVAL, "operator file paths are required");
+    for (long long i = 0; i < 3LL * n; ++i)
+        if (!std::isfinite(pos3n[i])) return fail(DDFMM_EINVAL, "non-finite point coordinate");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(DDFMM_ECUDA, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return fail(DDFMM_EINVAL, "device ordinal out of range");
+    ddfmm::SessionParams p;
+    p.tree.K = K;
+    p.tree.ctr = {{ctr3 ? ctr3[0] : 0.0, ctr3 ? ctr3[1] : 0.0, ctr3 ? ctr3[2] : 0.0}};
+    p.tree.ptsmax = ptsmax;
+    p.tree.maxlevel = maxlevel;
+    p.tree.npq = npq;
+    p.tree.ncell = ncell;
+    p.accu = accu;
+    p.kernel = kernel;
+    p.device = device;
+    ddfmm::Session* impl = nullptr;
+    int rc = guarded([&] { impl = new ddfmm::Session(pos3n, n, p, ld_path, hd_path); });
+    if (rc != DDFMM_OK) return rc;
+    *out = new ddfmm_session{impl};
+    return DDFMM_OK;
+}
+
+int ddfmm_eval(ddfmm_session* s, const double* den, double* val) {
+    if (!s || !s->impl) return fail(DDFMM_EINVAL, "NULL session");
+    if (!den || !val) return fail(DDFMM_EINVAL, "NULL density or value array");
+    return guarded([&] {
+        s->impl->eval_host(reinterpret_cast<const std::complex<double>*>(den),
+                           reinterpret_cast<std::complex<double>*>(val));
+    });
+}
+
+int ddfmm_eval_device(ddfmm_session* s, const void* den_dev, void* val_dev, void* stream) {
+    if (!s || !s->impl) return fail(DDFMM_EINVAL, "NULL session");
+    if (!den_dev || !val_dev) return fail(DDFMM_EINVAL, "NULL device array");
+    return guarded([&] {
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->impl->stream();
+        s->impl->eval_device(static_cast<const double2*>(den_dev), static_cast<double2*>(val_dev), st);
+    });
+}
+
+int ddfmm_direct(ddfmm_session* s, const double* den, const int* ids, int nids, double* out) {
+    if (!s || !s->impl) return fail(DDFMM_EINVAL, "NULL session");
+    if (!den || (nids > 0 && (!ids || !out)) || nids < 0) return fail(DDFMM_EINVAL, "bad direct-sum arguments");
+    return guarded([&] {
+        s->impl->direct_host(reinterpret_cast<const std::complex<double>*>(den), ids, nids,
+                             reinterpret_cast<std::complex<double>*>(out));
+    });
+}
+
+int ddfmm_session_stats(const ddfmm_session* s, ddfmm_stats* out) {
+    if (!s || !s->impl || !out) return fail(DDFMM_EINVAL, "NULL argument");
+    const ddfmm::SessionStats& t = s->impl->stats();
+    out->n_points = t.n_points;
+    out->n_boxes = t.n_boxes;
+    out->n_leaves = t.n_leaves;
+    out->n_lf_boxes = t.n_lf_boxes;
+    out->u_pairs = t.u_pairs;
+    out->u_interactions = t.u_interactions;
+    out->v_pairs = t.v_pairs;
+    out->w_pairs = t.w_pairs;
+    out->x_pairs = t.x_pairs;
+    out->hf_up_nodes = t.hf_up_nodes;
+    out->hf_down_nodes = t.hf_down_nodes;
+    out->hf_far_pairs = t.hf_far_pairs;
+    out->m2l_matrices = t.m2l_matrices;
+    out->gemm_launches = t.gemm_launches;
+    out->kernel_launches = t.kernel_launches;
+    out->flops_gemm = t.flops_gemm;
+    out->fft_spectra_bytes = t.fft_spectra_bytes;
+    out->setup_seconds = t.setup_seconds;
+    out->device_bytes = (long long)t.device_bytes;
+    return DDFMM_OK;
+}
+
+int ddfmm_tree_stats(const double* pos3n, int n, double K, const double* ctr3, int ptsmax, int maxlevel, int ncell,
+                     int npq, int* total_boxes, int* empty_boxes, int* nlevels, ddfmm_tree_level* levels) {
+    if (!pos3n || n <= 0 || !total_boxes || !empty_boxes || !nlevels || !levels)
+        return fail(DDFMM_EINVAL, "bad tree-stats arguments");
+    if (ncell < 1 || (ncell & (ncell - 1)) || K / ncell < 1 - 1e-12)
+        return fail(DDFMM_EINVAL, "ncell must be a power of two with K/ncell >= 1");
+    return guarded([&] {
+        ddfmm::TreeParams p;
+        p.K = K;
+        p.ctr = {{ctr3 ? ctr3[0] : 0.0, ctr3 ? ctr3[1] : 0.0, ctr3 ? ctr3[2] : 0.0}};
+        p.ptsmax = ptsmax;
+        p.maxlevel = maxlevel;
+        p.ncell = ncell;
+        p.npq = npq;
+        ddfmm::Tree t;
+        t.build(pos3n, n, p);
+        std::map<int, ddfmm_tree_level> lv;
+        int empty = 0;
+        for (const ddfmm::Box& b : t.boxes) {
+            if (!b.has_pts()) {
+                ++empty;
+                continue;
+            }
+            ddfmm_tree_level& L = lv[b.level];
+            L.level = b.level;
+            L.width = t.width(b.level);
+            L.boxes++;
+            if (b.terminal()) L.leaves++;
+            for (auto& kv : b.far) L.far_pairs += (long long)kv.second.size();
+            L.out_dirs += (long long)b.outdirs.size();
+            L.inc_dirs += (long long)b.incdirs.size();
+            L.u_pairs += (long long)b.ulist.size();
+            L.v_pairs += (long long)b.vlist.size();
+            L.w_pairs += (long long)b.wlist.size();
+            L.x_pairs += (long long)b.xlist.size();
+        }
+        if (lv.size() > 64) throw std::runtime_error("more than 64 levels");
+        int i = 0;
+        for (auto& kv : lv) levels[i++] = kv.second;
+        *nlevels = i;
+        *total_boxes = (int)t.boxes.size();
+        *empty_boxes = empty;
+    });
+}
+
+int ddfmm_session_destroy(ddfmm_session* s) {
+    if (!s) return DDFMM_OK;
+    int rc = guarded([&] { delete s->impl; });
+    delete s;
+    return rc;
+}
+
+}  // extern "C"

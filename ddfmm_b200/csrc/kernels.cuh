@@ -1,0 +1,86 @@
+// Device kernels of the directional FMM eval and their launch descriptors.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace ddfmm {
+
+enum KernelType { KERNEL_HELM = 0, KERNEL_EXPR = 1 };  // include/kernel3d.hpp:24-27
+enum GemmMode { GEMM_SET = 0, GEMM_ADD = 1, GEMM_ATOMIC = 2 };
+
+// One shared operator A (m x k, column-major, leading dimension lda) applied
+// to ncol gathered columns: y[yoff[c]..] (op)= A * x[xoff[c]..].
+struct GemmProblem {
+    const double2* A;
+    int m, k, lda;
+    int col0;  // first entry in the column arrays
+    int ncol;
+};
+// A launch is a list of 64 x 32 output tiles.
+struct GemmTile {
+    int prob;
+    int row0;
+    int col0;  // relative to the problem's first column
+    int pad;
+};
+
+// Kernel-matrix generation job: out(i,j) = G(trg_i + ts, src_j + ss),
+// trg/src are 3 x n point arrays (coordinate fastest), out column-major.
+struct KmatJob {
+    const double* trg;
+    const double* src;
+    double2* out;
+    double ts[3];
+    double ss[3];
+    int m, k;
+    long long elem0;  // prefix offset of this job's elements in the launch
+};
+
+// A set of points: p_k = scale * x[3k..3k+2] + shift.
+struct PtSet {
+    const double* x;
+    double shift[3];
+    double scale;
+    int n;
+};
+// Point-interaction work item: out[t] += sum_s G(trg_t, src_s) den[s] over
+// the source segments src_begin..src_end of the item.
+struct PtItem {
+    PtSet trg;
+    double2* out;
+    int src_begin, src_end;
+};
+struct PtSrc {
+    PtSet src;
+    const double2* den;
+};
+
+void launch_kmat(const KmatJob* jobs_dev, int njobs, long long total, int kernel, cudaStream_t s);
+void launch_gemm(const GemmProblem* probs_dev, const GemmTile* tiles_dev, int ntiles,
+                 const long long* xoff, const long long* yoff, const double2* X, double2* Y, int mode,
+                 cudaStream_t s);
+void launch_pt(const PtItem* items_dev, int nitems, const PtSrc* srcs_dev, int kernel, cudaStream_t s);
+
+// FFT-based low-frequency M2L on a G^3 grid (G = 2P), see kernels.cu.
+struct VlistLevel {
+    int G, P;
+    int nE;                 // equivalent / check points per box
+    const int* grid_idx;    // nE grid indices of the uep (== dcp) nodes
+    const double2* tns;     // 343 x G^3 FFT'd translation tensors (zero when near)
+    const double2* twf;     // G forward twiddles exp(-2 pi i m / G)
+    const double2* twb;     // G backward twiddles exp(+2 pi i m / G)
+};
+void vlist_init(int G);
+void launch_vlist_forward(const VlistLevel& L, const int* boxes, int nbox, const double2* upeq,
+                          double2* spec, cudaStream_t s);
+void launch_vlist_accum(const VlistLevel& L, const int* trg, int ntrg, const int* vptr,
+                        const int* vsrc, const int* voff, const double2* spec, double2* dnchk,
+                        cudaStream_t s);
+
+// gather/scatter helpers
+void launch_gather_den(const double2* den, const int* perm, double2* out, int n, cudaStream_t s);
+void launch_scatter_val(const double2* in, const int* perm, double2* val, int n, cudaStream_t s);
+void launch_direct(const double* pos, const double2* den, int n, const int* chk, int nchk,
+                   double2* out, int kernel, cudaStream_t s);
+
+}  // namespace ddfmm

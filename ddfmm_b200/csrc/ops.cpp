@@ -1,0 +1,149 @@
+// Reader for the reference's operator files (see ops.hpp).
+#include "ops.hpp"
+
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <stdexcept>
+
+namespace ddfmm {
+
+namespace {
+struct In {
+    std::vector<char> buf;
+    size_t o = 0;
+    std::string name;
+    void need(size_t n) {
+        if (o + n > buf.size())
+            throw std::runtime_error("operator file " + name + " is truncated");
+    }
+    int i32() {
+        need(4);
+        int v;
+        std::memcpy(&v, &buf[o], 4);
+        o += 4;
+        return v;
+    }
+    double f64() {
+        need(8);
+        double v;
+        std::memcpy(&v, &buf[o], 8);
+        o += 8;
+        return v;
+    }
+    int dim() {
+        int v = i32();
+        if (v < 0 || v > (1 << 26)) throw std::runtime_error("operator file " + name + ": bad dimension");
+        return v;
+    }
+    void dbl(double* dst, size_t n) {
+        need(8 * n);
+        std::memcpy(dst, &buf[o], 8 * n);
+        o += 8 * n;
+    }
+    PMat pmat() {
+        int m = dim(), n = dim();
+        if (m != 3 && !(m == 0 && n == 0)) throw std::runtime_error("operator file " + name + ": points are not 3 x n");
+        PMat p;
+        p.n = n;
+        p.x.resize((size_t)3 * n);
+        dbl(p.x.data(), p.x.size());
+        return p;
+    }
+    CMat cmat() {
+        CMat c;
+        c.m = dim();
+        c.n = dim();
+        c.a.resize((size_t)c.m * c.n);
+        dbl(reinterpret_cast<double*>(c.a.data()), 2 * c.a.size());
+        return c;
+    }
+    std::vector<cpx> ctns(int& edge) {
+        int m = dim(), n = dim(), p = dim();
+        std::vector<cpx> t((size_t)m * n * p);
+        dbl(reinterpret_cast<double*>(t.data()), 2 * t.size());
+        if (!t.empty()) {
+            if (m != n || n != p) throw std::runtime_error("operator file " + name + ": ue2dc tensor not cubic");
+            edge = m;
+        }
+        return t;
+    }
+};
+
+In slurp(const std::string& path) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) throw std::runtime_error("cannot open operator file " + path);
+    In in;
+    in.name = path;
+    in.buf.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+    return in;
+}
+}  // namespace
+
+void OperatorLib::load(const std::string& ld_path, const std::string& hd_path) {
+    ld.clear();
+    hd.clear();
+    In a = slurp(ld_path);
+    int nw = a.dim();
+    for (int w = 0; w < nw; ++w) {
+        LowFreqOp op;
+        op.W = a.f64();
+        op.uep = a.pmat();
+        op.ucp = a.pmat();
+        int nv = a.dim();
+        if (nv != 3) throw std::runtime_error("ld file: uc2ue must hold 3 matrices");
+        op.v = a.cmat();
+        op.is = a.cmat();
+        op.up = a.cmat();
+        int t0 = a.dim(), t1 = a.dim(), t2 = a.dim();
+        if (t0 != 7 || t1 != 7 || t2 != 7) throw std::runtime_error("ld file: ue2dc must be 7x7x7");
+        op.ue2dc.resize(343);
+        for (int i = 0; i < 343; ++i) op.ue2dc[i] = a.ctns(op.tdim);
+        ld[op.W] = std::move(op);
+    }
+    if (a.o != a.buf.size()) throw std::runtime_error("ld file has trailing bytes");
+    In b = slurp(hd_path);
+    nw = b.dim();
+    for (int w = 0; w < nw; ++w) {
+        double W = b.f64();
+        int nd = b.dim();
+        auto& lvl = hd[W];
+        for (int k = 0; k < nd; ++k) {
+            Idx3 key{{b.i32(), b.i32(), b.i32()}};
+            HighFreqOp op;
+            op.uep = b.pmat();
+            op.ucp = b.pmat();
+            int nv = b.dim();
+            if (nv != 3) throw std::runtime_error("hd file: uc2ue must hold 3 matrices");
+            op.E1 = b.cmat();
+            op.E2 = b.cmat();
+            op.E3 = b.cmat();
+            lvl[key] = std::move(op);
+        }
+    }
+    if (b.o != b.buf.size()) throw std::runtime_error("hd file has trailing bytes");
+}
+
+const LowFreqOp& OperatorLib::low(double W) const {
+    auto it = ld.find(W);
+    if (it == ld.end()) {
+        std::ostringstream s;
+        s << "no low-frequency operators for width " << W;
+        throw std::runtime_error(s.str());
+    }
+    return it->second;
+}
+
+const HighFreqOp& OperatorLib::high(double W, const Idx3& canon) const {
+    auto it = hd.find(W);
+    if (it != hd.end()) {
+        auto jt = it->second.find(canon);
+        if (jt != it->second.end()) return jt->second;
+    }
+    std::ostringstream s;
+    s << "no high-frequency operators for width " << W << " wedge (" << canon[0] << "," << canon[1] << ","
+      << canon[2] << ")";
+    throw std::runtime_error(s.str());
+}
+
+}  // namespace ddfmm

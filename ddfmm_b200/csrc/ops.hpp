@@ -1,0 +1,55 @@
+// Translation operators read from the reference's ld/hd operator files.
+//
+// File layouts (Mlib3d::setup, src/mlib3d.cpp:70-103; element formats
+// include/serialize.hpp):
+//   ld: map<double W, {DblNumMat uep, DblNumMat ucp, NumVec<CpxNumMat> uc2ue,
+//                      NumTns<CpxNumTns> ue2dc (7x7x7)}>   (mlib3d.cpp:361-379)
+//   hd: map<double W, map<Index3 wedge, {DblNumMat uep, DblNumMat ucp,
+//                      NumVec<CpxNumMat> uc2ue}>>          (mlib3d.cpp:382-405)
+// Matrices are column-major; points are 3 x n (coordinate fastest).
+#pragma once
+#include <complex>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "tree.hpp"
+
+namespace ddfmm {
+
+typedef std::complex<double> cpx;
+
+struct CMat {
+    int m = 0, n = 0;
+    std::vector<cpx> a;  // column-major
+    cpx& operator()(int i, int j) { return a[(size_t)j * m + i]; }
+    const cpx& operator()(int i, int j) const { return a[(size_t)j * m + i]; }
+};
+
+struct PMat {  // 3 x n points
+    int n = 0;
+    std::vector<double> x;  // x[3*k + d]
+};
+
+struct LowFreqOp {
+    double W = 0;
+    PMat uep, ucp;
+    CMat v, is, up;                   // uc2ue = {v, 1/sigma, U^H}
+    std::vector<std::vector<cpx> > ue2dc;  // 343 tensors (2P)^3, empty when near
+    int tdim = 0;                     // 2P
+};
+
+struct HighFreqOp {
+    PMat uep, ucp;   // skeleton source (r1) / target (r2) points
+    CMat E1, E2, E3; // uc2ue = {E1, E2, E3}
+};
+
+struct OperatorLib {
+    std::map<double, LowFreqOp> ld;
+    std::map<double, std::map<Idx3, HighFreqOp> > hd;
+    void load(const std::string& ld_path, const std::string& hd_path);
+    const LowFreqOp& low(double W) const;
+    const HighFreqOp& high(double W, const Idx3& canon) const;
+};
+
+}  // namespace ddfmm

@@ -1,0 +1,985 @@
+// Plan flattening and the eval launch sequence (see session.hpp).
+//
+// Pass structure and data flow follow Wave3d::eval (src/wave3d_eval.cpp:299-415):
+//   1. low-frequency upward, widths ascending        (EvalUpwardLow :418-490)
+//   2. high-frequency upward, widths ascending       (EvalUpwardHigh :773-854)
+//   3. high-frequency downward, widths descending    (EvalDownwardHigh :996-1040,
+//      HighFrequencyM2L :876-928, HighFrequencyL2L :931-993)
+//   4. low-frequency downward, widths descending     (EvalDownwardLow :493-583 with
+//      U/V/W/X lists :585-718)
+// The reference walks directions recursively (pre-order up, post-order down,
+// :721-751); every (box, wedge) only depends on its children (up) or its
+// parent (down), so processing whole widths at a time gives the same sums.
+// Operators are the reference's: Mlib3d::*Fetch (src/mlib3d.cpp:106-280).
+#include "session.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <unordered_map>
+
+namespace ddfmm {
+
+#define CK(x)                                                                                      \
+    do {                                                                                           \
+        cudaError_t e_ = (x);                                                                      \
+        if (e_ != cudaSuccess)                                                                     \
+            throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e_) + " (" + \
+                                     #x + ")");                                                    \
+    } while (0)
+
+static int accu_to_p(int accu) {
+    if (accu < 1 || accu > 3) throw std::runtime_error("ACCU must be 1, 2 or 3");  // src/wave3d.cpp:149
+    return accu == 1 ? 4 : (accu == 2 ? 6 : 8);
+}
+
+template <class T>
+T* Session::dalloc(size_t count) {
+    if (count == 0) count = 1;
+    void* p = nullptr;
+    CK(cudaMalloc(&p, count * sizeof(T)));
+    allocs_.push_back(p);
+    stats_.device_bytes += count * sizeof(T);
+    return static_cast<T*>(p);
+}
+
+template <class T>
+T* Session::upload(const std::vector<T>& v) {
+    T* d = dalloc<T>(v.size());
+    if (!v.empty()) CK(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream_));
+    // the host vector may die right after: make the copy complete
+    CK(cudaStreamSynchronize(stream_));
+    return d;
+}
+
+Session::Session(const double* pos3n, int n, const SessionParams& p, const std::string& ld_path,
+                 const std::string& hd_path)
+    : prm_(p), npts_(n) {
+    if (n <= 0) throw std::runtime_error("no points");
+    auto t0 = std::chrono::steady_clock::now();
+    CK(cudaSetDevice(p.device));
+    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    pos_.assign(pos3n, pos3n + 3 * (size_t)n);
+    ops_.load(ld_path, hd_path);
+    tree_.build(pos_.data(), n, p.tree);
+    build();
+    CK(cudaStreamSynchronize(stream_));
+    stats_.setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+Session::~Session() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (void* p : allocs_) cudaFree(p);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<long long> >& xo,
+                       std::vector<std::vector<long long> >& yo, const double2* X, double2* Y, int mode) {
+    std::vector<GemmProblem> P;
+    std::vector<GemmTile> tiles;
+    std::vector<long long> xs, ys;
+    for (size_t i = 0; i < probs.size(); ++i) {
+        if (xo[i].empty() || probs[i].m == 0 || probs[i].k == 0) continue;
+        GemmProblem q = probs[i];
+        q.col0 = (int)xs.size();
+        q.ncol = (int)xo[i].size();
+        int pid = (int)P.size();
+        P.push_back(q);
+        xs.insert(xs.end(), xo[i].begin(), xo[i].end());
+        ys.insert(ys.end(), yo[i].begin(), yo[i].end());
+        for (int r0 = 0; r0 < q.m; r0 += 64)
+            for (int c0 = 0; c0 < q.ncol; c0 += 32) tiles.push_back(GemmTile{pid, r0, c0, 0});
+        stats_.flops_gemm += 8.0 * q.m * q.k * (double)q.ncol;
+    }
+    if (tiles.empty()) return;
+    Step st{};
+    st.kind = 0;
+    st.g.probs = upload(P);
+    st.g.tiles = upload(tiles);
+    st.g.xoff = upload(xs);
+    st.g.yoff = upload(ys);
+    st.g.ntiles = (int)tiles.size();
+    st.g.X = X;
+    st.g.Y = Y;
+    st.g.mode = mode;
+    steps_.push_back(st);
+    stats_.gemm_launches++;
+}
+
+void Session::add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>& srcs) {
+    if (items.empty()) return;
+    Step st{};
+    st.kind = 1;
+    st.pt.items = upload(items);
+    st.pt.srcs = upload(srcs);
+    st.pt.nitems = (int)items.size();
+    steps_.push_back(st);
+}
+
+namespace {
+struct NodeKey {
+    uint64_t operator()(int box, const Idx3& d) const {
+        return ((uint64_t)box << 33) | ((uint64_t)(d[0] + 1024) << 22) | ((uint64_t)(d[1] + 1024) << 11) |
+               (uint64_t)(d[2] + 1024);
+    }
+};
+Pt3 shifted_point(int ind, double W) {  // ShiftedPoint, src/mlib3d.cpp:21-30
+    int a = (ind & 4) >> 2, b = (ind & 2) >> 1, c = ind & 1;
+    return Pt3{{(a - 0.5) * W / 2, (b - 0.5) * W / 2, (c - 0.5) * W / 2}};
+}
+// HighFetchShuffle, src/mlib3d.cpp:308-325: res(prm(d)) = tmp(d), then res(d) *= sgn(d)
+std::vector<double> shuffle(const PMat& p, const Idx3& prm, const Idx3& sgn, double extra_sign) {
+    std::vector<double> r((size_t)3 * p.n);
+    for (int k = 0; k < p.n; ++k) {
+        double t[3];
+        for (int d = 0; d < 3; ++d) t[prm[d]] = p.x[3 * k + d];
+        for (int d = 0; d < 3; ++d) r[3 * k + d] = extra_sign * (sgn[d] * t[d]);
+    }
+    return r;
+}
+std::vector<double2> to_d2(const CMat& m) {
+    std::vector<double2> r(m.a.size());
+    for (size_t i = 0; i < m.a.size(); ++i) r[i] = make_double2(m.a[i].real(), m.a[i].imag());
+    return r;
+}
+std::vector<double2> to_d2_transpose(const CMat& m) {  // Transpose, src/mlib3d.cpp:32-42
+    std::vector<double2> r(m.a.size());
+    for (int i = 0; i < m.m; ++i)
+        for (int j = 0; j < m.n; ++j) r[(size_t)i * m.n + j] = make_double2(m(i, j).real(), m(i, j).imag());
+    return r;
+}
+}  // namespace
+
+void Session::build() {
+    const double eps = 1e-12;
+    const int P = accu_to_p(prm_.accu), G = 2 * P, G3 = G * G * G;
+    const int nE = P * P * P - (P - 2) * (P - 2) * (P - 2);
+    const int kern = prm_.kernel;
+    if (kern != KERNEL_HELM && kern != KERNEL_EXPR) throw std::runtime_error("unknown kernel type");
+    Tree& T = tree_;
+    const int nb = (int)T.boxes.size();
+    stats_.n_points = npts_;
+    stats_.n_boxes = nb;
+
+    // ---------------------------------------------------------------- LF boxes, leaves, points
+    std::vector<int> lfbox, lfidx(nb, -1);
+    for (int b : T.order)
+        if (T.boxes[b].has_pts() && T.width(T.boxes[b].level) < 1 - eps) {
+            lfidx[b] = (int)lfbox.size();
+            lfbox.push_back(b);
+        }
+    const int nLF = (int)lfbox.size();
+    stats_.n_lf_boxes = nLF;
+    std::vector<int> perm, leaf_off(nLF, -1), leaf_cnt(nLF, 0);
+    std::vector<double> pos_sorted;
+    perm.reserve(npts_);
+    pos_sorted.reserve(3 * (size_t)npts_);
+    for (int l = 0; l < nLF; ++l) {
+        const Box& B = T.boxes[lfbox[l]];
+        if (!B.terminal()) continue;
+        leaf_off[l] = (int)perm.size();
+        leaf_cnt[l] = (int)B.pts.size();
+        for (int id : B.pts) {
+            perm.push_back(id);
+            for (int d = 0; d < 3; ++d) pos_sorted.push_back(pos_[3 * (size_t)id + d]);
+        }
+        stats_.n_leaves++;
+    }
+    if ((int)perm.size() != npts_) throw std::runtime_error("tree leaves do not hold every point exactly once");
+    d_perm_ = upload(perm);
+    d_pos_ids_ = upload(pos_);
+    d_pos_sorted_ = upload(pos_sorted);
+    d_den_sorted_ = dalloc<double2>(npts_);
+    d_val_sorted_ = dalloc<double2>(npts_);
+    d_den_io_ = dalloc<double2>(npts_);
+    d_val_io_ = dalloc<double2>(npts_);
+    zero_at_start_.push_back(Memset{d_val_sorted_, sizeof(double2) * npts_});
+
+    std::map<int, std::vector<int> > lflevels;  // level -> lf ids (key order)
+    for (int l = 0; l < nLF; ++l) lflevels[T.boxes[lfbox[l]].level].push_back(l);
+
+    double2* lf_upeq = dalloc<double2>((size_t)nLF * nE);
+    double2* lf_upchk = dalloc<double2>((size_t)nLF * nE);
+    double2* lf_mid = dalloc<double2>((size_t)nLF * nE);
+    double2* lf_dnchk = dalloc<double2>((size_t)nLF * nE);
+    double2* lf_dneq = dalloc<double2>((size_t)nLF * nE);
+    double2* lf_spec = dalloc<double2>((size_t)nLF * G3);
+    stats_.fft_spectra_bytes = (long long)nLF * G3 * 16;
+    zero_at_start_.push_back(Memset{lf_upchk, sizeof(double2) * (size_t)nLF * nE});
+    zero_at_start_.push_back(Memset{lf_dnchk, sizeof(double2) * (size_t)nLF * nE});
+
+    // per-LF-level device operators
+    struct LfLevelOps {
+        double W;
+        const double *uep, *ucp;
+        double2 *up_s, *v, *vT_s, *upT, *tns;
+        int* grid_idx;
+        int r;
+        double2* ue2uc[8];
+        double2* de2dc[8];
+        bool has_children;
+    };
+    std::map<int, LfLevelOps> lfops;
+    std::vector<KmatJob> jobs;  // kernel-matrix generation, run once below
+    long long job_elems = 0;
+    auto add_job = [&](const double* trg, Pt3 ts, const double* src, Pt3 ss, int m, int k, double2* out) {
+        KmatJob j;
+        j.trg = trg;
+        j.src = src;
+        j.out = out;
+        for (int d = 0; d < 3; ++d) {
+            j.ts[d] = ts[d];
+            j.ss[d] = ss[d];
+        }
+        j.m = m;
+        j.k = k;
+        j.elem0 = job_elems;
+        job_elems += (long long)m * k;
+        jobs.push_back(j);
+    };
+    const Pt3 zero3{{0, 0, 0}};
+    std::vector<double2> twf(G), twb(G);
+    {
+        const long double twopi = 6.283185307179586476925286766559005768L;
+        for (int m = 0; m < G; ++m) {
+            long double a = twopi * (long double)m / (long double)G;
+            twf[m] = make_double2((double)cosl(a), -(double)sinl(a));
+            twb[m] = make_double2((double)cosl(a), (double)sinl(a));
+        }
+    }
+    double2* d_twf = upload(twf);
+    double2* d_twb = upload(twb);
+    vlist_init(G);
+
+    for (auto& kv : lflevels) {
+        int level = kv.first;
+        double W = T.width(level);
+        const LowFreqOp& op = ops_.low(W);
+        if (op.uep.n != nE || op.ucp.n != nE)
+            throw std::runtime_error("low-frequency operator size does not match ACCU");
+        LfLevelOps L{};
+        L.W = W;
+        L.r = op.up.m;
+        L.uep = upload(op.uep.x);
+        L.ucp = upload(op.ucp.x);
+        // fold the 1/sigma scaling into the rows of U^H (up) and of v^T
+        std::vector<double2> up_s((size_t)L.r * nE), vT_s((size_t)L.r * nE);
+        for (int i = 0; i < L.r; ++i)
+            for (int j = 0; j < nE; ++j) {
+                cpx s = op.is(i, 0);
+                cpx a = s * op.up(i, j), b = s * op.v(j, i);
+                up_s[(size_t)j * L.r + i] = make_double2(a.real(), a.imag());
+                vT_s[(size_t)j * L.r + i] = make_double2(b.real(), b.imag());
+            }
+        L.up_s = upload(up_s);
+        L.vT_s = upload(vT_s);
+        L.v = upload(to_d2(op.v));
+        L.upT = upload(to_d2_transpose(op.up));
+        // V-list tensors and grid positions of the uep / dcp nodes (src/wave3d_eval.cpp:607-659)
+        if (op.tdim != 0 && op.tdim != G) throw std::runtime_error("ue2dc tensor size does not match ACCU");
+        std::vector<double2> tns((size_t)343 * G3, make_double2(0, 0));
+        for (int o = 0; o < 343; ++o) {
+            const auto& t = op.ue2dc[o];
+            if (t.empty()) continue;
+            for (int e = 0; e < G3; ++e) tns[(size_t)o * G3 + e] = make_double2(t[e].real(), t[e].imag());
+        }
+        L.tns = upload(tns);
+        std::vector<int> gidx(nE);
+        double step = W / (P - 1);
+        for (int k = 0; k < nE; ++k) {
+            int a[3];
+            for (int d = 0; d < 3; ++d) a[d] = (int)std::round((op.uep.x[3 * k + d] + W / 2) / step) + P;
+            for (int d = 0; d < 3; ++d)
+                if (a[d] < 0 || a[d] >= G) throw std::runtime_error("V-list grid index out of range");
+            gidx[k] = a[0] + G * (a[1] + G * a[2]);
+        }
+        L.grid_idx = upload(gidx);
+        L.has_children = false;
+        for (int l : kv.second)
+            if (!T.boxes[lfbox[l]].terminal()) L.has_children = true;
+        if (L.has_children) {
+            const LowFreqOp& ch = ops_.low(W / 2);  // UpwardLowFetch / DownwardLowFetch
+            const double* chuep = upload(ch.uep.x);
+            for (int ind = 0; ind < 8; ++ind) {
+                L.ue2uc[ind] = dalloc<double2>((size_t)nE * nE);
+                L.de2dc[ind] = dalloc<double2>((size_t)nE * nE);
+                add_job(L.ucp, zero3, chuep, shifted_point(ind, W), nE, nE, L.ue2uc[ind]);
+                add_job(chuep, shifted_point(ind, W), L.ucp, zero3, nE, nE, L.de2dc[ind]);
+            }
+        }
+        lfops[level] = L;
+    }
+
+    // ---------------------------------------------------------------- HF nodes
+    struct Node {
+        int box;
+        Idx3 dir;
+        int canon;           // index into hfcanon
+        long long off;       // upeq (up) / dnchk (down) offset
+        long long toff;      // temp offset within the level
+    };
+    struct Canon {
+        double W;
+        Idx3 srt;
+        const HighFreqOp* op;
+        int r1, r2;
+        double2 *E1, *E2, *E3, *E1t, *E2t, *E3t;
+        double *uep, *neg_uep;
+    };
+    std::vector<Canon> hfcanon;
+    std::map<std::pair<double, Idx3>, int> canon_id;
+    auto get_canon = [&](double W, const Idx3& dir, Idx3& sgn, Idx3& prmv) -> int {
+        Idx3 srt;
+        index3_sort(dir, srt, sgn, prmv);
+        auto key = std::make_pair(W, srt);
+        auto it = canon_id.find(key);
+        if (it != canon_id.end()) return it->second;
+        Canon c{};
+        c.W = W;
+        c.srt = srt;
+        c.op = &ops_.high(W, srt);
+        c.r1 = c.op->uep.n;
+        c.r2 = c.op->ucp.n;
+        if (c.op->E1.m != c.r1 || c.op->E1.n != c.r1 || c.op->E2.m != c.r1 || c.op->E2.n != c.r2 ||
+            c.op->E3.m != c.r2 || c.op->E3.n != c.r2)
+            throw std::runtime_error("high-frequency operator shapes are inconsistent");
+        if (c.r1 > 400 || c.r2 > 400)  // DVMAX, src/wave3d_eval.cpp:25,842-844
+            throw std::runtime_error("high-frequency rank exceeds DVMAX=400");
+        c.E1 = upload(to_d2(c.op->E1));
+        c.E2 = upload(to_d2(c.op->E2));
+        c.E3 = upload(to_d2(c.op->E3));
+        c.E1t = upload(to_d2_transpose(c.op->E1));
+        c.E2t = upload(to_d2_transpose(c.op->E2));
+        c.E3t = upload(to_d2_transpose(c.op->E3));
+        c.uep = upload(c.op->uep.x);
+        std::vector<double> neg(c.op->uep.x);
+        for (double& v : neg) v = -v;
+        c.neg_uep = upload(neg);
+        int id = (int)hfcanon.size();
+        hfcanon.push_back(c);
+        canon_id[key] = id;
+        return id;
+    };
+    // per (W, dir) shuffled point sets
+    struct DirPts {
+        double *ucp, *dep, *uep, *dcp;  // S*ucp, -S*ucp, S*uep, -S*uep
+        int r1, r2, canon;
+    };
+    std::map<std::pair<double, Idx3>, DirPts> dirpts;
+    auto get_dir = [&](double W, const Idx3& dir) -> const DirPts& {
+        auto key = std::make_pair(W, dir);
+        auto it = dirpts.find(key);
+        if (it != dirpts.end()) return it->second;
+        Idx3 sgn, pv;
+        int c = get_canon(W, dir, sgn, pv);
+        const HighFreqOp& op = *hfcanon[c].op;
+        DirPts d{};
+        d.canon = c;
+        d.r1 = hfcanon[c].r1;
+        d.r2 = hfcanon[c].r2;
+        d.ucp = upload(shuffle(op.ucp, pv, sgn, 1.0));
+        d.dep = upload(shuffle(op.ucp, pv, sgn, -1.0));
+        d.uep = upload(shuffle(op.uep, pv, sgn, 1.0));
+        d.dcp = upload(shuffle(op.uep, pv, sgn, -1.0));
+        return dirpts[key] = d;
+    };
+
+    std::map<int, std::vector<int> > hflevels;  // level -> tree boxes with points, width >= 1
+    for (int b : T.order)
+        if (T.boxes[b].has_pts() && T.width(T.boxes[b].level) > 1 - eps) hflevels[T.boxes[b].level].push_back(b);
+
+    std::vector<Node> up, dn;
+    std::unordered_map<uint64_t, int> upmap, dnmap;
+    NodeKey nk;
+    std::map<int, std::pair<int, int> > uprange, dnrange;  // level -> [begin, end)
+    long long upeq_total = 0, dnchk_total = 0, tmp_max = 0;
+    for (auto& kv : hflevels) {
+        double W = T.width(kv.first);
+        long long tmp_up = 0, tmp_dn = 0;
+        int u0 = (int)up.size(), d0 = (int)dn.size();
+        for (int b : kv.second) {
+            for (const Idx3& d : T.boxes[b].outdirs) {
+                const DirPts& dp = get_dir(W, d);
+                Node nd{b, d, dp.canon, upeq_total, tmp_up};
+                upeq_total += dp.r1;
+                tmp_up += std::max(dp.r1, dp.r2);
+                upmap[nk(b, d)] = (int)up.size();
+                up.push_back(nd);
+            }
+            for (const Idx3& d : T.boxes[b].incdirs) {
+                const DirPts& dp = get_dir(W, d);
+                Node nd{b, d, dp.canon, dnchk_total, tmp_dn};
+                dnchk_total += dp.r1;
+                tmp_dn += std::max(dp.r1, dp.r2);
+                dnmap[nk(b, d)] = (int)dn.size();
+                dn.push_back(nd);
+            }
+        }
+        uprange[kv.first] = std::make_pair(u0, (int)up.size());
+        dnrange[kv.first] = std::make_pair(d0, (int)dn.size());
+        tmp_max = std::max(tmp_max, std::max(tmp_up, tmp_dn));
+    }
+    stats_.hf_up_nodes = (long long)up.size();
+    stats_.hf_down_nodes = (long long)dn.size();
+    double2* hf_upeq = dalloc<double2>((size_t)upeq_total);
+    double2* hf_dnchk = dalloc<double2>((size_t)dnchk_total);
+    double2* T0 = dalloc<double2>((size_t)tmp_max);
+    double2* T1 = dalloc<double2>((size_t)tmp_max);
+    double2* T2 = dalloc<double2>((size_t)tmp_max);
+    zero_at_start_.push_back(Memset{hf_dnchk, sizeof(double2) * (size_t)dnchk_total});
+
+    // HF M2M / L2L matrices per (W, dir, child) and M2L matrices per
+    // (W, canonical wedge, canonical offset); all generated once here.
+    struct DirMats {
+        double2* m2m[8];
+        double2* l2l[8];
+        int mrows, mcols;  // m2m: r2 x rc ; l2l: rc x r2
+    };
+    std::map<std::pair<double, Idx3>, DirMats> m2m_mats, l2l_mats;
+    const LowFreqOp* lf_half = nullptr;
+    const double* lf_half_uep = nullptr;
+    if (!hflevels.empty()) {
+        lf_half = &ops_.low(0.5);
+        if (lf_half->uep.n != nE) throw std::runtime_error("width-1/2 operators do not match ACCU");
+        lf_half_uep = upload(lf_half->uep.x);
+    }
+    auto child_pts = [&](double W, const Idx3& dir, bool upward, int& rc) -> const double* {
+        if (W == 1.0) {
+            rc = nE;
+            return lf_half_uep;  // LF uep at W/2 for both directions (src/mlib3d.cpp:199-202,254-257)
+        }
+        const DirPts& cp = get_dir(W / 2, predir(dir));
+        rc = cp.r1;
+        return upward ? cp.uep : cp.dcp;
+    };
+    for (auto& kv : hflevels) {
+        double W = T.width(kv.first);
+        auto ur = uprange[kv.first], dr = dnrange[kv.first];
+        for (int i = ur.first; i < ur.second; ++i) {
+            auto key = std::make_pair(W, up[i].dir);
+            if (m2m_mats.count(key)) continue;
+            const DirPts& dp = get_dir(W, up[i].dir);
+            int rc;
+            const double* cp = child_pts(W, up[i].dir, true, rc);
+            DirMats M{};
+            M.mrows = dp.r2;
+            M.mcols = rc;
+            for (int ind = 0; ind < 8; ++ind) {
+                M.m2m[ind] = dalloc<double2>((size_t)dp.r2 * rc);
+                add_job(dp.ucp, zero3, cp, shifted_point(ind, W), dp.r2, rc, M.m2m[ind]);
+            }
+            m2m_mats[key] = M;
+        }
+        for (int i = dr.first; i < dr.second; ++i) {
+            auto key = std::make_pair(W, dn[i].dir);
+            if (l2l_mats.count(key)) continue;
+            const DirPts& dp = get_dir(W, dn[i].dir);
+            int rc;
+            const double* cp = child_pts(W, dn[i].dir, false, rc);
+            DirMats M{};
+            M.mrows = rc;
+            M.mcols = dp.r2;
+            for (int ind = 0; ind < 8; ++ind) {
+                M.l2l[ind] = dalloc<double2>((size_t)rc * dp.r2);
+                add_job(cp, shifted_point(ind, W), dp.dep, zero3, rc, dp.r2, M.l2l[ind]);
+            }
+            l2l_mats[key] = M;
+        }
+    }
+    // M2L: canonical offset o_c = S^-1 (c_t - c_s) (see DESIGN: M(dir, o) = M(canon, S^-1 o))
+    std::map<std::tuple<int, int, int, int>, int> m2l_id;  // (canon, ox, oy, oz) -> problem
+    struct M2LMat {
+        double2* A;
+        int r1;
+    };
+    std::vector<M2LMat> m2l_mats;
+    std::map<int, std::vector<std::vector<long long> > > m2l_x, m2l_y;  // level -> per problem columns
+    std::map<int, std::vector<int> > m2l_probs;                         // level -> problem ids
+    for (auto& kv : hflevels) {
+        int level = kv.first;
+        double W = T.width(level);
+        auto dr = dnrange[level];
+        std::map<int, int> local;  // global m2l id -> local problem index
+        auto& X = m2l_x[level];
+        auto& Y = m2l_y[level];
+        auto& Pids = m2l_probs[level];
+        for (int i = dr.first; i < dr.second; ++i) {
+            const Node& t = dn[i];
+            const Box& tb = T.boxes[t.box];
+            auto fit = tb.far.find(t.dir);
+            if (fit == tb.far.end()) continue;
+            Idx3 sgn, pv, srt;
+            index3_sort(t.dir, srt, sgn, pv);
+            for (int s : fit->second) {
+                auto uit = upmap.find(nk(s, t.dir));
+                if (uit == upmap.end()) throw std::runtime_error("M2L source has no outgoing equivalent density");
+                const Box& sb = T.boxes[s];
+                int o[3], oc[3];
+                for (int d = 0; d < 3; ++d) o[d] = tb.idx[d] - sb.idx[d];
+                for (int d = 0; d < 3; ++d) oc[d] = sgn[pv[d]] * o[pv[d]];
+                auto key = std::make_tuple(t.canon, oc[0], oc[1], oc[2]);
+                auto mit = m2l_id.find(key);
+                int gid;
+                if (mit == m2l_id.end()) {
+                    const Canon& c = hfcanon[t.canon];
+                    gid = (int)m2l_mats.size();
+                    M2LMat M{dalloc<double2>((size_t)c.r1 * c.r1), c.r1};
+                    Pt3 sh{{oc[0] * W, oc[1] * W, oc[2] * W}};
+                    add_job(c.neg_uep, sh, c.uep, zero3, c.r1, c.r1, M.A);
+                    m2l_mats.push_back(M);
+                    m2l_id[key] = gid;
+                } else {
+                    gid = mit->second;
+                }
+                auto lit = local.find(gid);
+                int li;
+                if (lit == local.end()) {
+                    li = (int)Pids.size();
+                    local[gid] = li;
+                    Pids.push_back(gid);
+                    X.emplace_back();
+                    Y.emplace_back();
+                } else {
+                    li = lit->second;
+                }
+                X[li].push_back(up[uit->second].off);
+                Y[li].push_back(t.off);
+                stats_.hf_far_pairs++;
+            }
+        }
+    }
+    stats_.m2l_matrices = (long long)m2l_mats.size();
+
+    // generate every kernel matrix now
+    if (!jobs.empty()) {
+        KmatJob* d_jobs = upload(jobs);
+        launch_kmat(d_jobs, (int)jobs.size(), job_elems, kern, stream_);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(stream_));
+    }
+
+    // ---------------------------------------------------------------- steps: LF upward
+    auto lf_set = [&](const double* x, int n, Pt3 shift, double scale) {
+        PtSet s;
+        s.x = x;
+        s.n = n;
+        for (int d = 0; d < 3; ++d) s.shift[d] = shift[d];
+        s.scale = scale;
+        return s;
+    };
+    auto leaf_set = [&](int l) { return lf_set(d_pos_sorted_ + 3 * (size_t)leaf_off[l], leaf_cnt[l], zero3, 1.0); };
+    auto single = [&](const GemmProblem& p, const std::vector<long long>& x, const std::vector<long long>& y,
+                      const double2* X, double2* Y, int mode) {
+        std::vector<GemmProblem> ps(1, p);
+        std::vector<std::vector<long long> > xo(1, x), yo(1, y);
+        add_gemm(ps, xo, yo, X, Y, mode);
+    };
+    for (auto it = lflevels.rbegin(); it != lflevels.rend(); ++it) {
+        const LfLevelOps& L = lfops[it->first];
+        const auto& ids = it->second;
+        // S2M at leaves (src/wave3d_eval.cpp:441-451)
+        std::vector<PtItem> items;
+        std::vector<PtSrc> srcs;
+        for (int l : ids) {
+            const Box& B = T.boxes[lfbox[l]];
+            if (!B.terminal()) continue;
+            PtItem itm;
+            itm.trg = lf_set(L.ucp, nE, T.center(B), 1.0);
+            itm.out = lf_upchk + (size_t)l * nE;
+            itm.src_begin = (int)srcs.size();
+            srcs.push_back(PtSrc{leaf_set(l), d_den_sorted_ + leaf_off[l]});
+            itm.src_end = (int)srcs.size();
+            items.push_back(itm);
+        }
+        add_pt(items, srcs);
+        // M2M from children (src/wave3d_eval.cpp:452-463)
+        if (L.has_children)
+            for (int ind = 0; ind < 8; ++ind) {
+                std::vector<long long> x, y;
+                for (int l : ids) {
+                    int b = lfbox[l];
+                    if (T.boxes[b].terminal()) continue;
+                    int c = T.child(b, ind);
+                    if (c < 0 || !T.boxes[c].has_pts()) continue;
+                    x.push_back((long long)lfidx[c] * nE);
+                    y.push_back((long long)l * nE);
+                }
+                single(GemmProblem{L.ue2uc[ind], nE, nE, nE, 0, 0}, x, y, lf_upeq, lf_upchk, GEMM_ADD);
+            }
+        // upeqnden = v * (1/sigma .* (U^H * upchk))   (src/wave3d_eval.cpp:466-478)
+        std::vector<long long> a, b2;
+        for (int l : ids) {
+            a.push_back((long long)l * nE);
+            b2.push_back((long long)l * nE);
+        }
+        single(GemmProblem{L.up_s, L.r, nE, L.r, 0, 0}, a, b2, lf_upchk, lf_mid, GEMM_SET);
+        single(GemmProblem{L.v, nE, L.r, nE, 0, 0}, a, b2, lf_mid, lf_upeq, GEMM_SET);
+    }
+
+    // ---------------------------------------------------------------- steps: HF upward
+    for (auto& kv : hflevels) {
+        int level = kv.first;
+        double W = T.width(level);
+        auto ur = uprange[level];
+        if (ur.first == ur.second) continue;
+        Step ms{};
+        ms.kind = 4;
+        ms.ms = Memset{T0, sizeof(double2) * (size_t)tmp_max};
+        steps_.push_back(ms);
+        // M2M: upchk = sum_children ue2uc(abc) * child's upeqnden (src/wave3d_eval.cpp:796-834)
+        for (int ind = 0; ind < 8; ++ind) {
+            std::map<Idx3, int> pid;
+            std::vector<GemmProblem> probs;
+            std::vector<std::vector<long long> > xo, yo;
+            for (int i = ur.first; i < ur.second; ++i) {
+                const Node& u = up[i];
+                int c = T.child(u.box, ind);
+                if (c < 0 || !T.boxes[c].has_pts()) continue;
+                long long xoff;
+                if (W == 1.0) {
+                    xoff = (long long)lfidx[c] * nE;
+                } else {
+                    auto cit = upmap.find(nk(c, predir(u.dir)));
+                    if (cit == upmap.end()) throw std::runtime_error("child has no directional equivalent density");
+                    xoff = up[cit->second].off;
+                }
+                auto pit = pid.find(u.dir);
+                int p;
+                if (pit == pid.end()) {
+                    const DirMats& M = m2m_mats.at(std::make_pair(W, u.dir));
+                    p = (int)probs.size();
+                    pid[u.dir] = p;
+                    probs.push_back(GemmProblem{M.m2m[ind], M.mrows, M.mcols, M.mrows, 0, 0});
+                    xo.emplace_back();
+                    yo.emplace_back();
+                } else {
+                    p = pit->second;
+                }
+                xo[p].push_back(xoff);
+                yo[p].push_back(u.toff);
+            }
+            add_gemm(probs, xo, yo, W == 1.0 ? lf_upeq : hf_upeq, T0, GEMM_ADD);
+        }
+        // upeqnden = E1 * (E2 * (E3 * upchk))   (src/wave3d_eval.cpp:837-849)
+        std::map<int, int> cp;
+        std::vector<GemmProblem> p3, p2, p1;
+        std::vector<std::vector<long long> > xa, ya, xb;
+        for (int i = ur.first; i < ur.second; ++i) {
+            const Node& u = up[i];
+            auto it2 = cp.find(u.canon);
+            int p;
+            if (it2 == cp.end()) {
+                const Canon& c = hfcanon[u.canon];
+                p = (int)p3.size();
+                cp[u.canon] = p;
+                p3.push_back(GemmProblem{c.E3, c.r2, c.r2, c.r2, 0, 0});
+                p2.push_back(GemmProblem{c.E2, c.r1, c.r2, c.r1, 0, 0});
+                p1.push_back(GemmProblem{c.E1, c.r1, c.r1, c.r1, 0, 0});
+                xa.emplace_back();
+                ya.emplace_back();
+            } else {
+                p = it2->second;
+            }
+            xa[p].push_back(u.toff);
+            ya[p].push_back(u.off);
+        }
+        add_gemm(p3, xa, xa, T0, T1, GEMM_SET);
+        add_gemm(p2, xa, xa, T1, T2, GEMM_SET);
+        add_gemm(p1, xa, ya, T2, hf_upeq, GEMM_SET);
+    }
+
+    // ---------------------------------------------------------------- steps: HF downward
+    for (auto it = hflevels.rbegin(); it != hflevels.rend(); ++it) {
+        int level = it->first;
+        double W = T.width(level);
+        auto dr = dnrange[level];
+        if (dr.first == dr.second) continue;
+        // M2L (src/wave3d_eval.cpp:876-928)
+        {
+            std::vector<GemmProblem> probs;
+            for (int gid : m2l_probs[level]) {
+                const M2LMat& M = m2l_mats[gid];
+                probs.push_back(GemmProblem{M.A, M.r1, M.r1, M.r1, 0, 0});
+            }
+            add_gemm(probs, m2l_x[level], m2l_y[level], hf_upeq, hf_dnchk, GEMM_ATOMIC);
+        }
+        // dneqnden = E3^T (E2^T (E1^T dnchk))   (src/wave3d_eval.cpp:938-948, src/mlib3d.cpp:246-250)
+        std::map<int, int> cp;
+        std::vector<GemmProblem> p1, p2, p3;
+        std::vector<std::vector<long long> > xa, xt;
+        for (int i = dr.first; i < dr.second; ++i) {
+            const Node& d = dn[i];
+            auto it2 = cp.find(d.canon);
+            int p;
+            if (it2 == cp.end()) {
+                const Canon& c = hfcanon[d.canon];
+                p = (int)p1.size();
+                cp[d.canon] = p;
+                p1.push_back(GemmProblem{c.E1t, c.r1, c.r1, c.r1, 0, 0});
+                p2.push_back(GemmProblem{c.E2t, c.r2, c.r1, c.r2, 0, 0});
+                p3.push_back(GemmProblem{c.E3t, c.r2, c.r2, c.r2, 0, 0});
+                xa.emplace_back();
+                xt.emplace_back();
+            } else {
+                p = it2->second;
+            }
+            xa[p].push_back(d.off);
+            xt[p].push_back(d.toff);
+        }
+        add_gemm(p1, xa, xt, hf_dnchk, T0, GEMM_SET);
+        add_gemm(p2, xt, xt, T0, T1, GEMM_SET);
+        add_gemm(p3, xt, xt, T1, T2, GEMM_SET);
+        // L2L into the children's (pdir) check values, or LF dnchkval at W=1 (src/wave3d_eval.cpp:950-991)
+        for (int ind = 0; ind < 8; ++ind) {
+            std::map<Idx3, int> pid;
+            std::vector<GemmProblem> probs;
+            std::vector<std::vector<long long> > xo, yo;
+            for (int i = dr.first; i < dr.second; ++i) {
+                const Node& d = dn[i];
+                int c = T.child(d.box, ind);
+                if (c < 0 || !T.boxes[c].has_pts()) continue;
+                long long yoff;
+                if (W == 1.0) {
+                    yoff = (long long)lfidx[c] * nE;
+                } else {
+                    auto cit = dnmap.find(nk(c, predir(d.dir)));
+                    if (cit == dnmap.end()) throw std::runtime_error("child has no directional check value");
+                    yoff = dn[cit->second].off;
+                }
+                auto pit = pid.find(d.dir);
+                int p;
+                if (pit == pid.end()) {
+                    const DirMats& M = l2l_mats.at(std::make_pair(W, d.dir));
+                    p = (int)probs.size();
+                    pid[d.dir] = p;
+                    probs.push_back(GemmProblem{M.l2l[ind], M.mrows, M.mcols, M.mrows, 0, 0});
+                    xo.emplace_back();
+                    yo.emplace_back();
+                } else {
+                    p = pit->second;
+                }
+                xo[p].push_back(d.toff);
+                yo[p].push_back(yoff);
+            }
+            add_gemm(probs, xo, yo, T2, W == 1.0 ? lf_dnchk : hf_dnchk, GEMM_ATOMIC);
+        }
+    }
+
+    // ---------------------------------------------------------------- steps: LF downward
+    for (auto& kv : lflevels) {  // levels ascending = widths descending
+        int level = kv.first;
+        const LfLevelOps& L = lfops[level];
+        const auto& ids = kv.second;
+        double W = L.W;
+        // V list: FFT M2L (src/wave3d_eval.cpp:602-661)
+        {
+            std::vector<int> trg, vptr(1, 0), vsrc, voff;
+            std::vector<char> is_src(nLF, 0);
+            for (int l : ids) {
+                const Box& B = T.boxes[lfbox[l]];
+                if (B.vlist.empty()) continue;
+                Pt3 tc = T.center(B);
+                trg.push_back(l);
+                for (int s : B.vlist) {
+                    Pt3 sc = T.center(T.boxes[s]);
+                    int o[3];
+                    for (int d = 0; d < 3; ++d) o[d] = (int)std::round((tc[d] - sc[d]) / W);
+                    vsrc.push_back(lfidx[s]);
+                    voff.push_back((o[0] + 3) + 7 * ((o[1] + 3) + 7 * (o[2] + 3)));
+                    is_src[lfidx[s]] = 1;
+                    stats_.v_pairs++;
+                }
+                vptr.push_back((int)vsrc.size());
+            }
+            if (!trg.empty()) {
+                std::vector<int> srcb;
+                for (int l = 0; l < nLF; ++l)
+                    if (is_src[l]) srcb.push_back(l);
+                VlistLevel VL{G, P, nE, L.grid_idx, L.tns, d_twf, d_twb};
+                Step f{};
+                f.kind = 2;
+                f.v.L = VL;
+                f.v.src_boxes = upload(srcb);
+                f.v.nsrc = (int)srcb.size();
+                f.v.upeq = lf_upeq;
+                f.v.spec = lf_spec;
+                steps_.push_back(f);
+                Step a{};
+                a.kind = 3;
+                a.v.L = VL;
+                a.v.trg = upload(trg);
+                a.v.vptr = upload(vptr);
+                a.v.vsrc = upload(vsrc);
+                a.v.voff = upload(voff);
+                a.v.ntrg = (int)trg.size();
+                a.v.spec = lf_spec;
+                a.v.dnchk = lf_dnchk;
+                steps_.push_back(a);
+            }
+        }
+        // X list (src/wave3d_eval.cpp:663-686), into dnchk or, for small leaves, into extval
+        {
+            std::vector<PtItem> itemsA, itemsB;
+            std::vector<PtSrc> srcsA, srcsB;
+            for (int l : ids) {
+                const Box& B = T.boxes[lfbox[l]];
+                if (B.xlist.empty()) continue;
+                bool direct = B.terminal() && leaf_cnt[l] < nE;
+                PtItem itm;
+                itm.trg = direct ? leaf_set(l) : lf_set(L.uep, nE, T.center(B), 1.0);
+                itm.out = direct ? d_val_sorted_ + leaf_off[l] : lf_dnchk + (size_t)l * nE;
+                auto& S = direct ? srcsA : srcsB;
+                itm.src_begin = (int)S.size();
+                for (int s : B.xlist) {
+                    int ls = lfidx[s];
+                    S.push_back(PtSrc{leaf_set(ls), d_den_sorted_ + leaf_off[ls]});
+                    stats_.x_pairs++;
+                }
+                itm.src_end = (int)S.size();
+                (direct ? itemsA : itemsB).push_back(itm);
+            }
+            add_pt(itemsA, srcsA);
+            add_pt(itemsB, srcsB);
+        }
+        // U list (src/wave3d_eval.cpp:585-600) and W list (:688-718) into extval
+        {
+            std::vector<PtItem> items, witems;
+            std::vector<PtSrc> srcs, wsrcs;
+            for (int l : ids) {
+                const Box& B = T.boxes[lfbox[l]];
+                if (!B.ulist.empty()) {
+                    PtItem itm;
+                    itm.trg = leaf_set(l);
+                    itm.out = d_val_sorted_ + leaf_off[l];
+                    itm.src_begin = (int)srcs.size();
+                    for (int s : B.ulist) {
+                        int ls = lfidx[s];
+                        srcs.push_back(PtSrc{leaf_set(ls), d_den_sorted_ + leaf_off[ls]});
+                        stats_.u_pairs++;
+                        stats_.u_interactions += (long long)leaf_cnt[l] * leaf_cnt[ls];
+                    }
+                    itm.src_end = (int)srcs.size();
+                    items.push_back(itm);
+                }
+                if (!B.wlist.empty()) {
+                    PtItem itm;
+                    itm.trg = leaf_set(l);
+                    itm.out = d_val_sorted_ + leaf_off[l];
+                    itm.src_begin = (int)wsrcs.size();
+                    for (int s : B.wlist) {
+                        int ls = lfidx[s];
+                        const Box& SB = T.boxes[s];
+                        if (SB.terminal() && leaf_cnt[ls] < nE) {
+                            wsrcs.push_back(PtSrc{leaf_set(ls), d_den_sorted_ + leaf_off[ls]});
+                        } else {
+                            double coef = T.width(SB.level) / W;
+                            wsrcs.push_back(PtSrc{lf_set(L.uep, nE, T.center(SB), coef), lf_upeq + (size_t)ls * nE});
+                        }
+                        stats_.w_pairs++;
+                    }
+                    itm.src_end = (int)wsrcs.size();
+                    witems.push_back(itm);
+                }
+            }
+            add_pt(items, srcs);
+            add_pt(witems, wsrcs);
+        }
+        // dneqnden = up^T (1/sigma .* (v^T dnchk))   (src/wave3d_eval.cpp:536-547, src/mlib3d.cpp:147-152)
+        std::vector<long long> a;
+        for (int l : ids) a.push_back((long long)l * nE);
+        single(GemmProblem{L.vT_s, L.r, nE, L.r, 0, 0}, a, a, lf_dnchk, lf_mid, GEMM_SET);
+        single(GemmProblem{L.upT, nE, L.r, nE, 0, 0}, a, a, lf_mid, lf_dneq, GEMM_SET);
+        // L2T at leaves (src/wave3d_eval.cpp:550-560)
+        {
+            std::vector<PtItem> items;
+            std::vector<PtSrc> srcs;
+            for (int l : ids) {
+                const Box& B = T.boxes[lfbox[l]];
+                if (!B.terminal()) continue;
+                PtItem itm;
+                itm.trg = leaf_set(l);
+                itm.out = d_val_sorted_ + leaf_off[l];
+                itm.src_begin = (int)srcs.size();
+                srcs.push_back(PtSrc{lf_set(L.ucp, nE, T.center(B), 1.0), lf_dneq + (size_t)l * nE});
+                itm.src_end = (int)srcs.size();
+                items.push_back(itm);
+            }
+            add_pt(items, srcs);
+        }
+        // L2L to the children (src/wave3d_eval.cpp:562-579)
+        if (L.has_children)
+            for (int ind = 0; ind < 8; ++ind) {
+                std::vector<long long> x, y;
+                for (int l : ids) {
+                    int b = lfbox[l];
+                    if (T.boxes[b].terminal()) continue;
+                    int c = T.child(b, ind);
+                    if (c < 0 || !T.boxes[c].has_pts()) continue;
+                    x.push_back((long long)l * nE);
+                    y.push_back((long long)lfidx[c] * nE);
+                }
+                single(GemmProblem{L.de2dc[ind], nE, nE, nE, 0, 0}, x, y, lf_dneq, lf_dnchk, GEMM_ADD);
+            }
+    }
+    stats_.kernel_launches = (long long)steps_.size() + 2;
+}
+
+void Session::run_steps(cudaStream_t s) {
+    for (const Memset& m : zero_at_start_) CK(cudaMemsetAsync(m.p, 0, m.bytes, s));
+    for (const Step& st : steps_) {
+        switch (st.kind) {
+            case 0:
+                launch_gemm(st.g.probs, st.g.tiles, st.g.ntiles, st.g.xoff, st.g.yoff, st.g.X, st.g.Y, st.g.mode, s);
+                break;
+            case 1:
+                launch_pt(st.pt.items, st.pt.nitems, st.pt.srcs, prm_.kernel, s);
+                break;
+            case 2:
+                launch_vlist_forward(st.v.L, st.v.src_boxes, st.v.nsrc, st.v.upeq, st.v.spec, s);
+                break;
+            case 3:
+                launch_vlist_accum(st.v.L, st.v.trg, st.v.ntrg, st.v.vptr, st.v.vsrc, st.v.voff, st.v.spec,
+                                   st.v.dnchk, s);
+                break;
+            case 4:
+                CK(cudaMemsetAsync(st.ms.p, 0, st.ms.bytes, s));
+                break;
+        }
+    }
+}
+
+void Session::eval_device(const double2* den, double2* val, cudaStream_t s) {
+    launch_gather_den(den, d_perm_, d_den_sorted_, npts_, s);
+    run_steps(s);
+    launch_scatter_val(d_val_sorted_, d_perm_, val, npts_, s);
+    CK(cudaGetLastError());
+}
+
+void Session::eval_host(const std::complex<double>* den, std::complex<double>* val) {
+    CK(cudaMemcpyAsync(d_den_io_, den, sizeof(double2) * npts_, cudaMemcpyHostToDevice, stream_));
+    eval_device(d_den_io_, d_val_io_, stream_);
+    CK(cudaMemcpyAsync(val, d_val_io_, sizeof(double2) * npts_, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void Session::direct_host(const std::complex<double>* den, const int* ids, int nids, std::complex<double>* out) {
+    if (nids <= 0) return;
+    for (int i = 0; i < nids; ++i)
+        if (ids[i] < 0 || ids[i] >= npts_) throw std::runtime_error("check id out of range");
+    int* d_ids = nullptr;
+    double2* d_out = nullptr;
+    CK(cudaMalloc(&d_ids, sizeof(int) * nids));
+    CK(cudaMalloc(&d_out, sizeof(double2) * nids));
+    CK(cudaMemcpyAsync(d_den_io_, den, sizeof(double2) * npts_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(d_ids, ids, sizeof(int) * nids, cudaMemcpyHostToDevice, stream_));
+    launch_direct(d_pos_ids_, d_den_io_, npts_, d_ids, nids, d_out, prm_.kernel, stream_);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, d_out, sizeof(double2) * nids, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    cudaFree(d_ids);
+    cudaFree(d_out);
+}
+
+}  // namespace ddfmm

@@ -1,0 +1,127 @@
+// One FMM instance resident on one GPU: tree, lists, operators and buffers
+// built once (Wave3d::setup, src/wave3d_setup.cpp:21-97), then any number of
+// matvecs (Wave3d::eval, src/wave3d_eval.cpp:299-415) with fresh densities.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <complex>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "ops.hpp"
+#include "tree.hpp"
+
+namespace ddfmm {
+
+struct SessionParams {
+    TreeParams tree;
+    int accu = 1;    // -wave3d_ACCU: P = 4/6/8 (src/wave3d.cpp:145-158)
+    int kernel = 0;  // KERNEL_HELM / KERNEL_EXPR
+    int device = 0;
+};
+
+struct SessionStats {
+    int n_points = 0, n_boxes = 0, n_leaves = 0, n_lf_boxes = 0;
+    long long u_pairs = 0, u_interactions = 0, v_pairs = 0, w_pairs = 0, x_pairs = 0;
+    long long hf_up_nodes = 0, hf_down_nodes = 0, hf_far_pairs = 0;
+    long long m2l_matrices = 0, gemm_launches = 0, kernel_launches = 0;
+    double flops_gemm = 0;        // 8 real flops per complex multiply-add
+    long long fft_spectra_bytes = 0;
+    double setup_seconds = 0;
+    size_t device_bytes = 0;
+};
+
+class Session {
+public:
+    Session(const double* pos3n, int n, const SessionParams& p, const std::string& ld_path,
+            const std::string& hd_path);
+    ~Session();
+    Session(const Session&) = delete;
+    Session& operator=(const Session&) = delete;
+
+    // val = G * den at every point; arrays in point-id order, complex128.
+    void eval_host(const std::complex<double>* den, std::complex<double>* val);
+    void eval_device(const double2* den, double2* val, cudaStream_t s);
+    // FP64 direct sum at the given point ids (Wave3d::check, src/wave3d_check.cpp:22-100)
+    void direct_host(const std::complex<double>* den, const int* ids, int nids, std::complex<double>* out);
+
+    const SessionStats& stats() const { return stats_; }
+    int npts() const { return npts_; }
+    cudaStream_t stream() const { return stream_; }
+
+private:
+    struct GemmLaunch {
+        GemmProblem* probs = nullptr;
+        GemmTile* tiles = nullptr;
+        long long* xoff = nullptr;
+        long long* yoff = nullptr;
+        int ntiles = 0;
+        const double2* X = nullptr;
+        double2* Y = nullptr;
+        int mode = 0;
+    };
+    struct PtLaunch {
+        PtItem* items = nullptr;
+        PtSrc* srcs = nullptr;
+        int nitems = 0;
+    };
+    struct VLaunch {
+        VlistLevel L;
+        int* src_boxes = nullptr;
+        int nsrc = 0;
+        int* trg = nullptr;
+        int* vptr = nullptr;
+        int* vsrc = nullptr;
+        int* voff = nullptr;
+        int ntrg = 0;
+        const double2* upeq = nullptr;
+        double2* spec = nullptr;
+        double2* dnchk = nullptr;
+    };
+    struct Memset {
+        void* p;
+        size_t bytes;
+    };
+    // one step of the eval: exactly one of these is used
+    struct Step {
+        int kind;  // 0 gemm, 1 pt, 2 vfwd, 3 vacc, 4 memset
+        GemmLaunch g;
+        PtLaunch pt;
+        VLaunch v;
+        Memset ms;
+    };
+
+    template <class T>
+    T* dalloc(size_t count);
+    template <class T>
+    T* upload(const std::vector<T>& v);
+    void add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<long long> >& xo,
+                  std::vector<std::vector<long long> >& yo, const double2* X, double2* Y, int mode);
+    void add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>& srcs);
+    void build();
+    void run_steps(cudaStream_t s);
+
+    SessionParams prm_;
+    int npts_ = 0;
+    std::vector<double> pos_;
+    Tree tree_;
+    OperatorLib ops_;
+    std::vector<void*> allocs_;
+    std::vector<Step> steps_;
+    cudaStream_t stream_ = nullptr;
+    SessionStats stats_;
+
+    // device state
+    int* d_perm_ = nullptr;
+    double* d_pos_ids_ = nullptr;
+    double* d_pos_sorted_ = nullptr;
+    double2* d_den_sorted_ = nullptr;
+    double2* d_val_sorted_ = nullptr;
+    double2* d_den_io_ = nullptr;
+    double2* d_val_io_ = nullptr;
+    std::vector<Memset> zero_at_start_;
+};
+
+}  // namespace ddfmm

@@ -49,6 +49,27 @@ def ellipsoid_points(n: int, K: float, seed: int = 0, axes=(0.5, 0.25, 0.125)) -
     return np.concatenate(out)[:n]
 
 
+def cluster_points(n: int, K: float, seed: int = 0) -> np.ndarray:
+    """Strongly non-uniform cloud for adaptive trees: half the points on a
+    sphere of diameter 0.8 K, the rest in three tight Gaussian blobs, plus a
+    few exact duplicates (coincident pairs exercise the r := 1 rule of
+    src/kernel3d.cpp:47-49)."""
+    rng = np.random.default_rng(seed)
+    n_s = n // 2
+    v = rng.standard_normal((n_s, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    parts = [v * 0.4 * K]
+    centres = np.array([[0.2, 0.1, -0.15], [-0.25, 0.2, 0.1], [0.05, -0.3, 0.3]]) * K
+    n_b = n - n_s - 8
+    for i in range(3):
+        m = n_b // 3 + (1 if i < n_b % 3 else 0)
+        parts.append(centres[i] + rng.standard_normal((m, 3)) * (0.02 * K))
+    pts = np.concatenate(parts)
+    pts = np.clip(pts, -0.5 * K * SHRINK, 0.5 * K * SHRINK)
+    dup = pts[rng.choice(pts.shape[0], size=8, replace=False)]
+    return np.concatenate([pts, dup])
+
+
 def sphere_n_for(K: float, pts_per_wl2: float = 25.0) -> int:
     """N for a sphere of diameter K at a given density (area pi K^2)."""
     return int(round(pts_per_wl2 * math.pi * K * K))

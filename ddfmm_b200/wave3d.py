@@ -1,0 +1,173 @@
+"""Host-side mirror of the reference's Wave3d / Mlib3d interface.
+
+Usage follows the reference driver (src/tt.cpp:103-185):
+
+    mlib = Mlib3d("mlib3d_"); mlib.kernel = kernel; mlib.setup(opts)
+    wave = Wave3d("wave3d_")
+    wave.posptr = pos            # (N, 3) float64, point ids 0..N-1
+    wave.kernel = kernel
+    wave.mlibptr = mlib
+    wave.geomprtn = nc           # cells per edge of the partition tensor
+    wave.setup(opts)             # -wave3d_ACCU/NPQ/K/ctr/ptsmax/maxlevel
+    wave.eval(den, val)          # val[:] = FMM matvec of den
+    relerr = wave.check(den, val, chkkeys)
+
+ParVec<int, cpx, PtPrtn> becomes a complex128 array indexed by point id.
+Failures raise DDFMMError where the reference throws std::exception.
+Every eval runs on the GPU through libddfmm_b200.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _lib
+
+
+def _opt(opts, key, default, conv):
+    v = opts.get(key)
+    return conv(v) if v is not None else default
+
+
+class Mlib3d:
+    """Operator library handle: the ld/hd files named by -<prefix>ldname and
+    -<prefix>hdname (src/mlib3d.cpp:70-103).  The files are read by the
+    native library when a Wave3d session is set up."""
+
+    def __init__(self, prefix="mlib3d_"):
+        self.prefix = prefix
+        self.kernel = 0
+        self.NPQ = 4
+        self.ldname = None
+        self.hdname = None
+
+    def setup(self, opts):
+        p = "-" + self.prefix
+        self.NPQ = _opt(opts, p + "NPQ", self.NPQ, int)
+        self.ldname = _opt(opts, p + "ldname", self.ldname, str)
+        self.hdname = _opt(opts, p + "hdname", self.hdname, str)
+        for f in (self.ldname, self.hdname):
+            if not f or not os.path.exists(f):
+                raise _lib.DDFMMError(3, "operator file not found: %r" % (f,))
+        return 0
+
+
+class Wave3d:
+    def __init__(self, prefix="wave3d_", device=0):
+        self.prefix = prefix
+        self.posptr = None
+        self.kernel = 0
+        self.mlibptr = None
+        self.geomprtn = None
+        self.ACCU = 1
+        self.NPQ = 4
+        self.K = 64.0
+        self.ctr = (0.0, 0.0, 0.0)
+        self.ptsmax = 100
+        self.maxlevel = None
+        self.device = device
+        self._s = None
+        self._n = 0
+
+    # src/wave3d_setup.cpp:21-97
+    def setup(self, opts):
+        lib = _lib.load()
+        p = "-" + self.prefix
+        self.ACCU = _opt(opts, p + "ACCU", self.ACCU, int)
+        self.NPQ = _opt(opts, p + "NPQ", self.NPQ, int)
+        self.K = _opt(opts, p + "K", self.K, float)
+        self.ctr = _opt(opts, p + "ctr", self.ctr, lambda s: tuple(float(x) for x in s.split()))
+        self.ptsmax = _opt(opts, p + "ptsmax", self.ptsmax, int)
+        self.maxlevel = _opt(opts, p + "maxlevel", self.maxlevel, int)
+        if self.maxlevel is None:
+            raise _lib.DDFMMError(1, "-%smaxlevel is required" % self.prefix)
+        if self.posptr is None or self.mlibptr is None or self.geomprtn is None:
+            raise _lib.DDFMMError(1, "posptr, mlibptr and geomprtn must be set before setup")
+        pos = np.ascontiguousarray(self.posptr, dtype=np.float64).reshape(-1, 3)
+        nc = self.geomprtn if isinstance(self.geomprtn, int) else int(np.asarray(self.geomprtn).shape[0])
+        self.close()
+        ctr = (C.c_double * 3)(*self.ctr)
+        out = C.c_void_p()
+        rc = lib.ddfmm_session_create(pos.ctypes.data_as(C.POINTER(C.c_double)), pos.shape[0], int(self.kernel),
+                                      self.ACCU, self.NPQ, self.K, ctr, self.ptsmax, self.maxlevel, nc,
+                                      self.mlibptr.ldname.encode(), self.mlibptr.hdname.encode(), self.device,
+                                      C.byref(out))
+        _lib.check(rc)
+        self._s = out
+        self._n = pos.shape[0]
+        return 0
+
+    def _need(self):
+        if self._s is None:
+            raise _lib.DDFMMError(1, "setup() has not been called")
+
+    # src/wave3d_eval.cpp:299-415
+    def eval(self, den, val):
+        self._need()
+        d = np.ascontiguousarray(den, dtype=np.complex128)
+        if d.shape != (self._n,):
+            raise _lib.DDFMMError(1, "den must hold %d complex values" % self._n)
+        if not (isinstance(val, np.ndarray) and val.dtype == np.complex128 and val.shape == (self._n,)
+                and val.flags.c_contiguous):
+            raise _lib.DDFMMError(1, "val must be a contiguous complex128 array of length %d" % self._n)
+        dp = C.POINTER(C.c_double)
+        _lib.check(_lib.load().ddfmm_eval(self._s, d.ctypes.data_as(dp), val.ctypes.data_as(dp)))
+        return 0
+
+    def eval_device(self, den_ptr, val_ptr, stream_ptr=None):
+        """den_ptr / val_ptr: device addresses of N complex128 values."""
+        self._need()
+        _lib.check(_lib.load().ddfmm_eval_device(self._s, C.c_void_p(den_ptr), C.c_void_p(val_ptr),
+                                                 C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def direct(self, den, ids):
+        """FP64 direct sum at the given point ids."""
+        self._need()
+        d = np.ascontiguousarray(den, dtype=np.complex128)
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        out = np.zeros(ids.shape[0], dtype=np.complex128)
+        dp = C.POINTER(C.c_double)
+        _lib.check(_lib.load().ddfmm_direct(self._s, d.ctypes.data_as(dp), ids.ctypes.data_as(C.POINTER(C.c_int)),
+                                            ids.shape[0], out.ctypes.data_as(dp)))
+        return out
+
+    # src/wave3d_check.cpp:22-100: relerr = |direct - fmm| / |fmm| at chkkeys
+    def check(self, den, val, chkkeys):
+        ids = np.asarray(chkkeys, dtype=np.int32)
+        truth = self.direct(den, ids)
+        fmm = np.asarray(val)[ids]
+        return float(np.linalg.norm(truth - fmm) / np.linalg.norm(fmm))
+
+    def stats(self):
+        self._need()
+        st = _lib.ddfmm_stats()
+        _lib.check(_lib.load().ddfmm_session_stats(self._s, C.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if self._s is not None:
+            _lib.load().ddfmm_session_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def from_workload(w, device=0):
+    """Set up a Wave3d for a workloads.Workload (operators created on demand)."""
+    ld, hd = w.operators()
+    mlib = Mlib3d()
+    mlib.kernel = w.kernel
+    mlib.setup({"-mlib3d_ldname": ld, "-mlib3d_hdname": hd, "-mlib3d_NPQ": str(w.npq)})
+    wave = Wave3d(device=device)
+    wave.posptr = w.points()
+    wave.kernel = w.kernel
+    wave.mlibptr = mlib
+    wave.geomprtn = w.nc
+    wave.setup(w.options())
+    return wave

@@ -51,6 +51,8 @@ class Workload:
             return geometry.sphere_points(self.N, self.K, self.seed)
         if self.geometry == "ellipsoid":
             return geometry.ellipsoid_points(self.N, self.K, self.seed)
+        if self.geometry == "cluster":
+            return geometry.cluster_points(self.N, self.K, self.seed)
         raise ValueError("unknown geometry %r" % self.geometry)
 
     def densities(self, dtype=np.complex128) -> np.ndarray:
@@ -82,6 +84,11 @@ def sphere(K, N=None, accu=1, kernel=0, seed=0, ptsmax=100):
 def ellipsoid(K, N, accu=1, kernel=0, seed=0, ptsmax=100):
     return Workload("ellipsoid_K%g_N%d_P%d_k%d" % (K, N, precompute.accu_to_p(accu), kernel),
                     "ellipsoid", float(K), int(N), accu, kernel, ptsmax, 4, seed)
+
+
+def cluster(K, N, accu=1, kernel=0, seed=0, ptsmax=8):
+    return Workload("cluster_K%g_N%d_P%d_k%d_m%d" % (K, N, precompute.accu_to_p(accu), kernel, ptsmax),
+                    "cluster", float(K), int(N), accu, kernel, ptsmax, 4, seed)
 
 
 # the small plain-method case the reference binary runs in seconds

@@ -1,0 +1,105 @@
+/* C ABI of the B200 directional FMM matvec (drop-in for Wave3d::eval).
+ *
+ * The reference's interface for this path is the C++ class Wave3d
+ * (include/wave3d.hpp:219-265 of arbenson/ddfmm):
+ *   wave.posptr() = &pos; wave.kernel() = k; wave.mlibptr() = &mlib;
+ *   wave.geomprtn() = geomprtn;            (src/tt.cpp:134-138)
+ *   wave.setup(opts);                      (src/wave3d_setup.cpp:21-97)
+ *   wave.eval(den, val);                   (src/wave3d_eval.cpp:299-415)
+ *   wave.check(den, val, chk, relerr);     (src/wave3d_check.cpp:22-100)
+ * with Mlib3d::setup reading the ld/hd operator files
+ * (src/mlib3d.cpp:70-103).  Each entry point below replaces one of those
+ * calls; the reference's ParVec<int,...> maps become dense arrays indexed by
+ * point id 0..n-1 (the map's key order).  Complex values are interleaved
+ * (re, im) doubles, i.e. std::complex<double> / cpx.
+ *
+ * All functions return DDFMM_OK (0) or a nonzero status; the reference
+ * throws `new std::exception()` in the same situations
+ * (include/commoninc.hpp:52-53).  ddfmm_last_error() describes the last
+ * failure of the calling thread.  The library owns all device memory; the
+ * caller owns every host array.  A session is used by one host thread at a
+ * time (the reference keeps one active Wave3d per process,
+ * src/wave3d.cpp:21). */
+#ifndef DDFMM_B200_H
+#define DDFMM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    DDFMM_OK = 0,
+    DDFMM_EINVAL = 1,   /* bad argument (reference: CHECK_TRUE failure) */
+    DDFMM_ECUDA = 2,    /* CUDA runtime error or no usable GPU */
+    DDFMM_ESETUP = 3,   /* tree / operator inconsistency, unreadable operator file */
+    DDFMM_ENOMEM = 4
+};
+
+enum { DDFMM_KERNEL_HELM = 0, DDFMM_KERNEL_EXPR = 1 }; /* include/kernel3d.hpp:24-27 */
+
+typedef struct ddfmm_session ddfmm_session;
+
+typedef struct ddfmm_stats {
+    int n_points, n_boxes, n_leaves, n_lf_boxes;
+    long long u_pairs, u_interactions, v_pairs, w_pairs, x_pairs;
+    long long hf_up_nodes, hf_down_nodes, hf_far_pairs, m2l_matrices;
+    long long gemm_launches, kernel_launches;
+    double flops_gemm;          /* 8 real flops per complex multiply-add */
+    long long fft_spectra_bytes;
+    double setup_seconds;
+    long long device_bytes;
+} ddfmm_stats;
+
+/* Wave3d::setup + Mlib3d::setup.  pos3n: n points, x/y/z interleaved, in
+ * wavelengths.  kernel: DDFMM_KERNEL_HELM (exp(ir)/r) or DDFMM_KERNEL_EXPR.
+ * accu, npq, K, ctr, ptsmax, maxlevel: the -wave3d_* options.  ncell:
+ * geomprtn.m(), the cells per edge of the partition tensor (power of two,
+ * K/ncell >= 1).  ld_path / hd_path: operator files in the reference format
+ * (-mlib3d_ldname / -mlib3d_hdname).  device: CUDA ordinal. */
+int ddfmm_session_create(const double* pos3n, int n, int kernel, int accu, int npq, double K,
+                         const double* ctr3, int ptsmax, int maxlevel, int ncell,
+                         const char* ld_path, const char* hd_path, int device,
+                         ddfmm_session** out);
+
+/* Wave3d::eval: val[i] = sum_j G(p_i, p_j) den[j] via the directional FMM.
+ * den, val: host arrays of n complex128 in point-id order.  Unlike the
+ * reference, repeated calls do not accumulate (src/wave3d_eval.cpp:518-521). */
+int ddfmm_eval(ddfmm_session* s, const double* den, double* val);
+
+/* Same, with den / val already in device memory of the session's GPU
+ * (n complex128 each); stream is a cudaStream_t or NULL for the session's
+ * own stream.  Returns after enqueueing; the caller synchronises. */
+int ddfmm_eval_device(ddfmm_session* s, const void* den_dev, void* val_dev, void* stream);
+
+/* Wave3d::check's direct sum: out[k] = sum_j G(p_ids[k], p_j) den[j] in
+ * FP64 over all points (self pair included, r:=1 when r < 1e-8). */
+int ddfmm_direct(ddfmm_session* s, const double* den, const int* ids, int nids, double* out);
+
+int ddfmm_session_stats(const ddfmm_session* s, ddfmm_stats* out);
+
+/* Host-only (no GPU): build the octree and interaction lists of
+ * Wave3d::setup (src/wave3d_setup.cpp:100-299) and report, per level, what
+ * Wave3d::eval prints about them (src/wave3d_eval.cpp:345-372): boxes with
+ * points, and the summed directional far-list sizes; plus the total number
+ * of boxes created and how many are empty.  levels must hold 64 entries;
+ * *nlevels receives the count used. */
+typedef struct ddfmm_tree_level {
+    int level;
+    double width;
+    int boxes;          /* boxes with points */
+    int leaves;         /* terminal boxes with points */
+    long long far_pairs;
+    long long out_dirs; /* (box, outgoing wedge) pairs */
+    long long inc_dirs; /* (box, incoming wedge) pairs */
+    long long u_pairs, v_pairs, w_pairs, x_pairs;
+} ddfmm_tree_level;
+int ddfmm_tree_stats(const double* pos3n, int n, double K, const double* ctr3, int ptsmax, int maxlevel,
+                     int ncell, int npq, int* total_boxes, int* empty_boxes, int* nlevels,
+                     ddfmm_tree_level* levels);
+int ddfmm_session_destroy(ddfmm_session* s);
+const char* ddfmm_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
