@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""Throughput of the directional FMM matvec (Wave3d::eval) on B200.
+
+Workload: the large single instance -- points uniform by area on a sphere of
+diameter K=64 wavelengths (N = 321,699, about 25 per square wavelength),
+kernel exp(ir)/r, P=6 (ACCU 2), NPQ 4, ptsmax 100, complex128 N(0,1)
+densities, seed 0.  One step = one matvec with fresh densities on a fixed
+geometry (setup excluded, reported separately).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own replica of the instance on its GPU
+(independent matvecs, no collective on the data path): weak scaling.
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FMM matvecs/sec & points/sec at stated rel. err vs FP64 direct; p50/p99 latency"
+CAP_FRACTION = 64  # the reference's bounded sample: a 1/64 spherical cap of the same sphere
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="large", choices=["large", "small"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-json", default=None, help="write the per-pass profile here")
+    return ap.parse_args()
+
+
+def workload(name):
+    from ddfmm_b200 import workloads as wl
+    return wl.LARGE if name == "large" else wl.SMALL
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        except OSError:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def fp64_peak_tflops(torch, dev):
+    """Measured FP64 GEMM throughput (cuBLAS DGEMM via torch.matmul) as the
+    denominator of the FP64 roofline; the driver's peak file has no FP64 entry."""
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def reference_sample(w, steps, timeout=600):
+    """Time the reference binary (oracle/_ref/ref_eval, built from the
+    reference's sources) on a bounded sample of the workload: the points of
+    the same sphere inside a 1/CAP_FRACTION spherical cap (z >= z0), same K,
+    P, NPQ, ptsmax and maxlevel.  One eval per process (the reference's eval
+    is not re-entrant).  Returns per-step eval seconds and the sample size."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import run_ref
+    if not run_ref.available():
+        raise RuntimeError("reference binary not built (make -C oracle)")
+    pos, den = w.points(), w.densities()
+    R = np.abs(pos).max()
+    m = pos[:, 2] >= R * (1 - 2.0 / CAP_FRACTION)
+    ld, hd = w.operators()
+    times = []
+    for _ in range(steps):
+        r = run_ref.run(pos[m], den[m], K=w.K, accu=w.accu, kernel=w.kernel, nc=w.nc, maxlevel=w.maxlevel,
+                        ld_path=ld, hd_path=hd, ptsmax=w.ptsmax, npq=w.npq, timeout=timeout)
+        times.append(r["eval_s"])
+    return times, int(m.sum())
+
+
+def sample_desc(ns, w):
+    return ("reference Wave3d::eval (oracle/_ref, built from the reference sources; 1 process, 1 core: the "
+            "reference has no threads and no MPI is installed) on the points of the same K=%g sphere inside a "
+            "1/%d spherical cap (N_s=%d of %d, same P/NPQ/ptsmax/maxlevel), scaled to the full workload by point "
+            "count; the full workload costs more per point (longer far-field lists), so this favours the "
+            "reference" % (w.K, CAP_FRACTION, ns, w.N))
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    w = workload(args.workload)
+    times, ns = reference_sample(w, args.warmup + args.steps)
+    t = times[args.warmup:] if len(times) > args.warmup else times
+    sec = float(np.median(t))
+    mv = (ns / w.N) / sec  # full-workload matvecs per second at the sample's cost per point
+    line = {"metric": METRIC, "impl": "reference", "value": mv, "unit": "matvec/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec * w.N / ns,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic", "points_per_sec": mv * w.N,
+            "config": {"workload": w.name, "geometry": w.geometry, "K": w.K, "N": w.N, "P": w.P,
+                       "kernel": "exp(ir)/r", "npq": w.npq, "ptsmax": w.ptsmax},
+            "cpu_baseline": {"value": mv, "unit": "matvec/s", "cores": 1, "kind": "reference",
+                             "sample": sample_desc(ns, w)},
+            "e2e": {"value": mv, "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    from ddfmm_b200 import wave3d
+    w = workload(args.workload)
+    w.operators()
+    t0 = time.perf_counter()
+    wave = wave3d.from_workload(w, device=local)
+    setup_s = time.perf_counter() - t0
+    st = wave.stats()
+    den = w.densities()
+    chk = w.check_ids()
+    # device-resident inputs (value) -----------------------------------------
+    rng = np.random.default_rng(1 + rank)
+    n_inputs = 4  # fresh densities per step, cycled
+    dens = [den] + [(rng.standard_normal(w.N) + 1j * rng.standard_normal(w.N)) for _ in range(n_inputs - 1)]
+    den_d = [torch.from_numpy(np.ascontiguousarray(d).view(np.float64)).to(dev) for d in dens]
+    val_d = torch.empty(2 * w.N, dtype=torch.float64, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+    for i in range(args.warmup):
+        wave.eval_device(den_d[i % n_inputs].data_ptr(), val_d.data_ptr(), sp)
+    stream.synchronize()
+    # accuracy of this path against the FP64 direct sum at 200 targets
+    wave.eval_device(den_d[0].data_ptr(), val_d.data_ptr(), sp)
+    stream.synchronize()
+    val0 = val_d.cpu().numpy().view(np.complex128)
+    relerr = wave.check(den, val0, chk)
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    wave.profile(True)
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                ev[i][0].record(stream)
+            wave.eval_device(den_d[i % n_inputs].data_ptr(), val_d.data_ptr(), sp)
+            with torch.cuda.stream(stream):
+                ev[i][1].record(stream)
+        stream.synchronize()
+    prof = wave.profile_read(reset=True)
+    wave.profile(False)
+    torch.cuda.synchronize(dev)
+    if ws > 1:
+        torch.distributed.barrier()
+    lat = np.array([a.elapsed_time(b) for a, b in ev])
+    total_ms = ev[0][0].elapsed_time(ev[-1][1])
+    ms_per_step = total_ms / args.steps
+    if ws > 1:
+        t = torch.tensor([ms_per_step], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_per_step = float(t.item())
+    value = ws * 1e3 / ms_per_step  # whole-job matvecs / s (every rank runs its own instance)
+    # end to end through the public API with pinned host buffers ---------------
+    den_h = torch.from_numpy(np.ascontiguousarray(den).view(np.float64)).pin_memory()
+    val_h = torch.empty(2 * w.N, dtype=torch.float64).pin_memory()
+    dh = den_h.numpy().view(np.complex128)
+    vh = val_h.numpy().view(np.complex128)
+    wave.eval(dh, vh)
+    e2e_steps = max(1, min(args.steps, 5))
+    if ws > 1:
+        torch.distributed.barrier()
+    t1 = time.perf_counter()
+    for _ in range(e2e_steps):
+        wave.eval(dh, vh)
+    e2e_s = (time.perf_counter() - t1) / e2e_steps
+    if ws > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_relerr = float(np.linalg.norm(vh - val0) / np.linalg.norm(val0))
+    # roofline of the dominant kernel -------------------------------------------
+    by_kernel = {}
+    for lab, e in prof.items():
+        k = by_kernel.setdefault(e["kernel"], dict(ms=0.0, launches=0, flops=0.0, bytes=0.0))
+        for f in ("ms", "launches", "flops", "bytes"):
+            k[f] += e[f]
+    dom = max(by_kernel, key=lambda k: by_kernel[k]["ms"])
+    dk = by_kernel[dom]
+    peaks = measured_peaks()
+    if dom in ("zgemm_kernel", "pt_kernel"):
+        peak = fp64_peak_tflops(torch, dev)
+        achieved = dk["flops"] / (dk["ms"] * 1e-3) / 1e12
+        roof = {"bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None,
+                "peak_source": "measured cuBLAS DGEMM 4096^3 on this GPU (FP64 has no entry in MEASURED_PEAKS.json)",
+                "launches": dk["launches"]}
+    else:
+        peak = peaks.get("hbm_gbs", 6650.0)
+        achieved = dk["bytes"] / (dk["ms"] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+                "launches": dk["launches"]}
+    passes = {lab: {"ms_per_step": e["ms"] / args.steps, "launches_per_step": e["launches"] / args.steps,
+                    "gflop_per_step": e["flops"] / args.steps / 1e9, "kernel": e["kernel"]}
+              for lab, e in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])}
+    launches = sum(e["launches"] for lab, e in prof.items() if e["kernel"] != "memset") + 2 * args.steps
+    clocks = clk.summary()
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "large":
+        try:
+            times, ns = reference_sample(w, 1)
+            mv = (ns / w.N) / times[0]
+            cpu = {"value": mv, "unit": "matvec/s", "cores": 1, "kind": "reference", "sample": sample_desc(ns, w)}
+        except Exception as ex:  # the reference binary travels with the tree; report when it does not
+            cpu = {"value": None, "unit": "matvec/s", "cores": 1, "kind": "reference", "sample": "unavailable: %s" % ex}
+    if args.profile_json and rank == 0:
+        json.dump({"passes": passes, "by_kernel": by_kernel, "stats": st}, open(args.profile_json, "w"), indent=1)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+                "points_per_sec": value * w.N, "relerr_vs_fp64_direct": relerr,
+                "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+                "config": {"workload": w.name, "geometry": w.geometry, "K": w.K, "N": w.N, "P": w.P,
+                           "kernel": "exp(ir)/r", "npq": w.npq, "ptsmax": w.ptsmax, "form": "plain FP64",
+                           "l2": "inputs larger than L2 (device working set %.1f GB)" % (st["device_bytes"] / 1e9),
+                           "parallelism": "replicas" if ws > 1 else "single GPU", "setup_s": setup_s},
+                "e2e": {"value": 1.0 / e2e_s, "unit": "matvec/s", "h2d_bytes_per_step": 16 * w.N,
+                        "d2h_bytes_per_step": 16 * w.N, "rel_diff_vs_device_path": e2e_relerr},
+                "roofline": roof, "gpu_launches": int(round(launches / args.steps)) * args.steps,
+                "clocks": clocks, "cpu_baseline": cpu, "passes": passes}
+        print(json.dumps(line), flush=True)
+    wave.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

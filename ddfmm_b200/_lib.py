@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libddfmm_b200.so")
 EXPORTS = (
     "ddfmm_session_create", "ddfmm_eval", "ddfmm_eval_device", "ddfmm_direct",
     "ddfmm_session_stats", "ddfmm_session_destroy", "ddfmm_last_error", "ddfmm_tree_stats",
+    "ddfmm_profile_enable", "ddfmm_profile_read",
 )
 
 
@@ -37,6 +38,11 @@ class ddfmm_tree_level(C.Structure):
                 ("far_pairs", C.c_longlong), ("out_dirs", C.c_longlong), ("inc_dirs", C.c_longlong),
                 ("u_pairs", C.c_longlong), ("v_pairs", C.c_longlong), ("w_pairs", C.c_longlong),
                 ("x_pairs", C.c_longlong)]
+
+
+class ddfmm_profile_entry(C.Structure):
+    _fields_ = [("label", C.c_char * 32), ("kernel", C.c_char * 32), ("launches", C.c_int), ("ms", C.c_double),
+                ("flops", C.c_double), ("bytes", C.c_double)]
 
 
 _lib = None
@@ -69,6 +75,11 @@ def load():
                                      C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(ddfmm_tree_level)]
     lib.ddfmm_tree_stats.restype = C.c_int
+    lib.ddfmm_profile_enable.argtypes = [C.c_void_p, C.c_int]
+    lib.ddfmm_profile_enable.restype = C.c_int
+    lib.ddfmm_profile_read.argtypes = [C.c_void_p, C.POINTER(ddfmm_profile_entry), C.c_int, C.POINTER(C.c_int),
+                                       C.c_int]
+    lib.ddfmm_profile_read.restype = C.c_int
     lib.ddfmm_last_error.argtypes = []
     lib.ddfmm_last_error.restype = C.c_char_p
     _lib = lib

@@ -183,6 +183,32 @@ int ddfmm_tree_stats(const double* pos3n, int n, double K, const double* ctr3, i
     });
 }
 
+int ddfmm_profile_enable(ddfmm_session* s, int on) {
+    if (!s || !s->impl) return fail(DDFMM_EINVAL, "NULL session");
+    return guarded([&] { s->impl->profile_enable(on != 0); });
+}
+
+int ddfmm_profile_read(ddfmm_session* s, ddfmm_profile_entry* out, int max_entries, int* n_entries, int reset) {
+    if (!s || !s->impl || !n_entries || (max_entries > 0 && !out)) return fail(DDFMM_EINVAL, "bad profile arguments");
+    return guarded([&] {
+        auto v = s->impl->profile_read();
+        int n = 0;
+        for (auto& e : v) {
+            if (n >= max_entries) break;
+            ddfmm_profile_entry& o = out[n++];
+            std::memset(&o, 0, sizeof(o));
+            std::strncpy(o.label, e.label.c_str(), sizeof(o.label) - 1);
+            std::strncpy(o.kernel, e.kernel.c_str(), sizeof(o.kernel) - 1);
+            o.launches = e.launches;
+            o.ms = e.ms;
+            o.flops = e.flops;
+            o.bytes = e.bytes;
+        }
+        *n_entries = n;
+        if (reset) s->impl->profile_reset();
+    });
+}
+
 int ddfmm_session_destroy(ddfmm_session* s) {
     if (!s) return DDFMM_OK;
     int rc = guarded([&] { delete s->impl; });

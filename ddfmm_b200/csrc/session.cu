@@ -71,12 +71,15 @@ Session::Session(const double* pos3n, int n, const SessionParams& p, const std::
 
 Session::~Session() {
     if (stream_) cudaStreamSynchronize(stream_);
+    for (cudaEvent_t e : ev_) cudaEventDestroy(e);
     for (void* p : allocs_) cudaFree(p);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
 void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<long long> >& xo,
-                       std::vector<std::vector<long long> >& yo, const double2* X, double2* Y, int mode) {
+                       std::vector<std::vector<long long> >& yo, const double2* X, double2* Y, int mode,
+                       const char* label) {
+    double flops = 0, bytes = 0;
     std::vector<GemmProblem> P;
     std::vector<GemmTile> tiles;
     std::vector<long long> xs, ys;
@@ -91,11 +94,17 @@ void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<
         ys.insert(ys.end(), yo[i].begin(), yo[i].end());
         for (int r0 = 0; r0 < q.m; r0 += 64)
             for (int c0 = 0; c0 < q.ncol; c0 += 32) tiles.push_back(GemmTile{pid, r0, c0, 0});
-        stats_.flops_gemm += 8.0 * q.m * q.k * (double)q.ncol;
+        flops += 8.0 * q.m * q.k * (double)q.ncol;
+        // operator once, each input and output column once (read-modify-write for += modes)
+        bytes += 16.0 * ((double)q.m * q.k + (double)q.k * q.ncol + (mode == GEMM_SET ? 1.0 : 2.0) * q.m * q.ncol);
     }
+    stats_.flops_gemm += flops;
     if (tiles.empty()) return;
     Step st{};
     st.kind = 0;
+    st.label = label;
+    st.flops = flops;
+    st.bytes = bytes;
     st.g.probs = upload(P);
     st.g.tiles = upload(tiles);
     st.g.xoff = upload(xs);
@@ -108,10 +117,18 @@ void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<
     stats_.gemm_launches++;
 }
 
-void Session::add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>& srcs) {
+void Session::add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>& srcs, const char* label) {
     if (items.empty()) return;
     Step st{};
     st.kind = 1;
+    st.label = label;
+    for (const PtItem& it : items) {
+        long long ns = 0;
+        for (int k = it.src_begin; k < it.src_end; ++k) ns += srcs[k].src.n;
+        // one kernel evaluation (sqrt, reciprocal, sincospi) + one complex MAC per pair
+        st.flops += 20.0 * it.trg.n * (double)ns;
+        st.bytes += 40.0 * ns + 56.0 * it.trg.n;
+    }
     st.pt.items = upload(items);
     st.pt.srcs = upload(srcs);
     st.pt.nitems = (int)items.size();
@@ -571,10 +588,10 @@ void Session::build() {
     };
     auto leaf_set = [&](int l) { return lf_set(d_pos_sorted_ + 3 * (size_t)leaf_off[l], leaf_cnt[l], zero3, 1.0); };
     auto single = [&](const GemmProblem& p, const std::vector<long long>& x, const std::vector<long long>& y,
-                      const double2* X, double2* Y, int mode) {
+                      const double2* X, double2* Y, int mode, const char* label) {
         std::vector<GemmProblem> ps(1, p);
         std::vector<std::vector<long long> > xo(1, x), yo(1, y);
-        add_gemm(ps, xo, yo, X, Y, mode);
+        add_gemm(ps, xo, yo, X, Y, mode, label);
     };
     for (auto it = lflevels.rbegin(); it != lflevels.rend(); ++it) {
         const LfLevelOps& L = lfops[it->first];
@@ -593,7 +610,7 @@ void Session::build() {
             itm.src_end = (int)srcs.size();
             items.push_back(itm);
         }
-        add_pt(items, srcs);
+        add_pt(items, srcs, "lf_s2m");
         // M2M from children (src/wave3d_eval.cpp:452-463)
         if (L.has_children)
             for (int ind = 0; ind < 8; ++ind) {
@@ -606,7 +623,7 @@ void Session::build() {
                     x.push_back((long long)lfidx[c] * nE);
                     y.push_back((long long)l * nE);
                 }
-                single(GemmProblem{L.ue2uc[ind], nE, nE, nE, 0, 0}, x, y, lf_upeq, lf_upchk, GEMM_ADD);
+                single(GemmProblem{L.ue2uc[ind], nE, nE, nE, 0, 0}, x, y, lf_upeq, lf_upchk, GEMM_ADD, "lf_m2m");
             }
         // upeqnden = v * (1/sigma .* (U^H * upchk))   (src/wave3d_eval.cpp:466-478)
         std::vector<long long> a, b2;
@@ -614,18 +631,20 @@ void Session::build() {
             a.push_back((long long)l * nE);
             b2.push_back((long long)l * nE);
         }
-        single(GemmProblem{L.up_s, L.r, nE, L.r, 0, 0}, a, b2, lf_upchk, lf_mid, GEMM_SET);
-        single(GemmProblem{L.v, nE, L.r, nE, 0, 0}, a, b2, lf_mid, lf_upeq, GEMM_SET);
+        single(GemmProblem{L.up_s, L.r, nE, L.r, 0, 0}, a, b2, lf_upchk, lf_mid, GEMM_SET, "lf_uc2ue");
+        single(GemmProblem{L.v, nE, L.r, nE, 0, 0}, a, b2, lf_mid, lf_upeq, GEMM_SET, "lf_uc2ue");
     }
 
     // ---------------------------------------------------------------- steps: HF upward
-    for (auto& kv : hflevels) {
-        int level = kv.first;
+    // widths ascending = levels descending
+    for (auto hit = hflevels.rbegin(); hit != hflevels.rend(); ++hit) {
+        int level = hit->first;
         double W = T.width(level);
         auto ur = uprange[level];
         if (ur.first == ur.second) continue;
         Step ms{};
         ms.kind = 4;
+        ms.label = "memset";
         ms.ms = Memset{T0, sizeof(double2) * (size_t)tmp_max};
         steps_.push_back(ms);
         // M2M: upchk = sum_children ue2uc(abc) * child's upeqnden (src/wave3d_eval.cpp:796-834)
@@ -660,7 +679,7 @@ void Session::build() {
                 xo[p].push_back(xoff);
                 yo[p].push_back(u.toff);
             }
-            add_gemm(probs, xo, yo, W == 1.0 ? lf_upeq : hf_upeq, T0, GEMM_ADD);
+            add_gemm(probs, xo, yo, W == 1.0 ? lf_upeq : hf_upeq, T0, GEMM_ADD, "hf_m2m");
         }
         // upeqnden = E1 * (E2 * (E3 * upchk))   (src/wave3d_eval.cpp:837-849)
         std::map<int, int> cp;
@@ -685,13 +704,14 @@ void Session::build() {
             xa[p].push_back(u.toff);
             ya[p].push_back(u.off);
         }
-        add_gemm(p3, xa, xa, T0, T1, GEMM_SET);
-        add_gemm(p2, xa, xa, T1, T2, GEMM_SET);
-        add_gemm(p1, xa, ya, T2, hf_upeq, GEMM_SET);
+        add_gemm(p3, xa, xa, T0, T1, GEMM_SET, "hf_uc2ue");
+        add_gemm(p2, xa, xa, T1, T2, GEMM_SET, "hf_uc2ue");
+        add_gemm(p1, xa, ya, T2, hf_upeq, GEMM_SET, "hf_uc2ue");
     }
 
     // ---------------------------------------------------------------- steps: HF downward
-    for (auto it = hflevels.rbegin(); it != hflevels.rend(); ++it) {
+    // widths descending = levels ascending
+    for (auto it = hflevels.begin(); it != hflevels.end(); ++it) {
         int level = it->first;
         double W = T.width(level);
         auto dr = dnrange[level];
@@ -703,7 +723,7 @@ void Session::build() {
                 const M2LMat& M = m2l_mats[gid];
                 probs.push_back(GemmProblem{M.A, M.r1, M.r1, M.r1, 0, 0});
             }
-            add_gemm(probs, m2l_x[level], m2l_y[level], hf_upeq, hf_dnchk, GEMM_ATOMIC);
+            add_gemm(probs, m2l_x[level], m2l_y[level], hf_upeq, hf_dnchk, GEMM_ATOMIC, "hf_m2l");
         }
         // dneqnden = E3^T (E2^T (E1^T dnchk))   (src/wave3d_eval.cpp:938-948, src/mlib3d.cpp:246-250)
         std::map<int, int> cp;
@@ -728,9 +748,9 @@ void Session::build() {
             xa[p].push_back(d.off);
             xt[p].push_back(d.toff);
         }
-        add_gemm(p1, xa, xt, hf_dnchk, T0, GEMM_SET);
-        add_gemm(p2, xt, xt, T0, T1, GEMM_SET);
-        add_gemm(p3, xt, xt, T1, T2, GEMM_SET);
+        add_gemm(p1, xa, xt, hf_dnchk, T0, GEMM_SET, "hf_dc2de");
+        add_gemm(p2, xt, xt, T0, T1, GEMM_SET, "hf_dc2de");
+        add_gemm(p3, xt, xt, T1, T2, GEMM_SET, "hf_dc2de");
         // L2L into the children's (pdir) check values, or LF dnchkval at W=1 (src/wave3d_eval.cpp:950-991)
         for (int ind = 0; ind < 8; ++ind) {
             std::map<Idx3, int> pid;
@@ -763,7 +783,7 @@ void Session::build() {
                 xo[p].push_back(d.toff);
                 yo[p].push_back(yoff);
             }
-            add_gemm(probs, xo, yo, T2, W == 1.0 ? lf_dnchk : hf_dnchk, GEMM_ATOMIC);
+            add_gemm(probs, xo, yo, T2, W == 1.0 ? lf_dnchk : hf_dnchk, GEMM_ATOMIC, "hf_l2l");
         }
     }
 
@@ -800,6 +820,9 @@ void Session::build() {
                 VlistLevel VL{G, P, nE, L.grid_idx, L.tns, d_twf, d_twb};
                 Step f{};
                 f.kind = 2;
+                f.label = "lf_vlist_fft";
+                f.flops = 8.0 * 3 * (double)G3 * G * srcb.size();
+                f.bytes = 16.0 * ((double)nE + G3) * srcb.size();
                 f.v.L = VL;
                 f.v.src_boxes = upload(srcb);
                 f.v.nsrc = (int)srcb.size();
@@ -808,6 +831,10 @@ void Session::build() {
                 steps_.push_back(f);
                 Step a{};
                 a.kind = 3;
+                a.label = "lf_vlist_m2l";
+                a.flops = 8.0 * (double)G3 * vsrc.size() + 8.0 * 3 * (double)G3 * G * trg.size();
+                // compulsory: each source spectrum, the 316 tensors, each target's check values
+                a.bytes = 16.0 * ((double)G3 * srcb.size() + 316.0 * G3 + 2.0 * nE * trg.size());
                 a.v.L = VL;
                 a.v.trg = upload(trg);
                 a.v.vptr = upload(vptr);
@@ -840,8 +867,8 @@ void Session::build() {
                 itm.src_end = (int)S.size();
                 (direct ? itemsA : itemsB).push_back(itm);
             }
-            add_pt(itemsA, srcsA);
-            add_pt(itemsB, srcsB);
+            add_pt(itemsA, srcsA, "lf_xlist");
+            add_pt(itemsB, srcsB, "lf_xlist");
         }
         // U list (src/wave3d_eval.cpp:585-600) and W list (:688-718) into extval
         {
@@ -883,14 +910,14 @@ void Session::build() {
                     witems.push_back(itm);
                 }
             }
-            add_pt(items, srcs);
-            add_pt(witems, wsrcs);
+            add_pt(items, srcs, "lf_ulist");
+            add_pt(witems, wsrcs, "lf_wlist");
         }
         // dneqnden = up^T (1/sigma .* (v^T dnchk))   (src/wave3d_eval.cpp:536-547, src/mlib3d.cpp:147-152)
         std::vector<long long> a;
         for (int l : ids) a.push_back((long long)l * nE);
-        single(GemmProblem{L.vT_s, L.r, nE, L.r, 0, 0}, a, a, lf_dnchk, lf_mid, GEMM_SET);
-        single(GemmProblem{L.upT, nE, L.r, nE, 0, 0}, a, a, lf_mid, lf_dneq, GEMM_SET);
+        single(GemmProblem{L.vT_s, L.r, nE, L.r, 0, 0}, a, a, lf_dnchk, lf_mid, GEMM_SET, "lf_dc2de");
+        single(GemmProblem{L.upT, nE, L.r, nE, 0, 0}, a, a, lf_mid, lf_dneq, GEMM_SET, "lf_dc2de");
         // L2T at leaves (src/wave3d_eval.cpp:550-560)
         {
             std::vector<PtItem> items;
@@ -906,7 +933,7 @@ void Session::build() {
                 itm.src_end = (int)srcs.size();
                 items.push_back(itm);
             }
-            add_pt(items, srcs);
+            add_pt(items, srcs, "lf_l2t");
         }
         // L2L to the children (src/wave3d_eval.cpp:562-579)
         if (L.has_children)
@@ -920,15 +947,33 @@ void Session::build() {
                     x.push_back((long long)l * nE);
                     y.push_back((long long)lfidx[c] * nE);
                 }
-                single(GemmProblem{L.de2dc[ind], nE, nE, nE, 0, 0}, x, y, lf_dneq, lf_dnchk, GEMM_ADD);
+                single(GemmProblem{L.de2dc[ind], nE, nE, nE, 0, 0}, x, y, lf_dneq, lf_dnchk, GEMM_ADD, "lf_l2l");
             }
     }
     stats_.kernel_launches = (long long)steps_.size() + 2;
 }
 
+static const char* kernel_name(int kind) {
+    switch (kind) {
+        case 0: return "zgemm_kernel";
+        case 1: return "pt_kernel";
+        case 2: return "vlist_forward_kernel";
+        case 3: return "vlist_accum_kernel";
+        default: return "memset";
+    }
+}
+
 void Session::run_steps(cudaStream_t s) {
     for (const Memset& m : zero_at_start_) CK(cudaMemsetAsync(m.p, 0, m.bytes, s));
-    for (const Step& st : steps_) {
+    if (profiling_ && ev_.size() < 2 * steps_.size()) {
+        size_t have = ev_.size();
+        ev_.resize(2 * steps_.size());
+        for (size_t i = have; i < ev_.size(); ++i) CK(cudaEventCreate(&ev_[i]));
+    }
+    if (profiling_ && !ev_pending_.empty()) profile_read();  // keep one eval of events in flight at most
+    for (size_t i = 0; i < steps_.size(); ++i) {
+        const Step& st = steps_[i];
+        if (profiling_) CK(cudaEventRecord(ev_[2 * i], s));
         switch (st.kind) {
             case 0:
                 launch_gemm(st.g.probs, st.g.tiles, st.g.ntiles, st.g.xoff, st.g.yoff, st.g.X, st.g.Y, st.g.mode, s);
@@ -947,7 +992,36 @@ void Session::run_steps(cudaStream_t s) {
                 CK(cudaMemsetAsync(st.ms.p, 0, st.ms.bytes, s));
                 break;
         }
+        if (profiling_) {
+            CK(cudaEventRecord(ev_[2 * i + 1], s));
+            ev_pending_.push_back(std::make_pair((int)i, (int)(2 * i)));
+        }
     }
+}
+
+void Session::profile_enable(bool on) {
+    if (!on && !ev_pending_.empty()) profile_read();
+    profiling_ = on;
+}
+
+std::vector<Session::ProfileEntry> Session::profile_read() {
+    for (auto& pe : ev_pending_) {
+        CK(cudaEventSynchronize(ev_[pe.second + 1]));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev_[pe.second], ev_[pe.second + 1]));
+        const Step& st = steps_[pe.first];
+        ProfileEntry& e = prof_[st.label];
+        e.label = st.label;
+        e.kernel = kernel_name(st.kind);
+        e.launches += 1;
+        e.ms += ms;
+        e.flops += st.flops;
+        e.bytes += st.bytes;
+    }
+    ev_pending_.clear();
+    std::vector<ProfileEntry> out;
+    for (auto& kv : prof_) out.push_back(kv.second);
+    return out;
 }
 
 void Session::eval_device(const double2* den, double2* val, cudaStream_t s) {

@@ -48,6 +48,16 @@ public:
     void direct_host(const std::complex<double>* den, const int* ids, int nids, std::complex<double>* out);
 
     const SessionStats& stats() const { return stats_; }
+
+    struct ProfileEntry {
+        std::string label, kernel;
+        int launches = 0;
+        double ms = 0, flops = 0, bytes = 0;
+    };
+    // Event-timed per-step profile of subsequent evals (on their stream).
+    void profile_enable(bool on);
+    std::vector<ProfileEntry> profile_read();
+    void profile_reset() { prof_.clear(); }
     int npts() const { return npts_; }
     cudaStream_t stream() const { return stream_; }
 
@@ -87,6 +97,9 @@ private:
     // one step of the eval: exactly one of these is used
     struct Step {
         int kind;  // 0 gemm, 1 pt, 2 vfwd, 3 vacc, 4 memset
+        const char* label;  // pass name for profiling
+        double flops;       // algorithmic flops of the launch
+        double bytes;       // algorithmic DRAM bytes of the launch
         GemmLaunch g;
         PtLaunch pt;
         VLaunch v;
@@ -98,8 +111,9 @@ private:
     template <class T>
     T* upload(const std::vector<T>& v);
     void add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<long long> >& xo,
-                  std::vector<std::vector<long long> >& yo, const double2* X, double2* Y, int mode);
-    void add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>& srcs);
+                  std::vector<std::vector<long long> >& yo, const double2* X, double2* Y, int mode,
+                  const char* label);
+    void add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>& srcs, const char* label);
     void build();
     void run_steps(cudaStream_t s);
 
@@ -122,6 +136,10 @@ private:
     double2* d_den_io_ = nullptr;
     double2* d_val_io_ = nullptr;
     std::vector<Memset> zero_at_start_;
+    bool profiling_ = false;
+    std::vector<cudaEvent_t> ev_;
+    std::vector<std::pair<int, int> > ev_pending_;  // (step, event index) recorded, not yet read
+    std::map<std::string, ProfileEntry> prof_;
 };
 
 }  // namespace ddfmm

@@ -146,6 +146,19 @@ class Wave3d:
         _lib.check(_lib.load().ddfmm_session_stats(self._s, C.byref(st)))
         return st.as_dict()
 
+    def profile(self, on=True):
+        self._need()
+        _lib.check(_lib.load().ddfmm_profile_enable(self._s, 1 if on else 0))
+
+    def profile_read(self, reset=True):
+        """Per-pass totals since the last reset: {label: dict(kernel, launches, ms, flops, bytes)}."""
+        self._need()
+        arr = (_lib.ddfmm_profile_entry * 64)()
+        n = C.c_int()
+        _lib.check(_lib.load().ddfmm_profile_read(self._s, arr, 64, C.byref(n), 1 if reset else 0))
+        return {arr[i].label.decode(): dict(kernel=arr[i].kernel.decode(), launches=arr[i].launches, ms=arr[i].ms,
+                                            flops=arr[i].flops, bytes=arr[i].bytes) for i in range(n.value)}
+
     def close(self):
         if self._s is not None:
             _lib.load().ddfmm_session_destroy(self._s)

@@ -96,6 +96,23 @@ typedef struct ddfmm_tree_level {
 int ddfmm_tree_stats(const double* pos3n, int n, double K, const double* ctr3, int ptsmax, int maxlevel,
                      int ncell, int npq, int* total_boxes, int* empty_boxes, int* nlevels,
                      ddfmm_tree_level* levels);
+/* Per-pass profile: while enabled, every launch of ddfmm_eval* is bracketed
+ * by CUDA events on its stream.  ddfmm_profile_read returns the totals
+ * accumulated since the last reset (one entry per pass label), with the
+ * algorithmic flops and DRAM bytes of those launches.  The reference's
+ * counterpart is the per-pass wall time it prints (src/wave3d_eval.cpp:59-66). */
+typedef struct ddfmm_profile_entry {
+    char label[32];
+    char kernel[32];
+    int launches;
+    double ms;
+    double flops;
+    double bytes;
+} ddfmm_profile_entry;
+int ddfmm_profile_enable(ddfmm_session* s, int on);
+int ddfmm_profile_read(ddfmm_session* s, ddfmm_profile_entry* out, int max_entries, int* n_entries,
+                       int reset);
+
 int ddfmm_session_destroy(ddfmm_session* s);
 const char* ddfmm_last_error(void);
 
