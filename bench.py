@@ -39,7 +39,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="large", choices=["large", "small"])
+    ap.add_argument("--workload", default="large", choices=["large", "medium", "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-json", default=None, help="write the per-pass profile here")
     return ap.parse_args()
@@ -47,7 +47,7 @@ def parse():
 
 def workload(name):
     from ddfmm_b200 import workloads as wl
-    return wl.LARGE if name == "large" else wl.SMALL
+    return {"large": wl.LARGE, "medium": wl.MEDIUM, "small": wl.SMALL}[name]
 
 
 def dist_env():

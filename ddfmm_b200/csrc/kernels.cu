@@ -56,69 +56,94 @@ void launch_kmat(const KmatJob* jobs, int njobs, long long total, int kernel, cu
 }
 
 // ---------------------------------------------------------------- gemm
-// 64 x 32 complex output tile per 256-thread block; thread (tx, ty) owns
-// rows tx + 16*i (i < 4) and columns ty + 16*j (j < 2), so consecutive lanes
-// write consecutive rows of one output vector.
-constexpr int BM = 64, BN = 32, BK = 8;
+// Grouped complex FP64 GEMM with gathered input columns and scattered output
+// columns.  A 256-thread block computes up to 64 rows x 64 columns: thread
+// (tx, ty) owns rows tx + 16*i (i < MT) and columns ty + 16*j (j < 4), so
+// consecutive lanes write consecutive rows of one output vector.  MT =
+// ceil(tile rows / 16) is a compile-time specialisation chosen per tile, so
+// an 80-150-row translation operator wastes at most 15 rows and the inner
+// loop carries no guards.  K is consumed in slices of 16 through a 3-stage
+// cp.async pipeline; rows, columns and k beyond the problem are zero-filled
+// by the copy (src-size 0).
+constexpr int BM = 64, BN = 64, BK = 16, GSTAGES = 3;
+constexpr int GEMM_SMEM = GSTAGES * (BK * BM + BK * BN) * (int)sizeof(double2);
 
-__global__ void __launch_bounds__(256) zgemm_kernel(const GemmProblem* __restrict__ probs,
-                                                    const GemmTile* __restrict__ tiles,
-                                                    const long long* __restrict__ xoff,
-                                                    const long long* __restrict__ yoff,
-                                                    const double2* __restrict__ X, double2* Y, int mode) {
-    __shared__ double2 As[BK][BM];
-    __shared__ double2 Xs[BK][BN];
-    __shared__ long long xo[BN], yo[BN];
-    const GemmTile t = tiles[blockIdx.x];
-    const GemmProblem p = probs[t.prob];
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <int MT>
+__device__ __forceinline__ void zgemm_tile(const GemmProblem& p, const GemmTile& t, int ncol, int rows,
+                                           const long long* xo, const long long* yo, const double2* __restrict__ X,
+                                           double2* Y, int mode, double2* gsm) {
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    const int ncol = min(BN, p.ncol - t.col0);
-    if (tid < BN) {
-        xo[tid] = tid < ncol ? xoff[p.col0 + t.col0 + tid] : 0;
-        yo[tid] = tid < ncol ? yoff[p.col0 + t.col0 + tid] : 0;
+    auto load = [&](int stage, int k0) {
+        double2* As = gsm + stage * (BK * (BM + BN));
+        double2* Xs = As + BK * BM;
+#pragma unroll
+        for (int q = 0; q < MT; ++q) {  // BK x (16*MT) elements of A, MT per thread
+            int e = tid + 256 * q, row = e % (16 * MT), kk = e / (16 * MT);
+            int gk = k0 + kk;
+            bool ok = row < rows && gk < p.k;
+            cp_async16(&As[kk * BM + row], ok ? (const void*)(p.A + (size_t)gk * p.lda + t.row0 + row) : (const void*)p.A,
+                       ok ? 16 : 0);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            int e = tid + 256 * q, kk = e & 15, col = e >> 4;
+            int gk = k0 + kk;
+            bool ok = col < ncol && gk < p.k;
+            cp_async16(&Xs[col * BK + kk], ok ? (const void*)(X + xo[col] + gk) : (const void*)X, ok ? 16 : 0);
+        }
+    };
+    double2 acc[MT][4];
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
+    const int nk = (p.k + BK - 1) / BK;
+#pragma unroll
+    for (int s = 0; s < GSTAGES - 1; ++s) {
+        if (s < nk) load(s, s * BK);
+        cp_async_commit();
     }
-    __syncthreads();
-    double2 acc[4][2];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) acc[i][j] = make_double2(0.0, 0.0);
-    const double2 z = make_double2(0.0, 0.0);
-    for (int k0 = 0; k0 < p.k; k0 += BK) {
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            int e = tid + 256 * q, row = e & 63, kk = e >> 6;
-            int gr = t.row0 + row, gk = k0 + kk;
-            As[kk][row] = (gr < p.m && gk < p.k) ? p.A[(size_t)gk * p.lda + gr] : z;
-        }
-        {
-            int col = tid >> 3, kk = tid & 7, gk = k0 + kk;
-            Xs[kk][col] = (col < ncol && gk < p.k) ? X[xo[col] + gk] : z;
-        }
+    for (int it = 0; it < nk; ++it) {
+        cp_async_wait<GSTAGES - 2>();
         __syncthreads();
+        {
+            int nx = it + GSTAGES - 1;
+            if (nx < nk) load(nx % GSTAGES, nx * BK);
+            cp_async_commit();
+        }
+        const double2* As = gsm + (it % GSTAGES) * (BK * (BM + BN));
+        const double2* Xs = As + BK * BM;
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
-            double2 a[4], x[2];
+            double2 a[MT], x[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
+            for (int i = 0; i < MT; ++i) a[i] = As[kk * BM + tx + 16 * i];
 #pragma unroll
-            for (int j = 0; j < 2; ++j) x[j] = Xs[kk][ty + 16 * j];
+            for (int j = 0; j < 4; ++j) x[j] = Xs[(ty + 16 * j) * BK + kk];
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < MT; ++i)
 #pragma unroll
-                for (int j = 0; j < 2; ++j) cfma(acc[i][j], a[i], x[j]);
+                for (int j = 0; j < 4; ++j) cfma(acc[i][j], a[i], x[j]);
         }
-        __syncthreads();
     }
+    cp_async_wait<0>();
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
+    for (int j = 0; j < 4; ++j) {
         int col = ty + 16 * j;
         if (col >= ncol) continue;
-        double2* y = Y + yo[col];
+        double2* y = Y + yo[col] + t.row0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            int row = t.row0 + tx + 16 * i;
-            if (row >= p.m) continue;
+        for (int i = 0; i < MT; ++i) {
+            int row = tx + 16 * i;
+            if (row >= rows) continue;
             if (mode == GEMM_SET) {
                 y[row] = acc[i][j];
             } else if (mode == GEMM_ADD) {
@@ -134,10 +159,39 @@ __global__ void __launch_bounds__(256) zgemm_kernel(const GemmProblem* __restric
     }
 }
 
+__global__ void __launch_bounds__(256, 2) zgemm_kernel(const GemmProblem* __restrict__ probs,
+                                                       const GemmTile* __restrict__ tiles,
+                                                       const long long* __restrict__ xoff,
+                                                       const long long* __restrict__ yoff,
+                                                       const double2* __restrict__ X, double2* Y, int mode) {
+    extern __shared__ double2 gsm[];
+    __shared__ long long xo[BN], yo[BN];
+    const GemmTile t = tiles[blockIdx.x];
+    const GemmProblem p = probs[t.prob];
+    const int tid = threadIdx.x;
+    const int ncol = min(BN, p.ncol - t.col0);
+    const int rows = min(BM, p.m - t.row0);
+    if (tid < BN) {
+        xo[tid] = tid < ncol ? xoff[p.col0 + t.col0 + tid] : 0;
+        yo[tid] = tid < ncol ? yoff[p.col0 + t.col0 + tid] : 0;
+    }
+    __syncthreads();
+    switch ((rows + 15) >> 4) {
+        case 1: zgemm_tile<1>(p, t, ncol, rows, xo, yo, X, Y, mode, gsm); break;
+        case 2: zgemm_tile<2>(p, t, ncol, rows, xo, yo, X, Y, mode, gsm); break;
+        case 3: zgemm_tile<3>(p, t, ncol, rows, xo, yo, X, Y, mode, gsm); break;
+        default: zgemm_tile<4>(p, t, ncol, rows, xo, yo, X, Y, mode, gsm); break;
+    }
+}
+
+void gemm_init() {
+    cudaFuncSetAttribute(zgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
+}
+
 void launch_gemm(const GemmProblem* probs, const GemmTile* tiles, int ntiles, const long long* xoff,
                  const long long* yoff, const double2* X, double2* Y, int mode, cudaStream_t s) {
     if (ntiles == 0) return;
-    zgemm_kernel<<<ntiles, 256, 0, s>>>(probs, tiles, xoff, yoff, X, Y, mode);
+    zgemm_kernel<<<ntiles, 256, GEMM_SMEM, s>>>(probs, tiles, xoff, yoff, X, Y, mode);
 }
 
 // ---------------------------------------------------------------- points

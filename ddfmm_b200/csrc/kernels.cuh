@@ -16,7 +16,9 @@ struct GemmProblem {
     int col0;  // first entry in the column arrays
     int ncol;
 };
-// A launch is a list of 64 x 32 output tiles.
+// A launch is a list of output tiles of up to GEMM_TILE_M rows x GEMM_TILE_N columns.
+constexpr int GEMM_TILE_M = 64, GEMM_TILE_N = 64;
+void gemm_init();
 struct GemmTile {
     int prob;
     int row0;

@@ -92,8 +92,8 @@ void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<
         P.push_back(q);
         xs.insert(xs.end(), xo[i].begin(), xo[i].end());
         ys.insert(ys.end(), yo[i].begin(), yo[i].end());
-        for (int r0 = 0; r0 < q.m; r0 += 64)
-            for (int c0 = 0; c0 < q.ncol; c0 += 32) tiles.push_back(GemmTile{pid, r0, c0, 0});
+        for (int r0 = 0; r0 < q.m; r0 += GEMM_TILE_M)
+            for (int c0 = 0; c0 < q.ncol; c0 += GEMM_TILE_N) tiles.push_back(GemmTile{pid, r0, c0, 0});
         flops += 8.0 * q.m * q.k * (double)q.ncol;
         // operator once, each input and output column once (read-modify-write for += modes)
         bytes += 16.0 * ((double)q.m * q.k + (double)q.k * q.ncol + (mode == GEMM_SET ? 1.0 : 2.0) * q.m * q.ncol);
@@ -136,6 +136,48 @@ void Session::add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>&
 }
 
 namespace {
+// Setup-time matrix products C = A * B for many small operators in one
+// launch: each product is one grouped-GEMM problem whose "columns" are the
+// columns of B (read from pool X) and of C (written to pool Y).
+struct GemmBatch {
+    std::vector<GemmProblem> probs;
+    std::vector<long long> xs, ys;
+    // A (m x k, lda m, device pointer), B = X[bx ..] (k x n), C = Y[cy ..] (m x n)
+    void product(const double2* A, int m, int k, size_t bx, int n, size_t cy) {
+        GemmProblem p{A, m, k, m, (int)xs.size(), n};
+        for (int j = 0; j < n; ++j) {
+            xs.push_back((long long)(bx + (size_t)j * k));
+            ys.push_back((long long)(cy + (size_t)j * m));
+        }
+        probs.push_back(p);
+    }
+    void run(const double2* X, double2* Y, cudaStream_t s) {
+        if (probs.empty()) return;
+        std::vector<GemmTile> tiles;
+        for (size_t i = 0; i < probs.size(); ++i)
+            for (int r0 = 0; r0 < probs[i].m; r0 += GEMM_TILE_M)
+                for (int c0 = 0; c0 < probs[i].ncol; c0 += GEMM_TILE_N) tiles.push_back(GemmTile{(int)i, r0, c0, 0});
+        GemmProblem* dp;
+        GemmTile* dt;
+        long long *dx, *dy;
+        CK(cudaMalloc(&dp, sizeof(GemmProblem) * probs.size()));
+        CK(cudaMalloc(&dt, sizeof(GemmTile) * tiles.size()));
+        CK(cudaMalloc(&dx, sizeof(long long) * xs.size()));
+        CK(cudaMalloc(&dy, sizeof(long long) * ys.size()));
+        CK(cudaMemcpyAsync(dp, probs.data(), sizeof(GemmProblem) * probs.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(dt, tiles.data(), sizeof(GemmTile) * tiles.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(dx, xs.data(), sizeof(long long) * xs.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(dy, ys.data(), sizeof(long long) * ys.size(), cudaMemcpyHostToDevice, s));
+        launch_gemm(dp, dt, (int)tiles.size(), dx, dy, X, Y, GEMM_SET, s);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s));
+        cudaFree(dp);
+        cudaFree(dt);
+        cudaFree(dx);
+        cudaFree(dy);
+    }
+};
+
 struct NodeKey {
     uint64_t operator()(int box, const Idx3& d) const {
         return ((uint64_t)box << 33) | ((uint64_t)(d[0] + 1024) << 22) | ((uint64_t)(d[1] + 1024) << 11) |
@@ -269,6 +311,7 @@ void Session::build() {
     double2* d_twf = upload(twf);
     double2* d_twb = upload(twb);
     vlist_init(G);
+    gemm_init();
 
     for (auto& kv : lflevels) {
         int level = kv.first;
@@ -444,31 +487,46 @@ void Session::build() {
     double2* hf_dnchk = dalloc<double2>((size_t)dnchk_total);
     double2* T0 = dalloc<double2>((size_t)tmp_max);
     double2* T1 = dalloc<double2>((size_t)tmp_max);
-    double2* T2 = dalloc<double2>((size_t)tmp_max);
     zero_at_start_.push_back(Memset{hf_dnchk, sizeof(double2) * (size_t)dnchk_total});
 
-    // HF M2M / L2L matrices per (W, dir, child) and M2L matrices per
-    // (W, canonical wedge, canonical offset); all generated once here.
+    // ---------------------------------------------------------------- HF operators
+    // Raw kernel matrices -- M2M ue2uc and L2L de2dc per (W, wedge, child), M2L per
+    // (W, canonical wedge, canonical offset) -- are generated once, then folded
+    // with the skeleton factors of uc2ue = {E1, E2, E3} (src/mlib3d.cpp:204-207,
+    // :246-250) so that the eval applies one dense operator per translation plus
+    // E2 / E2^T per (box, wedge):
+    //   upward   w    = E2 * sum_c [E3 * ue2uc_c * E1(child)] w_c        (upeqnden = E1 w)
+    //   M2L      u_t += [E1^T * M(o) * E1] w_s                          (u = E1^T dnchkval)
+    //   downward u_c += [E1(child)^T * de2dc_c * E3^T] (E2^T u)          (dneqnden = E3^T E2^T u)
+    // At W = 1 the children are low-frequency boxes and carry no E1 factor.
+    // E1 = inv(R1) and E3 = inv(R2^H) are ill-conditioned (~1e7), so they are
+    // only ever multiplied into the smooth kernel matrices, never into each other.
+    auto take = [](size_t& pool, size_t n) {
+        size_t o = pool;
+        pool += (n + 15) & ~(size_t)15;
+        return o;
+    };
+    size_t scr = 0, keep = 0;
     struct DirMats {
-        double2* m2m[8];
-        double2* l2l[8];
-        int mrows, mcols;  // m2m: r2 x rc ; l2l: rc x r2
+        size_t raw[8], tmp[8], fin[8];
+        int mrows, mcols, canon, ccanon;
     };
     std::map<std::pair<double, Idx3>, DirMats> m2m_mats, l2l_mats;
-    const LowFreqOp* lf_half = nullptr;
     const double* lf_half_uep = nullptr;
     if (!hflevels.empty()) {
-        lf_half = &ops_.low(0.5);
-        if (lf_half->uep.n != nE) throw std::runtime_error("width-1/2 operators do not match ACCU");
-        lf_half_uep = upload(lf_half->uep.x);
+        const LowFreqOp& lf_half = ops_.low(0.5);
+        if (lf_half.uep.n != nE) throw std::runtime_error("width-1/2 operators do not match ACCU");
+        lf_half_uep = upload(lf_half.uep.x);
     }
-    auto child_pts = [&](double W, const Idx3& dir, bool upward, int& rc) -> const double* {
+    auto child_pts = [&](double W, const Idx3& dir, bool upward, int& rc, int& ccanon) -> const double* {
         if (W == 1.0) {
             rc = nE;
+            ccanon = -1;
             return lf_half_uep;  // LF uep at W/2 for both directions (src/mlib3d.cpp:199-202,254-257)
         }
         const DirPts& cp = get_dir(W / 2, predir(dir));
         rc = cp.r1;
+        ccanon = cp.canon;
         return upward ? cp.uep : cp.dcp;
     };
     for (auto& kv : hflevels) {
@@ -478,14 +536,15 @@ void Session::build() {
             auto key = std::make_pair(W, up[i].dir);
             if (m2m_mats.count(key)) continue;
             const DirPts& dp = get_dir(W, up[i].dir);
-            int rc;
-            const double* cp = child_pts(W, up[i].dir, true, rc);
             DirMats M{};
+            child_pts(W, up[i].dir, true, M.mcols, M.ccanon);
             M.mrows = dp.r2;
-            M.mcols = rc;
+            M.canon = dp.canon;
             for (int ind = 0; ind < 8; ++ind) {
-                M.m2m[ind] = dalloc<double2>((size_t)dp.r2 * rc);
-                add_job(dp.ucp, zero3, cp, shifted_point(ind, W), dp.r2, rc, M.m2m[ind]);
+                size_t n = (size_t)M.mrows * M.mcols;
+                M.raw[ind] = take(scr, n);
+                if (M.ccanon >= 0) M.tmp[ind] = take(scr, n);
+                M.fin[ind] = take(keep, n);
             }
             m2m_mats[key] = M;
         }
@@ -493,32 +552,34 @@ void Session::build() {
             auto key = std::make_pair(W, dn[i].dir);
             if (l2l_mats.count(key)) continue;
             const DirPts& dp = get_dir(W, dn[i].dir);
-            int rc;
-            const double* cp = child_pts(W, dn[i].dir, false, rc);
             DirMats M{};
-            M.mrows = rc;
+            child_pts(W, dn[i].dir, false, M.mrows, M.ccanon);
             M.mcols = dp.r2;
+            M.canon = dp.canon;
             for (int ind = 0; ind < 8; ++ind) {
-                M.l2l[ind] = dalloc<double2>((size_t)rc * dp.r2);
-                add_job(cp, shifted_point(ind, W), dp.dep, zero3, rc, dp.r2, M.l2l[ind]);
+                size_t n = (size_t)M.mrows * M.mcols;
+                M.raw[ind] = take(scr, n);
+                M.fin[ind] = take(keep, n);
+                M.tmp[ind] = M.ccanon >= 0 ? take(scr, n) : M.fin[ind];
             }
             l2l_mats[key] = M;
         }
     }
-    // M2L: canonical offset o_c = S^-1 (c_t - c_s) (see DESIGN: M(dir, o) = M(canon, S^-1 o))
-    std::map<std::tuple<int, int, int, int>, int> m2l_id;  // (canon, ox, oy, oz) -> problem
+    // M2L: canonical offset o_c = S^-1 (c_t - c_s), so M(dir, o) = M(canon, o_c)
+    std::map<std::tuple<int, int, int, int>, int> m2l_id;  // (canon, ox, oy, oz) -> matrix
     struct M2LMat {
-        double2* A;
-        int r1;
+        size_t raw, tmp, fin;
+        int canon, r1;
+        Pt3 shift;
     };
     std::vector<M2LMat> m2l_mats;
     std::map<int, std::vector<std::vector<long long> > > m2l_x, m2l_y;  // level -> per problem columns
-    std::map<int, std::vector<int> > m2l_probs;                         // level -> problem ids
+    std::map<int, std::vector<int> > m2l_probs;                         // level -> matrix ids
     for (auto& kv : hflevels) {
         int level = kv.first;
         double W = T.width(level);
         auto dr = dnrange[level];
-        std::map<int, int> local;  // global m2l id -> local problem index
+        std::map<int, int> local;  // matrix id -> local problem index
         auto& X = m2l_x[level];
         auto& Y = m2l_y[level];
         auto& Pids = m2l_probs[level];
@@ -529,10 +590,10 @@ void Session::build() {
             if (fit == tb.far.end()) continue;
             Idx3 sgn, pv, srt;
             index3_sort(t.dir, srt, sgn, pv);
-            for (int s : fit->second) {
-                auto uit = upmap.find(nk(s, t.dir));
+            for (int sb_i : fit->second) {
+                auto uit = upmap.find(nk(sb_i, t.dir));
                 if (uit == upmap.end()) throw std::runtime_error("M2L source has no outgoing equivalent density");
-                const Box& sb = T.boxes[s];
+                const Box& sb = T.boxes[sb_i];
                 int o[3], oc[3];
                 for (int d = 0; d < 3; ++d) o[d] = tb.idx[d] - sb.idx[d];
                 for (int d = 0; d < 3; ++d) oc[d] = sgn[pv[d]] * o[pv[d]];
@@ -542,9 +603,9 @@ void Session::build() {
                 if (mit == m2l_id.end()) {
                     const Canon& c = hfcanon[t.canon];
                     gid = (int)m2l_mats.size();
-                    M2LMat M{dalloc<double2>((size_t)c.r1 * c.r1), c.r1};
-                    Pt3 sh{{oc[0] * W, oc[1] * W, oc[2] * W}};
-                    add_job(c.neg_uep, sh, c.uep, zero3, c.r1, c.r1, M.A);
+                    size_t n = (size_t)c.r1 * c.r1;
+                    M2LMat M{take(scr, n), take(scr, n), take(keep, n), t.canon, c.r1,
+                             Pt3{{oc[0] * W, oc[1] * W, oc[2] * W}}};
                     m2l_mats.push_back(M);
                     m2l_id[key] = gid;
                 } else {
@@ -568,6 +629,39 @@ void Session::build() {
         }
     }
     stats_.m2l_matrices = (long long)m2l_mats.size();
+    // right factors E1 and E3^T as gatherable columns in the scratch pool
+    std::vector<size_t> scr_E1(hfcanon.size()), scr_E3t(hfcanon.size());
+    for (size_t c = 0; c < hfcanon.size(); ++c) {
+        scr_E1[c] = take(scr, (size_t)hfcanon[c].r1 * hfcanon[c].r1);
+        scr_E3t[c] = take(scr, (size_t)hfcanon[c].r2 * hfcanon[c].r2);
+    }
+    double2* dkeep = dalloc<double2>(keep);
+    double2* dscr = nullptr;
+    if (scr) CK(cudaMalloc(&dscr, sizeof(double2) * scr));
+    for (size_t c = 0; c < hfcanon.size(); ++c) {
+        CK(cudaMemcpyAsync(dscr + scr_E1[c], hfcanon[c].E1, sizeof(double2) * hfcanon[c].r1 * hfcanon[c].r1,
+                           cudaMemcpyDeviceToDevice, stream_));
+        CK(cudaMemcpyAsync(dscr + scr_E3t[c], hfcanon[c].E3t, sizeof(double2) * hfcanon[c].r2 * hfcanon[c].r2,
+                           cudaMemcpyDeviceToDevice, stream_));
+    }
+    for (auto& kv : m2m_mats) {
+        double W = kv.first.first;
+        const DirPts& dp = get_dir(W, kv.first.second);
+        int rc, cc;
+        const double* cp = child_pts(W, kv.first.second, true, rc, cc);
+        for (int ind = 0; ind < 8; ++ind)
+            add_job(dp.ucp, zero3, cp, shifted_point(ind, W), dp.r2, rc, dscr + kv.second.raw[ind]);
+    }
+    for (auto& kv : l2l_mats) {
+        double W = kv.first.first;
+        const DirPts& dp = get_dir(W, kv.first.second);
+        int rc, cc;
+        const double* cp = child_pts(W, kv.first.second, false, rc, cc);
+        for (int ind = 0; ind < 8; ++ind)
+            add_job(cp, shifted_point(ind, W), dp.dep, zero3, rc, dp.r2, dscr + kv.second.raw[ind]);
+    }
+    for (const M2LMat& M : m2l_mats)
+        add_job(hfcanon[M.canon].neg_uep, M.shift, hfcanon[M.canon].uep, zero3, M.r1, M.r1, dscr + M.raw);
 
     // generate every kernel matrix now
     if (!jobs.empty()) {
@@ -575,6 +669,42 @@ void Session::build() {
         launch_kmat(d_jobs, (int)jobs.size(), job_elems, kern, stream_);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(stream_));
+    }
+
+    // fold: right products (raw * E1 or raw * E3^T), then left products (E3 * . or E1^T * .)
+    if (scr) {
+        GemmBatch right_s, right_k, left;
+        for (auto& kv : m2m_mats) {
+            const DirMats& M = kv.second;
+            for (int ind = 0; ind < 8; ++ind) {
+                if (M.ccanon >= 0) {  // tmp = ue2uc * E1(child)
+                    right_s.product(dscr + M.raw[ind], M.mrows, M.mcols, scr_E1[M.ccanon], M.mcols, M.tmp[ind]);
+                    left.product(hfcanon[M.canon].E3, M.mrows, M.mrows, M.tmp[ind], M.mcols, M.fin[ind]);
+                } else {
+                    left.product(hfcanon[M.canon].E3, M.mrows, M.mrows, M.raw[ind], M.mcols, M.fin[ind]);
+                }
+            }
+        }
+        for (auto& kv : l2l_mats) {
+            const DirMats& M = kv.second;
+            for (int ind = 0; ind < 8; ++ind) {
+                if (M.ccanon >= 0) {  // tmp = de2dc * E3^T ; fin = E1(child)^T * tmp
+                    right_s.product(dscr + M.raw[ind], M.mrows, M.mcols, scr_E3t[M.canon], M.mcols, M.tmp[ind]);
+                    left.product(hfcanon[M.ccanon].E1t, M.mrows, M.mrows, M.tmp[ind], M.mcols, M.fin[ind]);
+                } else {  // children are low-frequency boxes: fin = de2dc * E3^T
+                    right_k.product(dscr + M.raw[ind], M.mrows, M.mcols, scr_E3t[M.canon], M.mcols, M.fin[ind]);
+                }
+            }
+        }
+        for (const M2LMat& M : m2l_mats) {
+            right_s.product(dscr + M.raw, M.r1, M.r1, scr_E1[M.canon], M.r1, M.tmp);
+            left.product(hfcanon[M.canon].E1t, M.r1, M.r1, M.tmp, M.r1, M.fin);
+        }
+        right_s.run(dscr, dscr, stream_);
+        right_k.run(dscr, dkeep, stream_);
+        left.run(dscr, dkeep, stream_);
+        CK(cudaStreamSynchronize(stream_));
+        CK(cudaFree(dscr));
     }
 
     // ---------------------------------------------------------------- steps: LF upward
@@ -636,7 +766,7 @@ void Session::build() {
     }
 
     // ---------------------------------------------------------------- steps: HF upward
-    // widths ascending = levels descending
+    // widths ascending = levels descending; hf_upeq holds w (upeqnden = E1 w)
     for (auto hit = hflevels.rbegin(); hit != hflevels.rend(); ++hit) {
         int level = hit->first;
         double W = T.width(level);
@@ -647,7 +777,7 @@ void Session::build() {
         ms.label = "memset";
         ms.ms = Memset{T0, sizeof(double2) * (size_t)tmp_max};
         steps_.push_back(ms);
-        // M2M: upchk = sum_children ue2uc(abc) * child's upeqnden (src/wave3d_eval.cpp:796-834)
+        // M2M: E3 upchkval = sum_children [E3 ue2uc E1(child)] w_child (src/wave3d_eval.cpp:796-834)
         for (int ind = 0; ind < 8; ++ind) {
             std::map<Idx3, int> pid;
             std::vector<GemmProblem> probs;
@@ -670,7 +800,7 @@ void Session::build() {
                     const DirMats& M = m2m_mats.at(std::make_pair(W, u.dir));
                     p = (int)probs.size();
                     pid[u.dir] = p;
-                    probs.push_back(GemmProblem{M.m2m[ind], M.mrows, M.mcols, M.mrows, 0, 0});
+                    probs.push_back(GemmProblem{dkeep + M.fin[ind], M.mrows, M.mcols, M.mrows, 0, 0});
                     xo.emplace_back();
                     yo.emplace_back();
                 } else {
@@ -681,21 +811,19 @@ void Session::build() {
             }
             add_gemm(probs, xo, yo, W == 1.0 ? lf_upeq : hf_upeq, T0, GEMM_ADD, "hf_m2m");
         }
-        // upeqnden = E1 * (E2 * (E3 * upchk))   (src/wave3d_eval.cpp:837-849)
+        // w = E2 * (E3 upchkval)   (src/wave3d_eval.cpp:837-849)
         std::map<int, int> cp;
-        std::vector<GemmProblem> p3, p2, p1;
-        std::vector<std::vector<long long> > xa, ya, xb;
+        std::vector<GemmProblem> p2;
+        std::vector<std::vector<long long> > xa, ya;
         for (int i = ur.first; i < ur.second; ++i) {
             const Node& u = up[i];
             auto it2 = cp.find(u.canon);
             int p;
             if (it2 == cp.end()) {
                 const Canon& c = hfcanon[u.canon];
-                p = (int)p3.size();
+                p = (int)p2.size();
                 cp[u.canon] = p;
-                p3.push_back(GemmProblem{c.E3, c.r2, c.r2, c.r2, 0, 0});
                 p2.push_back(GemmProblem{c.E2, c.r1, c.r2, c.r1, 0, 0});
-                p1.push_back(GemmProblem{c.E1, c.r1, c.r1, c.r1, 0, 0});
                 xa.emplace_back();
                 ya.emplace_back();
             } else {
@@ -704,13 +832,11 @@ void Session::build() {
             xa[p].push_back(u.toff);
             ya[p].push_back(u.off);
         }
-        add_gemm(p3, xa, xa, T0, T1, GEMM_SET, "hf_uc2ue");
-        add_gemm(p2, xa, xa, T1, T2, GEMM_SET, "hf_uc2ue");
-        add_gemm(p1, xa, ya, T2, hf_upeq, GEMM_SET, "hf_uc2ue");
+        add_gemm(p2, xa, ya, T0, hf_upeq, GEMM_SET, "hf_uc2ue");
     }
 
     // ---------------------------------------------------------------- steps: HF downward
-    // widths descending = levels ascending
+    // widths descending = levels ascending; hf_dnchk holds u = E1^T dnchkval
     for (auto it = hflevels.begin(); it != hflevels.end(); ++it) {
         int level = it->first;
         double W = T.width(level);
@@ -721,13 +847,13 @@ void Session::build() {
             std::vector<GemmProblem> probs;
             for (int gid : m2l_probs[level]) {
                 const M2LMat& M = m2l_mats[gid];
-                probs.push_back(GemmProblem{M.A, M.r1, M.r1, M.r1, 0, 0});
+                probs.push_back(GemmProblem{dkeep + M.fin, M.r1, M.r1, M.r1, 0, 0});
             }
             add_gemm(probs, m2l_x[level], m2l_y[level], hf_upeq, hf_dnchk, GEMM_ATOMIC, "hf_m2l");
         }
-        // dneqnden = E3^T (E2^T (E1^T dnchk))   (src/wave3d_eval.cpp:938-948, src/mlib3d.cpp:246-250)
+        // t = E2^T u   (dneqnden = E3^T t, src/wave3d_eval.cpp:938-948, src/mlib3d.cpp:246-250)
         std::map<int, int> cp;
-        std::vector<GemmProblem> p1, p2, p3;
+        std::vector<GemmProblem> p2;
         std::vector<std::vector<long long> > xa, xt;
         for (int i = dr.first; i < dr.second; ++i) {
             const Node& d = dn[i];
@@ -735,11 +861,9 @@ void Session::build() {
             int p;
             if (it2 == cp.end()) {
                 const Canon& c = hfcanon[d.canon];
-                p = (int)p1.size();
+                p = (int)p2.size();
                 cp[d.canon] = p;
-                p1.push_back(GemmProblem{c.E1t, c.r1, c.r1, c.r1, 0, 0});
                 p2.push_back(GemmProblem{c.E2t, c.r2, c.r1, c.r2, 0, 0});
-                p3.push_back(GemmProblem{c.E3t, c.r2, c.r2, c.r2, 0, 0});
                 xa.emplace_back();
                 xt.emplace_back();
             } else {
@@ -748,10 +872,8 @@ void Session::build() {
             xa[p].push_back(d.off);
             xt[p].push_back(d.toff);
         }
-        add_gemm(p1, xa, xt, hf_dnchk, T0, GEMM_SET, "hf_dc2de");
-        add_gemm(p2, xt, xt, T0, T1, GEMM_SET, "hf_dc2de");
-        add_gemm(p3, xt, xt, T1, T2, GEMM_SET, "hf_dc2de");
-        // L2L into the children's (pdir) check values, or LF dnchkval at W=1 (src/wave3d_eval.cpp:950-991)
+        add_gemm(p2, xa, xt, hf_dnchk, T1, GEMM_SET, "hf_dc2de");
+        // L2L into the children's (pdir) u, or LF dnchkval at W=1 (src/wave3d_eval.cpp:950-991)
         for (int ind = 0; ind < 8; ++ind) {
             std::map<Idx3, int> pid;
             std::vector<GemmProblem> probs;
@@ -774,7 +896,7 @@ void Session::build() {
                     const DirMats& M = l2l_mats.at(std::make_pair(W, d.dir));
                     p = (int)probs.size();
                     pid[d.dir] = p;
-                    probs.push_back(GemmProblem{M.l2l[ind], M.mrows, M.mcols, M.mrows, 0, 0});
+                    probs.push_back(GemmProblem{dkeep + M.fin[ind], M.mrows, M.mcols, M.mrows, 0, 0});
                     xo.emplace_back();
                     yo.emplace_back();
                 } else {
@@ -783,7 +905,7 @@ void Session::build() {
                 xo[p].push_back(d.toff);
                 yo[p].push_back(yoff);
             }
-            add_gemm(probs, xo, yo, T2, W == 1.0 ? lf_dnchk : hf_dnchk, GEMM_ATOMIC, "hf_l2l");
+            add_gemm(probs, xo, yo, T1, W == 1.0 ? lf_dnchk : hf_dnchk, GEMM_ATOMIC, "hf_l2l");
         }
     }
 

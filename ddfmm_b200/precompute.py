@@ -296,6 +296,13 @@ def ensure_operators(cache_dir: str, kind: int, accu: int, wmax: int, workers: i
     widths 1..wmax.  Files are written atomically."""
     os.makedirs(cache_dir, exist_ok=True)
     ld_path, hd_path = operator_paths(cache_dir, kind, accu, wmax)
+    # a file built for wider boxes holds every narrower width too
+    w = max(1, wmax)
+    while not os.path.exists(hd_path) and w <= 64:
+        w *= 2
+        cand = operator_paths(cache_dir, kind, accu, w)[1]
+        if os.path.exists(cand):
+            hd_path = cand
     if not os.path.exists(ld_path):
         tmp = ld_path + ".tmp%d" % os.getpid()
         formats.write_ld(tmp, lowfreq_levels(accu, kind))

@@ -95,3 +95,5 @@ def cluster(K, N, accu=1, kernel=0, seed=0, ptsmax=8):
 SMALL = sphere(8, 5000, accu=1)
 # the large single instance (about 25 points per square wavelength)
 LARGE = sphere(64, None, accu=2)
+# a quarter-size instance of the same family (profiling captures)
+MEDIUM = sphere(32, None, accu=2)

@@ -35,6 +35,7 @@ def test_matches_reference_output(name, tmp_path):
     w.eval(c.den, val)
     rel = np.linalg.norm(val - c.val) / np.linalg.norm(c.val)
     worst = np.max(np.abs(val - c.val)) / np.max(np.abs(c.val))
+    print("parity %s: rel l2 %.3e, max %.3e" % (name, rel, worst))
     assert rel <= TOL and worst <= 10 * TOL, (rel, worst)
     # Wave3d::check against the FP64 direct sum reproduces the reference's relerr
     relerr = w.check(c.den, val, c.chk)
