@@ -57,16 +57,22 @@ void launch_kmat(const KmatJob* jobs, int njobs, long long total, int kernel, cu
 
 // ---------------------------------------------------------------- gemm
 // Grouped complex FP64 GEMM with gathered input columns and scattered output
-// columns.  A 256-thread block computes up to 64 rows x 64 columns: thread
-// (tx, ty) owns rows tx + 16*i (i < MT) and columns ty + 16*j (j < 4), so
-// consecutive lanes write consecutive rows of one output vector.  MT =
-// ceil(tile rows / 16) is a compile-time specialisation chosen per tile, so
-// an 80-150-row translation operator wastes at most 15 rows and the inner
-// loop carries no guards.  K is consumed in slices of 16 through a 3-stage
+// columns, on the FP64 tensor path (mma.sync m8n8k4 f64).  A 256-thread block
+// computes up to 64 rows x 64 columns; warp (wm, wn) owns the 16-row slab wm
+// (two 8-row MMA blocks) and columns wn*32 .. +32 (four 8-column blocks).  A
+// complex block product takes four real MMAs:
+//   Cr += Ar Br + (-Ai) Bi,   Ci += Ar Bi + Ai Br.
+// Slabs beyond the operator's rows are skipped (a tile carries
+// ceil(rows / 16) active slabs), so an 80-150-row translation operator
+// wastes at most 15 rows.  K is consumed in slices of 16 through a 3-stage
 // cp.async pipeline; rows, columns and k beyond the problem are zero-filled
-// by the copy (src-size 0).
-constexpr int BM = 64, BN = 64, BK = 16, GSTAGES = 3;
-constexpr int GEMM_SMEM = GSTAGES * (BK * BM + BK * BN) * (int)sizeof(double2);
+// by the copy (src-size 0).  128-bit shared loads are served in 8-lane
+// phases (lanes with g in {2p, 2p+1}, tig 0..3); both fragment layouts put
+// those 8 granules in 8 different bank groups: the operator slice is stored
+// [k][row ^ 2*(k & 3)] and the column slice [col][k] with a 20-granule stride.
+constexpr int BM = 64, BN = 64, BK = 16, BKP = 20, GSTAGES = 3;
+constexpr int GSTAGE = BK * BM + BN * BKP;  // double2 per stage
+constexpr int GEMM_SMEM = GSTAGES * GSTAGE * (int)sizeof(double2);
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
     unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -76,35 +82,55 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-template <int MT>
-__device__ __forceinline__ void zgemm_tile(const GemmProblem& p, const GemmTile& t, int ncol, int rows,
-                                           const long long* xo, const long long* yo, const double2* __restrict__ X,
-                                           double2* Y, int mode, double2* gsm) {
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(256, 2) zgemm_kernel(const GemmProblem* __restrict__ probs,
+                                                       const GemmTile* __restrict__ tiles,
+                                                       const long long* __restrict__ xoff,
+                                                       const long long* __restrict__ yoff,
+                                                       const double2* __restrict__ X, double2* Y, int mode) {
+    extern __shared__ double2 gsm[];
+    __shared__ long long xo[BN], yo[BN];
+    const GemmTile t = tiles[blockIdx.x];
+    const GemmProblem p = probs[t.prob];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, tig = lane & 3, wm = warp >> 1, wn = warp & 1;
+    const int ncol = min(BN, p.ncol - t.col0);
+    const int rows = min(BM, p.m - t.row0);
+    const int nrow = ((rows + 15) >> 4) << 4;  // rows of the active slabs
+    const bool active = wm * 16 < rows;
+    if (tid < BN) {
+        xo[tid] = tid < ncol ? xoff[p.col0 + t.col0 + tid] : 0;
+        yo[tid] = tid < ncol ? yoff[p.col0 + t.col0 + tid] : 0;
+    }
+    __syncthreads();
     auto load = [&](int stage, int k0) {
-        double2* As = gsm + stage * (BK * (BM + BN));
+        double2* As = gsm + stage * GSTAGE;
         double2* Xs = As + BK * BM;
-#pragma unroll
-        for (int q = 0; q < MT; ++q) {  // BK x (16*MT) elements of A, MT per thread
-            int e = tid + 256 * q, row = e % (16 * MT), kk = e / (16 * MT);
+        for (int e = tid; e < BK * nrow; e += 256) {
+            int kk = e / nrow, row = e - kk * nrow;
             int gk = k0 + kk;
             bool ok = row < rows && gk < p.k;
-            cp_async16(&As[kk * BM + row], ok ? (const void*)(p.A + (size_t)gk * p.lda + t.row0 + row) : (const void*)p.A,
-                       ok ? 16 : 0);
+            cp_async16(&As[kk * BM + (row ^ ((kk & 3) << 1))],
+                       ok ? (const void*)(p.A + (size_t)gk * p.lda + t.row0 + row) : (const void*)p.A, ok ? 16 : 0);
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             int e = tid + 256 * q, kk = e & 15, col = e >> 4;
             int gk = k0 + kk;
             bool ok = col < ncol && gk < p.k;
-            cp_async16(&Xs[col * BK + kk], ok ? (const void*)(X + xo[col] + gk) : (const void*)X, ok ? 16 : 0);
+            cp_async16(&Xs[col * BKP + kk], ok ? (const void*)(X + xo[col] + gk) : (const void*)X, ok ? 16 : 0);
         }
     };
-    double2 acc[MT][4];
+    double cr[2][4][2], ci[2][4][2];
 #pragma unroll
-    for (int i = 0; i < MT; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
+        for (int j = 0; j < 4; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
     const int nk = (p.k + BK - 1) / BK;
 #pragma unroll
     for (int s = 0; s < GSTAGES - 1; ++s) {
@@ -119,69 +145,63 @@ __device__ __forceinline__ void zgemm_tile(const GemmProblem& p, const GemmTile&
             if (nx < nk) load(nx % GSTAGES, nx * BK);
             cp_async_commit();
         }
-        const double2* As = gsm + (it % GSTAGES) * (BK * (BM + BN));
-        const double2* Xs = As + BK * BM;
+        if (active) {
+            const double2* As = gsm + (it % GSTAGES) * GSTAGE + tig * BM + ((wm * 16 + g) ^ (tig << 1));
+            const double2* Xs = gsm + (it % GSTAGES) * GSTAGE + BK * BM + (wn * 32 + g) * BKP + tig;
 #pragma unroll
-        for (int kk = 0; kk < BK; ++kk) {
-            double2 a[MT], x[4];
+            for (int ks = 0; ks < BK / 4; ++ks) {
+                double2 a[2], b[4];
 #pragma unroll
-            for (int i = 0; i < MT; ++i) a[i] = As[kk * BM + tx + 16 * i];
+                for (int i = 0; i < 2; ++i) a[i] = As[ks * 4 * BM + i * 8];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) x[j] = Xs[(ty + 16 * j) * BK + kk];
+                for (int j = 0; j < 4; ++j) b[j] = Xs[j * 8 * BKP + ks * 4];
+                // four passes over the 8 blocks: dependent MMAs are 8 apart
 #pragma unroll
-            for (int i = 0; i < MT; ++i)
+                for (int i = 0; i < 2; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) cfma(acc[i][j], a[i], x[j]);
-        }
-    }
-    cp_async_wait<0>();
+                    for (int j = 0; j < 4; ++j) dmma(cr[i][j], a[i].x, b[j].x);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        int col = ty + 16 * j;
-        if (col >= ncol) continue;
-        double2* y = Y + yo[col] + t.row0;
+                for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int i = 0; i < MT; ++i) {
-            int row = tx + 16 * i;
-            if (row >= rows) continue;
-            if (mode == GEMM_SET) {
-                y[row] = acc[i][j];
-            } else if (mode == GEMM_ADD) {
-                double2 v = y[row];
-                v.x += acc[i][j].x;
-                v.y += acc[i][j].y;
-                y[row] = v;
-            } else {
-                atomicAdd(&y[row].x, acc[i][j].x);
-                atomicAdd(&y[row].y, acc[i][j].y);
+                    for (int j = 0; j < 4; ++j) dmma(ci[i][j], a[i].x, b[j].y);
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) dmma(cr[i][j], -a[i].y, b[j].y);
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) dmma(ci[i][j], a[i].y, b[j].x);
             }
         }
     }
-}
-
-__global__ void __launch_bounds__(256, 2) zgemm_kernel(const GemmProblem* __restrict__ probs,
-                                                       const GemmTile* __restrict__ tiles,
-                                                       const long long* __restrict__ xoff,
-                                                       const long long* __restrict__ yoff,
-                                                       const double2* __restrict__ X, double2* Y, int mode) {
-    extern __shared__ double2 gsm[];
-    __shared__ long long xo[BN], yo[BN];
-    const GemmTile t = tiles[blockIdx.x];
-    const GemmProblem p = probs[t.prob];
-    const int tid = threadIdx.x;
-    const int ncol = min(BN, p.ncol - t.col0);
-    const int rows = min(BM, p.m - t.row0);
-    if (tid < BN) {
-        xo[tid] = tid < ncol ? xoff[p.col0 + t.col0 + tid] : 0;
-        yo[tid] = tid < ncol ? yoff[p.col0 + t.col0 + tid] : 0;
-    }
-    __syncthreads();
-    switch ((rows + 15) >> 4) {
-        case 1: zgemm_tile<1>(p, t, ncol, rows, xo, yo, X, Y, mode, gsm); break;
-        case 2: zgemm_tile<2>(p, t, ncol, rows, xo, yo, X, Y, mode, gsm); break;
-        case 3: zgemm_tile<3>(p, t, ncol, rows, xo, yo, X, Y, mode, gsm); break;
-        default: zgemm_tile<4>(p, t, ncol, rows, xo, yo, X, Y, mode, gsm); break;
-    }
+    cp_async_wait<0>();
+    if (!active) return;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            int col = wn * 32 + j * 8 + 2 * tig + e;
+            if (col >= ncol) continue;
+            double2* y = Y + yo[col] + t.row0;
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                int row = wm * 16 + i * 8 + g;
+                if (row >= rows) continue;
+                double2 v = make_double2(cr[i][j][e], ci[i][j][e]);
+                if (mode == GEMM_SET) {
+                    y[row] = v;
+                } else if (mode == GEMM_ADD) {
+                    double2 o = y[row];
+                    o.x += v.x;
+                    o.y += v.y;
+                    y[row] = o;
+                } else {
+                    atomicAdd(&y[row].x, v.x);
+                    atomicAdd(&y[row].y, v.y);
+                }
+            }
+        }
 }
 
 void gemm_init() {
@@ -231,68 +251,107 @@ void launch_pt(const PtItem* items, int nitems, const PtSrc* srcs, int kernel, c
 }
 
 // ---------------------------------------------------------------- V list
-// Separable DFT of a G^3 grid held in shared memory, element (a,b,c) at
-// a + G*(b + G*c) as in the reference's CpxNumTns (include/numtns.hpp:104-117).
-// sign -1 is FFTW_FORWARD, +1 FFTW_BACKWARD (unnormalised).
-__device__ void dft3_smem(double2* g, int G, const double2* __restrict__ tw, int nthreads) {
-    const int tot = G * G * G;
-    const int stride[3] = {1, G, G * G};
-    for (int ax = 0; ax < 3; ++ax) {
-        const int st = stride[ax];
-        double2 out[16];
-        int cnt = 0;
-        for (int e = threadIdx.x; e < tot; e += nthreads, ++cnt) {
-            int k = (e / st) % G;
-            int base = e - k * st;
-            double2 acc = make_double2(0.0, 0.0);
-            for (int j = 0; j < G; ++j) cfma(acc, g[base + j * st], tw[(j * k) % G]);
-            out[cnt] = acc;
-        }
-        __syncthreads();
-        cnt = 0;
-        for (int e = threadIdx.x; e < tot; e += nthreads, ++cnt) g[e] = out[cnt];
-        __syncthreads();
-    }
-}
+// FFT-based M2L of the low-frequency V list (src/wave3d_eval.cpp:602-661).
+// The reference scatters a box's equivalent density onto a G^3 grid (G = 2P)
+// at the surface nodes of the P^3 corner cube [P, 2P)^3, FFTs it, multiplies
+// by the FFT'd translation tensor of the box offset, inverse-FFTs and reads
+// the check values back at the same corner-cube nodes.  Grid element
+// (a, b, c) sits at a + G*(b + G*c) (CpxNumTns layout, include/numtns.hpp).
+// Both transforms are pruned to the corner cube: the forward DFT only reads
+// the P^3 cube (3 passes of G*P^2, G^2*P and G^3 outputs with P-term sums)
+// and the inverse only produces it (G^2*P, G*P^2 and P^3 outputs with G-term
+// sums), about a third of the work of full G^3 transforms.  Signs follow
+// FFTW: forward exp(-2 pi i jk/G), backward exp(+2 pi i jk/G), unnormalised.
 
 __global__ void vlist_forward_kernel(VlistLevel L, const int* __restrict__ boxes,
                                      const double2* __restrict__ upeq, double2* __restrict__ spec,
                                      const double2* __restrict__ twf) {
-    extern __shared__ double2 grid[];
-    const int G = L.G, tot = G * G * G;
+    extern __shared__ double2 sm[];
+    const int G = L.G, P = L.P, PP = P * P;
+    double2* cube = sm;             // [c'][b'][a'], a', b', c' < P
+    double2* b1 = cube + PP * P;    // [c'][b'][ka]
+    double2* b2 = b1 + G * PP;      // [c'][kb][ka]
     const int b = boxes[blockIdx.x];
-    for (int e = threadIdx.x; e < tot; e += blockDim.x) grid[e] = make_double2(0.0, 0.0);
+    for (int e = threadIdx.x; e < PP * P; e += blockDim.x) cube[e] = make_double2(0.0, 0.0);
     __syncthreads();
-    for (int k = threadIdx.x; k < L.nE; k += blockDim.x) grid[L.grid_idx[k]] = upeq[(size_t)b * L.nE + k];
+    for (int k = threadIdx.x; k < L.nE; k += blockDim.x) cube[L.cube_idx[k]] = upeq[(size_t)b * L.nE + k];
     __syncthreads();
-    dft3_smem(grid, G, twf, blockDim.x);
-    double2* o = spec + (size_t)b * tot;
-    for (int e = threadIdx.x; e < tot; e += blockDim.x) o[e] = grid[e];
+    for (int e = threadIdx.x; e < G * PP; e += blockDim.x) {
+        int ka = e % G, line = e / G;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int a = 0; a < P; ++a) cfma(acc, cube[line * P + a], twf[((P + a) * ka) % G]);
+        b1[e] = acc;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < G * G * P; e += blockDim.x) {
+        int ka = e % G, kb = (e / G) % G, c = e / (G * G);
+        double2 acc = make_double2(0.0, 0.0);
+        for (int bb = 0; bb < P; ++bb) cfma(acc, b1[(c * P + bb) * G + ka], twf[((P + bb) * kb) % G]);
+        b2[e] = acc;
+    }
+    __syncthreads();
+    double2* o = spec + (size_t)b * G * G * G;
+    for (int e = threadIdx.x; e < G * G * G; e += blockDim.x) {
+        int kab = e % (G * G), kc = e / (G * G);
+        double2 acc = make_double2(0.0, 0.0);
+        for (int c = 0; c < P; ++c) cfma(acc, b2[c * G * G + kab], twf[((P + c) * kc) % G]);
+        o[e] = acc;
+    }
 }
 
-__global__ void vlist_accum_kernel(VlistLevel L, const int* __restrict__ trg, const int* __restrict__ vptr,
-                                   const int* __restrict__ vsrc, const int* __restrict__ voff,
-                                   const double2* __restrict__ spec, double2* __restrict__ dnchk,
-                                   const double2* __restrict__ twb) {
-    extern __shared__ double2 grid[];
-    const int G = L.G, tot = G * G * G;
+template <int G>
+__global__ void __launch_bounds__(256) vlist_accum_kernel(VlistLevel L, const int* __restrict__ trg,
+                                                          const int* __restrict__ vptr, const int* __restrict__ vsrc,
+                                                          const int* __restrict__ voff,
+                                                          const double2* __restrict__ spec,
+                                                          double2* __restrict__ dnchk, const double2* __restrict__ twb) {
+    extern __shared__ double2 sm[];
+    constexpr int P = G / 2, PP = P * P, G3 = G * G * G, NE = (G3 + 255) / 256;
+    double2* grid = sm;          // G^3 accumulated spectrum, later [c'][b'][ka]
+    double2* c1 = sm + G3;       // [c'][kb][ka], later the P^3 cube
     const int ti = blockIdx.x, t = trg[ti];
-    double2 acc[16];
-    int cnt = 0;
-    for (int e = threadIdx.x; e < tot; e += blockDim.x, ++cnt) acc[cnt] = make_double2(0.0, 0.0);
+    double2 acc[NE];
+#pragma unroll
+    for (int q = 0; q < NE; ++q) acc[q] = make_double2(0.0, 0.0);
     for (int v = vptr[ti]; v < vptr[ti + 1]; ++v) {
-        const double2* sp = spec + (size_t)vsrc[v] * tot;
-        const double2* tn = L.tns + (size_t)voff[v] * tot;
-        cnt = 0;
-        for (int e = threadIdx.x; e < tot; e += blockDim.x, ++cnt) cfma(acc[cnt], sp[e], tn[e]);
+        const double2* sp = spec + (size_t)vsrc[v] * G3;
+        const double2* tn = L.tns + (size_t)voff[v] * G3;
+#pragma unroll
+        for (int q = 0; q < NE; ++q) {
+            int e = threadIdx.x + 256 * q;
+            if (e < G3) cfma(acc[q], __ldg(sp + e), __ldg(tn + e));
+        }
     }
-    cnt = 0;
-    for (int e = threadIdx.x; e < tot; e += blockDim.x, ++cnt) grid[e] = acc[cnt];
+#pragma unroll
+    for (int q = 0; q < NE; ++q) {
+        int e = threadIdx.x + 256 * q;
+        if (e < G3) grid[e] = acc[q];
+    }
     __syncthreads();
-    dft3_smem(grid, G, twb, blockDim.x);
-    const double coef = 1.0 / (double)(G * G * G);
+    for (int e = threadIdx.x; e < G * G * P; e += blockDim.x) {  // z: outputs c' < P
+        int kab = e % (G * G), c = e / (G * G);
+        double2 s = make_double2(0.0, 0.0);
+        for (int kc = 0; kc < G; ++kc) cfma(s, grid[kc * G * G + kab], twb[((P + c) * kc) % G]);
+        c1[e] = s;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < G * PP; e += blockDim.x) {  // y: outputs b' < P
+        int ka = e % G, bb = (e / G) % P, c = e / (G * P);
+        double2 s = make_double2(0.0, 0.0);
+        for (int kb = 0; kb < G; ++kb) cfma(s, c1[(c * G + kb) * G + ka], twb[((P + bb) * kb) % G]);
+        grid[e] = s;  // [c'][b'][ka]
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < PP * P; e += blockDim.x) {  // x: outputs a' < P
+        int a = e % P, line = e / P;
+        double2 s = make_double2(0.0, 0.0);
+        for (int ka = 0; ka < G; ++ka) cfma(s, grid[line * G + ka], twb[((P + a) * ka) % G]);
+        c1[e] = s;  // [c'][b'][a']
+    }
+    __syncthreads();
+    const double coef = 1.0 / (double)G3;
     for (int k = threadIdx.x; k < L.nE; k += blockDim.x) {
-        double2 v = grid[L.grid_idx[k]];
+        double2 v = c1[L.cube_idx[k]];
         double2 o = dnchk[(size_t)t * L.nE + k];
         o.x += v.x * coef;
         o.y += v.y * coef;
@@ -300,26 +359,33 @@ __global__ void vlist_accum_kernel(VlistLevel L, const int* __restrict__ trg, co
     }
 }
 
-void vlist_init(int G) {
-    int sm = (int)(sizeof(double2) * G * G * G);
-    cudaFuncSetAttribute(vlist_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    cudaFuncSetAttribute(vlist_accum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-}
+static size_t vfwd_smem(int G, int P) { return sizeof(double2) * (P * P * P + G * P * P + G * G * P); }
+static size_t vacc_smem(int G, int P) { return sizeof(double2) * (G * G * G + G * G * P); }
 
-static int vlist_threads(int G) { return G * G * G / 16 > 256 ? G * G * G / 16 : 256; }
+void vlist_init(int G) {
+    int P = G / 2;
+    cudaFuncSetAttribute(vlist_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vfwd_smem(G, P));
+    cudaFuncSetAttribute(vlist_accum_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vacc_smem(8, 4));
+    cudaFuncSetAttribute(vlist_accum_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vacc_smem(12, 6));
+    cudaFuncSetAttribute(vlist_accum_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vacc_smem(16, 8));
+}
 
 void launch_vlist_forward(const VlistLevel& L, const int* boxes, int nbox, const double2* upeq, double2* spec,
                           cudaStream_t s) {
     if (nbox == 0) return;
-    size_t sm = sizeof(double2) * L.G * L.G * L.G;
-    vlist_forward_kernel<<<nbox, vlist_threads(L.G), sm, s>>>(L, boxes, upeq, spec, L.twf);
+    vlist_forward_kernel<<<nbox, 256, vfwd_smem(L.G, L.P), s>>>(L, boxes, upeq, spec, L.twf);
 }
 
 void launch_vlist_accum(const VlistLevel& L, const int* trg, int ntrg, const int* vptr, const int* vsrc,
                         const int* voff, const double2* spec, double2* dnchk, cudaStream_t s) {
     if (ntrg == 0) return;
-    size_t sm = sizeof(double2) * L.G * L.G * L.G;
-    vlist_accum_kernel<<<ntrg, vlist_threads(L.G), sm, s>>>(L, trg, vptr, vsrc, voff, spec, dnchk, L.twb);
+    size_t sm = vacc_smem(L.G, L.P);
+    switch (L.G) {
+        case 8: vlist_accum_kernel<8><<<ntrg, 256, sm, s>>>(L, trg, vptr, vsrc, voff, spec, dnchk, L.twb); break;
+        case 12: vlist_accum_kernel<12><<<ntrg, 256, sm, s>>>(L, trg, vptr, vsrc, voff, spec, dnchk, L.twb); break;
+        case 16: vlist_accum_kernel<16><<<ntrg, 256, sm, s>>>(L, trg, vptr, vsrc, voff, spec, dnchk, L.twb); break;
+        default: break;
+    }
 }
 
 // ---------------------------------------------------------------- misc

@@ -67,7 +67,7 @@ void launch_pt(const PtItem* items_dev, int nitems, const PtSrc* srcs_dev, int k
 struct VlistLevel {
     int G, P;
     int nE;                 // equivalent / check points per box
-    const int* grid_idx;    // nE grid indices of the uep (== dcp) nodes
+    const int* cube_idx;    // nE indices of the uep (== dcp) nodes in the P^3 corner cube [P, 2P)^3
     const double2* tns;     // 343 x G^3 FFT'd translation tensors (zero when near)
     const double2* twf;     // G forward twiddles exp(-2 pi i m / G)
     const double2* twb;     // G backward twiddles exp(+2 pi i m / G)

@@ -274,7 +274,7 @@ void Session::build() {
         double W;
         const double *uep, *ucp;
         double2 *up_s, *v, *vT_s, *upT, *tns;
-        int* grid_idx;
+        int* cube_idx;
         int r;
         double2* ue2uc[8];
         double2* de2dc[8];
@@ -346,16 +346,17 @@ void Session::build() {
             for (int e = 0; e < G3; ++e) tns[(size_t)o * G3 + e] = make_double2(t[e].real(), t[e].imag());
         }
         L.tns = upload(tns);
-        std::vector<int> gidx(nE);
+        // (src/wave3d_eval.cpp:626-628,655-657): a = round((x + W/2)/step) + P in [P, 2P)
+        std::vector<int> cidx(nE);
         double step = W / (P - 1);
         for (int k = 0; k < nE; ++k) {
             int a[3];
             for (int d = 0; d < 3; ++d) a[d] = (int)std::round((op.uep.x[3 * k + d] + W / 2) / step) + P;
             for (int d = 0; d < 3; ++d)
-                if (a[d] < 0 || a[d] >= G) throw std::runtime_error("V-list grid index out of range");
-            gidx[k] = a[0] + G * (a[1] + G * a[2]);
+                if (a[d] < P || a[d] >= 2 * P) throw std::runtime_error("V-list grid index outside the corner cube");
+            cidx[k] = (a[0] - P) + P * ((a[1] - P) + P * (a[2] - P));
         }
-        L.grid_idx = upload(gidx);
+        L.cube_idx = upload(cidx);
         L.has_children = false;
         for (int l : kv.second)
             if (!T.boxes[lfbox[l]].terminal()) L.has_children = true;
@@ -919,7 +920,17 @@ void Session::build() {
         {
             std::vector<int> trg, vptr(1, 0), vsrc, voff;
             std::vector<char> is_src(nLF, 0);
-            for (int l : ids) {
+            // targets in Morton order, so blocks in flight share source spectra in L2
+            std::vector<int> mids(ids);
+            auto morton = [&](int l) {
+                const Idx3& x = T.boxes[lfbox[l]].idx;
+                uint64_t m = 0;
+                for (int bit = 0; bit < 21; ++bit)
+                    for (int d = 0; d < 3; ++d) m |= (uint64_t)((x[d] >> bit) & 1) << (3 * bit + d);
+                return m;
+            };
+            std::stable_sort(mids.begin(), mids.end(), [&](int a2, int b2) { return morton(a2) < morton(b2); });
+            for (int l : mids) {
                 const Box& B = T.boxes[lfbox[l]];
                 if (B.vlist.empty()) continue;
                 Pt3 tc = T.center(B);
@@ -939,7 +950,7 @@ void Session::build() {
                 std::vector<int> srcb;
                 for (int l = 0; l < nLF; ++l)
                     if (is_src[l]) srcb.push_back(l);
-                VlistLevel VL{G, P, nE, L.grid_idx, L.tns, d_twf, d_twb};
+                VlistLevel VL{G, P, nE, L.cube_idx, L.tns, d_twf, d_twb};
                 Step f{};
                 f.kind = 2;
                 f.label = "lf_vlist_fft";
