@@ -14,6 +14,7 @@
 #include "session.hpp"
 
 #include <algorithm>
+#include <cstdio>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -115,6 +116,17 @@ void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<
     st.g.mode = mode;
     steps_.push_back(st);
     stats_.gemm_launches++;
+}
+
+const char* Session::width_label(const char* pass, double W) {
+    char buf[64];
+    snprintf(buf, sizeof buf, "%s_w%g", pass, W);
+    for (const std::string& l : label_store_)
+        if (l == buf) return l.c_str();
+    label_store_.reserve(256);  // pointers into the store must stay valid
+    if (label_store_.size() >= 256) return pass;
+    label_store_.push_back(buf);
+    return label_store_.back().c_str();
 }
 
 void Session::add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>& srcs, const char* label) {
@@ -810,7 +822,7 @@ void Session::build() {
                 xo[p].push_back(xoff);
                 yo[p].push_back(u.toff);
             }
-            add_gemm(probs, xo, yo, W == 1.0 ? lf_upeq : hf_upeq, T0, GEMM_ADD, "hf_m2m");
+            add_gemm(probs, xo, yo, W == 1.0 ? lf_upeq : hf_upeq, T0, GEMM_ATOMIC, width_label("hf_m2m", W));
         }
         // w = E2 * (E3 upchkval)   (src/wave3d_eval.cpp:837-849)
         std::map<int, int> cp;
@@ -833,7 +845,7 @@ void Session::build() {
             xa[p].push_back(u.toff);
             ya[p].push_back(u.off);
         }
-        add_gemm(p2, xa, ya, T0, hf_upeq, GEMM_SET, "hf_uc2ue");
+        add_gemm(p2, xa, ya, T0, hf_upeq, GEMM_SET, width_label("hf_uc2ue", W));
     }
 
     // ---------------------------------------------------------------- steps: HF downward
@@ -850,7 +862,7 @@ void Session::build() {
                 const M2LMat& M = m2l_mats[gid];
                 probs.push_back(GemmProblem{dkeep + M.fin, M.r1, M.r1, M.r1, 0, 0});
             }
-            add_gemm(probs, m2l_x[level], m2l_y[level], hf_upeq, hf_dnchk, GEMM_ATOMIC, "hf_m2l");
+            add_gemm(probs, m2l_x[level], m2l_y[level], hf_upeq, hf_dnchk, GEMM_ATOMIC, width_label("hf_m2l", W));
         }
         // t = E2^T u   (dneqnden = E3^T t, src/wave3d_eval.cpp:938-948, src/mlib3d.cpp:246-250)
         std::map<int, int> cp;
@@ -873,7 +885,7 @@ void Session::build() {
             xa[p].push_back(d.off);
             xt[p].push_back(d.toff);
         }
-        add_gemm(p2, xa, xt, hf_dnchk, T1, GEMM_SET, "hf_dc2de");
+        add_gemm(p2, xa, xt, hf_dnchk, T1, GEMM_SET, width_label("hf_dc2de", W));
         // L2L into the children's (pdir) u, or LF dnchkval at W=1 (src/wave3d_eval.cpp:950-991)
         for (int ind = 0; ind < 8; ++ind) {
             std::map<Idx3, int> pid;
@@ -906,7 +918,7 @@ void Session::build() {
                 xo[p].push_back(d.toff);
                 yo[p].push_back(yoff);
             }
-            add_gemm(probs, xo, yo, T1, W == 1.0 ? lf_dnchk : hf_dnchk, GEMM_ATOMIC, "hf_l2l");
+            add_gemm(probs, xo, yo, T1, W == 1.0 ? lf_dnchk : hf_dnchk, GEMM_ATOMIC, width_label("hf_l2l", W));
         }
     }
 

@@ -140,6 +140,8 @@ private:
     std::vector<cudaEvent_t> ev_;
     std::vector<std::pair<int, int> > ev_pending_;  // (step, event index) recorded, not yet read
     std::map<std::string, ProfileEntry> prof_;
+    std::vector<std::string> label_store_;  // per-width pass labels (Step::label points here)
+    const char* width_label(const char* pass, double W);
 };
 
 }  // namespace ddfmm
