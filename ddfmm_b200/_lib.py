@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libddfmm_b200.so")
 EXPORTS = (
     "ddfmm_session_create", "ddfmm_eval", "ddfmm_eval_device", "ddfmm_direct",
     "ddfmm_session_stats", "ddfmm_session_destroy", "ddfmm_last_error", "ddfmm_tree_stats",
-    "ddfmm_profile_enable", "ddfmm_profile_read",
+    "ddfmm_profile_enable", "ddfmm_profile_read", "ddfmm_eval_device_noalloc",
 )
 
 
@@ -65,6 +65,8 @@ def load():
     lib.ddfmm_eval.restype = C.c_int
     lib.ddfmm_eval_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.ddfmm_eval_device.restype = C.c_int
+    lib.ddfmm_eval_device_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ddfmm_eval_device_noalloc.restype = C.c_int
     lib.ddfmm_direct.argtypes = [C.c_void_p, dp, C.POINTER(C.c_int), C.c_int, dp]
     lib.ddfmm_direct.restype = C.c_int
     lib.ddfmm_session_stats.argtypes = [C.c_void_p, C.POINTER(ddfmm_stats)]

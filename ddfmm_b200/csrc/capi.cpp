@@ -15,6 +15,10 @@ struct ddfmm_session {
     ddfmm::Session* impl;
 };
 
+namespace ddfmm {
+double2* noalloc_scratch(size_t* capacity);  // noalloc.cu
+}
+
 namespace {
 thread_local std::string g_err;
 
@@ -30,6 +34,8 @@ int guarded(F&& f) {
         return DDFMM_OK;
     } catch (const std::bad_alloc&) {
         return fail(DDFMM_ENOMEM, "host out of memory");
+    } catch (const std::invalid_argument& e) {
+        return fail(DDFMM_EINVAL, e.what());
     } catch (const std::runtime_error& e) {
         std::string m = e.what();
         if (m.rfind("CUDA error", 0) == 0) {
@@ -102,6 +108,24 @@ int ddfmm_eval_device(ddfmm_session* s, const void* den_dev, void* val_dev, void
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->impl->stream();
         s->impl->eval_device(static_cast<const double2*>(den_dev), static_cast<double2*>(val_dev), st);
     });
+}
+
+int ddfmm_eval_device_noalloc(ddfmm_session* s, const void* den_dev, void* val_dev, void* stream) {
+    if (!s || !s->impl) return fail(DDFMM_EINVAL, "NULL session");
+    if (!den_dev || !val_dev) return fail(DDFMM_EINVAL, "NULL device array");
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) return fail(DDFMM_ECUDA, "cudaGetDevice failed");
+    int rc = guarded([&] {
+        // the scratch address is per device: resolve it on the session's GPU
+        if (cudaSetDevice(s->impl->device()) != cudaSuccess) throw std::runtime_error("CUDA error: cudaSetDevice");
+        size_t cap = 0;
+        double2* spec = ddfmm::noalloc_scratch(&cap);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->impl->stream();
+        s->impl->eval_device_scratch(static_cast<const double2*>(den_dev), static_cast<double2*>(val_dev), st, spec,
+                                     cap);
+    });
+    cudaSetDevice(prev);
+    return rc;
 }
 
 int ddfmm_direct(ddfmm_session* s, const double* den, const int* ids, int nids, double* out) {

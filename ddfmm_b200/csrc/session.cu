@@ -277,6 +277,7 @@ void Session::build() {
     double2* lf_dnchk = dalloc<double2>((size_t)nLF * nE);
     double2* lf_dneq = dalloc<double2>((size_t)nLF * nE);
     double2* lf_spec = dalloc<double2>((size_t)nLF * G3);
+    spectra_elems_ = (size_t)nLF * G3;
     stats_.fft_spectra_bytes = (long long)nLF * G3 * 16;
     zero_at_start_.push_back(Memset{lf_upchk, sizeof(double2) * (size_t)nLF * nE});
     zero_at_start_.push_back(Memset{lf_dnchk, sizeof(double2) * (size_t)nLF * nE});
@@ -1172,6 +1173,44 @@ std::vector<Session::ProfileEntry> Session::profile_read() {
 void Session::eval_device(const double2* den, double2* val, cudaStream_t s) {
     launch_gather_den(den, d_perm_, d_den_sorted_, npts_, s);
     run_steps(s);
+    launch_scatter_val(d_val_sorted_, d_perm_, val, npts_, s);
+    CK(cudaGetLastError());
+}
+
+// A copy of run_steps whose V-list launches use `spec` for the spectra.
+void Session::run_steps_spec(cudaStream_t s, double2* spec) {
+    for (const Memset& m : zero_at_start_) CK(cudaMemsetAsync(m.p, 0, m.bytes, s));
+    for (const Step& st : steps_) {
+        switch (st.kind) {
+            case 0:
+                launch_gemm(st.g.probs, st.g.tiles, st.g.ntiles, st.g.xoff, st.g.yoff, st.g.X, st.g.Y, st.g.mode, s);
+                break;
+            case 1:
+                launch_pt(st.pt.items, st.pt.nitems, st.pt.srcs, prm_.kernel, s);
+                break;
+            case 2:
+                launch_vlist_forward(st.v.L, st.v.src_boxes, st.v.nsrc, st.v.upeq, spec, s);
+                break;
+            case 3:
+                launch_vlist_accum(st.v.L, st.v.trg, st.v.ntrg, st.v.vptr, st.v.vsrc, st.v.voff, spec, st.v.dnchk, s);
+                break;
+            case 4:
+                CK(cudaMemsetAsync(st.ms.p, 0, st.ms.bytes, s));
+                break;
+        }
+    }
+}
+
+void Session::eval_device_scratch(const double2* den, double2* val, cudaStream_t s, double2* spec, size_t capacity) {
+    if (spectra_elems_ > capacity) {
+        char msg[200];
+        snprintf(msg, sizeof msg,
+                 "the session's V-list spectra need %.1f MiB, more than the %.1f MiB of fixed scratch",
+                 spectra_elems_ * sizeof(double2) / 1048576.0, capacity * sizeof(double2) / 1048576.0);
+        throw std::invalid_argument(msg);
+    }
+    launch_gather_den(den, d_perm_, d_den_sorted_, npts_, s);
+    run_steps_spec(s, spec);
     launch_scatter_val(d_val_sorted_, d_perm_, val, npts_, s);
     CK(cudaGetLastError());
 }

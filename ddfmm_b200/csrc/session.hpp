@@ -44,6 +44,10 @@ public:
     // val = G * den at every point; arrays in point-id order, complex128.
     void eval_host(const std::complex<double>* den, std::complex<double>* val);
     void eval_device(const double2* den, double2* val, cudaStream_t s);
+    // Same matvec with the V-list spectra in caller-provided scratch of
+    // `capacity` double2 (must hold spectra_elems()); nothing is allocated.
+    void eval_device_scratch(const double2* den, double2* val, cudaStream_t s, double2* spec, size_t capacity);
+    size_t spectra_elems() const { return spectra_elems_; }
     // FP64 direct sum at the given point ids (Wave3d::check, src/wave3d_check.cpp:22-100)
     void direct_host(const std::complex<double>* den, const int* ids, int nids, std::complex<double>* out);
 
@@ -59,6 +63,7 @@ public:
     std::vector<ProfileEntry> profile_read();
     void profile_reset() { prof_.clear(); }
     int npts() const { return npts_; }
+    int device() const { return prm_.device; }
     cudaStream_t stream() const { return stream_; }
 
 private:
@@ -116,6 +121,7 @@ private:
     void add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>& srcs, const char* label);
     void build();
     void run_steps(cudaStream_t s);
+    void run_steps_spec(cudaStream_t s, double2* spec);
 
     SessionParams prm_;
     int npts_ = 0;
@@ -136,6 +142,7 @@ private:
     double2* d_den_io_ = nullptr;
     double2* d_val_io_ = nullptr;
     std::vector<Memset> zero_at_start_;
+    size_t spectra_elems_ = 0;
     bool profiling_ = false;
     std::vector<cudaEvent_t> ev_;
     std::vector<std::pair<int, int> > ev_pending_;  // (step, event index) recorded, not yet read

@@ -71,6 +71,26 @@ int ddfmm_eval(ddfmm_session* s, const double* den, double* val);
  * own stream.  Returns after enqueueing; the caller synchronises. */
 int ddfmm_eval_device(ddfmm_session* s, const void* den_dev, void* val_dev, void* stream);
 
+/* No counterpart in the reference.  ddfmm_eval_device for callers that must
+ * not allocate device memory per call site, e.g. code that owns a fixed
+ * device-memory budget or records its matvecs into a CUDA graph, where the
+ * per-eval V-list spectra cannot come from a growing pool.  The spectra (one
+ * (2P)^3 complex FFT per low-frequency box) go to one fixed, statically sized
+ * device array of 16 MiB that every GPU loading this library holds until the
+ * process exits; nothing else changes and the call allocates nothing.
+ * Limits and rules:
+ *  - sessions whose spectra exceed 16 MiB (about 2000 low-frequency boxes at
+ *    ACCU 1, 600 at ACCU 2, 250 at ACCU 3) get DDFMM_EINVAL and a message;
+ *  - the first call on each device resolves the array's device address
+ *    (cudaGetSymbolAddress) with that device current: make it before any
+ *    stream capture;
+ *  - every call and every session on a device share the one array: calls
+ *    whose work overlaps on the GPU race (use one stream, or serialise);
+ *  - each call writes every spectrum it reads, so no zeroing is needed and a
+ *    previous call's leftovers are never used.
+ * den_dev / val_dev / stream as in ddfmm_eval_device. */
+int ddfmm_eval_device_noalloc(ddfmm_session* s, const void* den_dev, void* val_dev, void* stream);
+
 /* Wave3d::check's direct sum: out[k] = sum_j G(p_ids[k], p_j) den[j] in
  * FP64 over all points (self pair included, r:=1 when r < 1e-8). */
 int ddfmm_direct(ddfmm_session* s, const double* den, const int* ids, int nids, double* out);
