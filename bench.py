@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--workload", default="large", choices=["large", "medium", "small"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-json", default=None, help="write the per-pass profile here")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form measurement")
     return ap.parse_args()
 
 
@@ -188,6 +189,53 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws):
+    """The mixed-precision form on the same workload: complex64 densities on
+    the device, 3xTF32 translations; reports matvec/s, its error vs the FP64
+    direct sum and latency percentiles."""
+    import torch
+    from ddfmm_b200 import _lib, wave3d
+    (local,) = wave_args
+    t0 = time.perf_counter()
+    m = wave3d.from_workload(w, device=local, precision=_lib.MIXED)
+    setup_s = time.perf_counter() - t0
+    den = w.densities(np.complex64)
+    rng = np.random.default_rng(7)
+    dens = [den] + [(rng.standard_normal(w.N) + 1j * rng.standard_normal(w.N)).astype(np.complex64)
+                    for _ in range(3)]
+    den_d = [torch.from_numpy(np.ascontiguousarray(d).view(np.float32)).to(dev) for d in dens]
+    val_d = torch.empty(2 * w.N, dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+    for i in range(warmup):
+        m.eval_device(den_d[i % 4].data_ptr(), val_d.data_ptr(), sp, c64=True)
+    m.eval_device(den_d[0].data_ptr(), val_d.data_ptr(), sp, c64=True)
+    stream.synchronize()
+    v = val_d.cpu().numpy().view(np.complex64).astype(np.complex128)
+    relerr = m.check(den.astype(np.complex128), v, chk)
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for i in range(steps):
+        with torch.cuda.stream(stream):
+            ev[i][0].record(stream)
+        m.eval_device(den_d[i % 4].data_ptr(), val_d.data_ptr(), sp, c64=True)
+        with torch.cuda.stream(stream):
+            ev[i][1].record(stream)
+    stream.synchronize()
+    lat = np.array([a.elapsed_time(b) for a, b in ev])
+    ms = ev[0][0].elapsed_time(ev[-1][1]) / steps
+    if ws > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    m.close()
+    return {"value": ws * 1e3 / ms, "unit": "matvec/s", "ms_per_step": ms, "dtype": "c64 (3xTF32 translations)",
+            "relerr_vs_fp64_direct": relerr, "setup_s": setup_s,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))}}
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_env()
@@ -301,6 +349,9 @@ def run_ours(args):
             cpu = {"value": mv, "unit": "matvec/s", "cores": 1, "kind": "reference", "sample": sample_desc(ns, w)}
         except Exception as ex:  # the reference binary travels with the tree; report when it does not
             cpu = {"value": None, "unit": "matvec/s", "cores": 1, "kind": "reference", "sample": "unavailable: %s" % ex}
+    mixed = None
+    if not args.no_mixed:
+        mixed = measure_mixed(w, wave_args=(local,), steps=args.steps, warmup=args.warmup, dev=dev, chk=chk, ws=ws)
     if args.profile_json and rank == 0:
         json.dump({"passes": passes, "by_kernel": by_kernel, "stats": st}, open(args.profile_json, "w"), indent=1)
     if rank == 0:
@@ -316,7 +367,7 @@ def run_ours(args):
                 "e2e": {"value": 1.0 / e2e_s, "unit": "matvec/s", "h2d_bytes_per_step": 16 * w.N,
                         "d2h_bytes_per_step": 16 * w.N, "rel_diff_vs_device_path": e2e_relerr},
                 "roofline": roof, "gpu_launches": int(round(launches / args.steps)) * args.steps,
-                "clocks": clocks, "cpu_baseline": cpu, "passes": passes}
+                "clocks": clocks, "cpu_baseline": cpu, "mixed_form": mixed, "passes": passes}
         print(json.dumps(line), flush=True)
     wave.close()
     if ws > 1:

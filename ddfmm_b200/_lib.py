@@ -15,7 +15,9 @@ EXPORTS = (
     "ddfmm_session_create", "ddfmm_eval", "ddfmm_eval_device", "ddfmm_direct",
     "ddfmm_session_stats", "ddfmm_session_destroy", "ddfmm_last_error", "ddfmm_tree_stats",
     "ddfmm_profile_enable", "ddfmm_profile_read", "ddfmm_eval_device_noalloc",
+    "ddfmm_session_create_ex", "ddfmm_eval_c64", "ddfmm_eval_device_c64",
 )
+PLAIN_FP64, MIXED = 0, 1
 
 
 class ddfmm_stats(C.Structure):
@@ -61,6 +63,15 @@ def load():
                                          C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_int,
                                          C.POINTER(C.c_void_p)]
     lib.ddfmm_session_create.restype = C.c_int
+    lib.ddfmm_session_create_ex.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, dp, C.c_int,
+                                            C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_int, C.c_int,
+                                            C.POINTER(C.c_void_p)]
+    lib.ddfmm_session_create_ex.restype = C.c_int
+    fp = C.POINTER(C.c_float)
+    lib.ddfmm_eval_c64.argtypes = [C.c_void_p, fp, fp]
+    lib.ddfmm_eval_c64.restype = C.c_int
+    lib.ddfmm_eval_device_c64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ddfmm_eval_device_c64.restype = C.c_int
     lib.ddfmm_eval.argtypes = [C.c_void_p, dp, dp]
     lib.ddfmm_eval.restype = C.c_int
     lib.ddfmm_eval_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]

@@ -56,6 +56,13 @@ const char* ddfmm_last_error(void) { return g_err.c_str(); }
 int ddfmm_session_create(const double* pos3n, int n, int kernel, int accu, int npq, double K, const double* ctr3,
                          int ptsmax, int maxlevel, int ncell, const char* ld_path, const char* hd_path, int device,
                          ddfmm_session** out) {
+    return ddfmm_session_create_ex(pos3n, n, kernel, accu, npq, K, ctr3, ptsmax, maxlevel, ncell, ld_path, hd_path,
+                                   device, DDFMM_PLAIN_FP64, out);
+}
+
+int ddfmm_session_create_ex(const double* pos3n, int n, int kernel, int accu, int npq, double K, const double* ctr3,
+                            int ptsmax, int maxlevel, int ncell, const char* ld_path, const char* hd_path, int device,
+                            int precision, ddfmm_session** out) {
     if (!out) return fail(DDFMM_EINVAL, "out is NULL");
     *out = nullptr;
     if (!pos3n || n <= 0) return fail(DDFMM_EINVAL, "need n > 0 points");
@@ -66,6 +73,8 @@ int ddfmm_session_create(const double* pos3n, int n, int kernel, int accu, int n
     if (ncell < 1 || (ncell & (ncell - 1)) || K / ncell < 1 - 1e-12)
         return fail(DDFMM_EINVAL, "ncell must be a power of two with K/ncell >= 1");
     if (ptsmax < 1 || maxlevel < 1) return fail(DDFMM_EINVAL, "ptsmax and maxlevel must be positive");
+    if (precision != DDFMM_PLAIN_FP64 && precision != DDFMM_MIXED)
+        return fail(DDFMM_EINVAL, "precision must be DDFMM_PLAIN_FP64 or DDFMM_MIXED");
     if (!ld_path || !hd_path) return fail(DDFMM_EINVAL, "operator file paths are required");
     for (long long i = 0; i < 3LL * n; ++i)
         if (!std::isfinite(pos3n[i])) return fail(DDFMM_EINVAL, "non-finite point coordinate");
@@ -85,6 +94,7 @@ int ddfmm_session_create(const double* pos3n, int n, int kernel, int accu, int n
     p.accu = accu;
     p.kernel = kernel;
     p.device = device;
+    p.precision = precision;
     ddfmm::Session* impl = nullptr;
     int rc = guarded([&] { impl = new ddfmm::Session(pos3n, n, p, ld_path, hd_path); });
     if (rc != DDFMM_OK) return rc;
@@ -107,6 +117,24 @@ int ddfmm_eval_device(ddfmm_session* s, const void* den_dev, void* val_dev, void
     return guarded([&] {
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->impl->stream();
         s->impl->eval_device(static_cast<const double2*>(den_dev), static_cast<double2*>(val_dev), st);
+    });
+}
+
+int ddfmm_eval_c64(ddfmm_session* s, const float* den, float* val) {
+    if (!s || !s->impl) return fail(DDFMM_EINVAL, "NULL session");
+    if (!den || !val) return fail(DDFMM_EINVAL, "NULL density or value array");
+    return guarded([&] {
+        s->impl->eval_host_c64(reinterpret_cast<const std::complex<float>*>(den),
+                               reinterpret_cast<std::complex<float>*>(val));
+    });
+}
+
+int ddfmm_eval_device_c64(ddfmm_session* s, const void* den_dev, void* val_dev, void* stream) {
+    if (!s || !s->impl) return fail(DDFMM_EINVAL, "NULL session");
+    if (!den_dev || !val_dev) return fail(DDFMM_EINVAL, "NULL device array");
+    return guarded([&] {
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->impl->stream();
+        s->impl->eval_device_c64(static_cast<const float2*>(den_dev), static_cast<float2*>(val_dev), st);
     });
 }
 

@@ -79,6 +79,23 @@ void launch_vlist_accum(const VlistLevel& L, const int* trg, int ntrg, const int
                         const int* vsrc, const int* voff, const double2* spec, double2* dnchk,
                         cudaStream_t s);
 
+// mixed-precision form (kernels_mixed.cu): complex FP32 data behind the same
+// descriptors; GemmProblem::A, PtItem::out, PtSrc::den and VlistLevel::tns /
+// twf / twb then point to float2 data.
+enum Precision { PRECISION_FP64 = 0, PRECISION_MIXED = 1 };
+void cgemm_init();
+void launch_cgemm(const GemmProblem* probs_dev, const GemmTile* tiles_dev, int ntiles, const long long* xoff,
+                  const long long* yoff, const void* X, void* Y, int mode, cudaStream_t s);
+void launch_pt32(const PtItem* items_dev, int nitems, const PtSrc* srcs_dev, int kernel, cudaStream_t s);
+void vlist32_init(int G);
+void launch_vlist_forward32(const VlistLevel& L, const int* boxes, int nbox, const void* upeq, void* spec,
+                            cudaStream_t s);
+void launch_vlist_accum32(const VlistLevel& L, const int* trg, int ntrg, const int* vptr, const int* vsrc,
+                          const int* voff, const void* spec, void* dnchk, cudaStream_t s);
+void launch_gather32(const void* den, const int* perm, void* out, int n, int c64, cudaStream_t s);
+void launch_scatter32(const void* in, const int* perm, void* val, int n, int c64, cudaStream_t s);
+void launch_to_c64(const double2* a, float2* b, long long n, cudaStream_t s);
+
 // gather/scatter helpers
 void launch_gather_den(const double2* den, const int* perm, double2* out, int n, cudaStream_t s);
 void launch_scatter_val(const double2* in, const int* perm, double2* val, int n, cudaStream_t s);

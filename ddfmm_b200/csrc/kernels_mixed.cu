@@ -1,0 +1,451 @@
+// Device kernels of the mixed-precision form: complex FP32 storage, FP32
+// accumulation, translations on the tensor cores as 3xTF32 products.
+//
+// 3xTF32: a float x = hi + lo with hi = tf32(x), lo = tf32(x - hi); a product
+// is hi*hi' + hi*lo' + lo*hi' (the lo*lo' term is below FP32 rounding), so
+// three TF32 MMAs reproduce an FP32 product to about FP32 accuracy.
+// Point interactions evaluate the reference kernel (src/kernel3d.cpp:26-107)
+// in FP32 on coordinate differences formed in FP64 (|p_t - p_s| is then
+// exact to FP32 and the phase 2 pi r stays accurate however far from the
+// origin the leaf sits).
+#include "kernels.cuh"
+
+namespace ddfmm {
+
+__device__ __forceinline__ float2 kfun32(double dx, double dy, double dz, int kernel) {
+    float x = (float)dx, y = (float)dy, z = (float)dz;
+    float r2 = x * x + y * y + z * z;
+    if (r2 < 1e-16f) r2 = 1.0f;
+    float r = sqrtf(r2);
+    float s, c;
+    sincospif(2.0f * r, &s, &c);
+    if (kernel == KERNEL_HELM) {
+        float ir = 1.0f / r;
+        return make_float2(c * ir, s * ir);
+    }
+    return make_float2(c, s);
+}
+
+__device__ __forceinline__ void cfma32(float2& acc, float2 a, float2 b) {
+    acc.x = fmaf(a.x, b.x, acc.x);
+    acc.x = fmaf(-a.y, b.y, acc.x);
+    acc.y = fmaf(a.x, b.y, acc.y);
+    acc.y = fmaf(a.y, b.x, acc.y);
+}
+
+// ---------------------------------------------------------------- 3xTF32 complex GEMM
+// Same problem/tile/column conventions as zgemm_kernel (kernels.cuh), data in
+// float2.  Block: 64 rows x 64 columns; warp (wm, wn) owns rows wm*32..+32 (two
+// m16 blocks) and columns wn*16..+16 (two n8 blocks).  K slices of 32 through a
+// 3-stage cp.async pipeline (8-byte copies: operator columns of odd length are
+// only 8-byte aligned).  Operator slice stored [k][row ^ 4*(k & 3)], column
+// slice [col][k] with a 36-element stride: both fragment loads are free of
+// bank conflicts.
+constexpr int CBM = 64, CBN = 64, CBK = 32, CBKP = 36, CSTAGES = 3;
+constexpr int CSTAGE = CBK * CBM + CBN * CBKP;  // float2 per stage
+constexpr int CGEMM_SMEM = CSTAGES * CSTAGE * (int)sizeof(float2);
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int src_bytes) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit32() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait32() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ unsigned tf32(float x) {
+    unsigned r;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void split(float x, unsigned& hi, unsigned& lo) {
+    hi = tf32(x);
+    lo = tf32(x - __uint_as_float(hi));
+}
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+    asm(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(256, 2) cgemm_kernel(const GemmProblem* __restrict__ probs,
+                                                       const GemmTile* __restrict__ tiles,
+                                                       const long long* __restrict__ xoff,
+                                                       const long long* __restrict__ yoff,
+                                                       const float2* __restrict__ X, float2* Y, int mode) {
+    extern __shared__ float2 csm[];
+    __shared__ long long xo[CBN], yo[CBN];
+    const GemmTile t = tiles[blockIdx.x];
+    const GemmProblem p = probs[t.prob];
+    const float2* A = reinterpret_cast<const float2*>(p.A);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, tg = lane & 3, wm = warp >> 2, wn = warp & 3;
+    const int ncol = min(CBN, p.ncol - t.col0);
+    const int rows = min(CBM, p.m - t.row0);
+    const bool active = wm * 32 < rows && wn * 16 < ncol;
+    if (tid < CBN) {
+        xo[tid] = tid < ncol ? xoff[p.col0 + t.col0 + tid] : 0;
+        yo[tid] = tid < ncol ? yoff[p.col0 + t.col0 + tid] : 0;
+    }
+    __syncthreads();
+    auto load = [&](int stage, int k0) {
+        float2* As = csm + stage * CSTAGE;
+        float2* Xs = As + CBK * CBM;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            int e = tid + 256 * q, row = e & 63, kk = e >> 6;
+            int gk = k0 + kk;
+            bool ok = row < rows && gk < p.k;
+            cp_async8(&As[kk * CBM + (row ^ ((kk & 3) << 2))],
+                      ok ? (const void*)(A + (size_t)gk * p.lda + t.row0 + row) : (const void*)A, ok ? 8 : 0);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            int e = tid + 256 * q, kk = e & 31, col = e >> 5;
+            int gk = k0 + kk;
+            bool ok = col < ncol && gk < p.k;
+            cp_async8(&Xs[col * CBKP + kk], ok ? (const void*)(X + xo[col] + gk) : (const void*)X, ok ? 8 : 0);
+        }
+    };
+    float cr[2][2][4], ci[2][2][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) cr[i][j][e] = ci[i][j][e] = 0.f;
+    const int nk = (p.k + CBK - 1) / CBK;
+#pragma unroll
+    for (int s = 0; s < CSTAGES - 1; ++s) {
+        if (s < nk) load(s, s * CBK);
+        cp_async_commit32();
+    }
+    for (int it = 0; it < nk; ++it) {
+        cp_async_wait32<CSTAGES - 2>();
+        __syncthreads();
+        {
+            int nx = it + CSTAGES - 1;
+            if (nx < nk) load(nx % CSTAGES, nx * CBK);
+            cp_async_commit32();
+        }
+        if (active) {
+            const float2* As = csm + (it % CSTAGES) * CSTAGE;
+            const float2* Xs = As + CBK * CBM;
+#pragma unroll
+            for (int ks = 0; ks < CBK / 8; ++ks) {
+                // B fragments (8 x 8, col): b0 = X[col g][k tg], b1 = X[col g][k tg+4]
+                unsigned brh[2][2], brl[2][2], bih[2][2], bil[2][2];
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const float2* xp = Xs + (wn * 16 + j * 8 + g) * CBKP + ks * 8 + tg;
+                    float2 b0 = xp[0], b1 = xp[4];
+                    split(b0.x, brh[j][0], brl[j][0]);
+                    split(b1.x, brh[j][1], brl[j][1]);
+                    split(b0.y, bih[j][0], bil[j][0]);
+                    split(b1.y, bih[j][1], bil[j][1]);
+                }
+                // A fragments (16 x 8, row): rows g, g+8; k tg, tg+4; split re / im / -im into hi, lo
+                unsigned arh[2][4], arl[2][4], aih[2][4], ail[2][4], anh[2][4], anl[2][4];
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const int r = wm * 32 + i * 16 + g;
+                    const int k = ks * 8 + tg;
+                    const int sw = (k & 3) << 2;
+                    float2 a[4] = {As[k * CBM + (r ^ sw)], As[k * CBM + ((r + 8) ^ sw)],
+                                   As[(k + 4) * CBM + (r ^ sw)], As[(k + 4) * CBM + ((r + 8) ^ sw)]};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        split(a[e].x, arh[i][e], arl[i][e]);
+                        split(a[e].y, aih[i][e], ail[i][e]);
+                        anh[i][e] = aih[i][e] ^ 0x80000000u;  // -Ai
+                        anl[i][e] = ail[i][e] ^ 0x80000000u;
+                    }
+                }
+                // Cr += Ar Br - Ai Bi ; Ci += Ar Bi + Ai Br, each product as hi*hi + hi*lo + lo*hi;
+                // every term runs over the four output blocks before the next one
+#define DDFMM_TERM(ACC, AF, BF)                                                    \
+    _Pragma("unroll") for (int i = 0; i < 2; ++i) _Pragma("unroll") for (int j = 0; j < 2; ++j) { \
+        const unsigned bb[2] = {BF[j][0], BF[j][1]};                               \
+        mma_tf32(ACC[i][j], AF[i], bb);                                            \
+    }
+                DDFMM_TERM(cr, arh, brh)
+                DDFMM_TERM(ci, arh, bih)
+                DDFMM_TERM(cr, anh, bih)
+                DDFMM_TERM(ci, aih, brh)
+                DDFMM_TERM(cr, arh, brl)
+                DDFMM_TERM(ci, arh, bil)
+                DDFMM_TERM(cr, anh, bil)
+                DDFMM_TERM(ci, aih, brl)
+                DDFMM_TERM(cr, arl, brh)
+                DDFMM_TERM(ci, arl, bih)
+                DDFMM_TERM(cr, anl, bih)
+                DDFMM_TERM(ci, ail, brh)
+#undef DDFMM_TERM
+            }
+        }
+    }
+    cp_async_wait32<0>();
+    if (!active) return;
+    // C fragment (16 x 8): c0 = C[g][2tg], c1 = C[g][2tg+1], c2 = C[g+8][2tg], c3 = C[g+8][2tg+1]
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                int row = wm * 32 + i * 16 + g + (e >> 1) * 8;
+                int col = wn * 16 + j * 8 + 2 * tg + (e & 1);
+                if (row >= rows || col >= ncol) continue;
+                float2* y = Y + yo[col] + t.row0 + row;
+                float2 v = make_float2(cr[i][j][e], ci[i][j][e]);
+                if (mode == GEMM_SET) {
+                    *y = v;
+                } else if (mode == GEMM_ADD) {
+                    float2 o = *y;
+                    *y = make_float2(o.x + v.x, o.y + v.y);
+                } else {
+                    atomicAdd(&y->x, v.x);
+                    atomicAdd(&y->y, v.y);
+                }
+            }
+}
+
+void cgemm_init() { cudaFuncSetAttribute(cgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CGEMM_SMEM); }
+
+void launch_cgemm(const GemmProblem* probs, const GemmTile* tiles, int ntiles, const long long* xoff,
+                  const long long* yoff, const void* X, void* Y, int mode, cudaStream_t s) {
+    if (ntiles == 0) return;
+    cgemm_kernel<<<ntiles, 256, CGEMM_SMEM, s>>>(probs, tiles, xoff, yoff, static_cast<const float2*>(X),
+                                                  static_cast<float2*>(Y), mode);
+}
+
+// ---------------------------------------------------------------- points (FP32)
+// One warp per item as pt_kernel; densities / outputs are float2 (the
+// descriptors' double2 pointers are reinterpreted).  Differences of the FP64
+// coordinates are taken in FP64, the kernel is evaluated in FP32.
+__global__ void pt32_kernel(const PtItem* __restrict__ items, int nitems, const PtSrc* __restrict__ srcs,
+                            int kernel) {
+    int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= nitems) return;
+    const PtItem it = items[w];
+    float2* out = reinterpret_cast<float2*>(it.out);
+    for (int t = lane; t < it.trg.n; t += 32) {
+        const double* tp = it.trg.x + 3 * t;
+        double tx = it.trg.scale * tp[0] + it.trg.shift[0];
+        double ty = it.trg.scale * tp[1] + it.trg.shift[1];
+        double tz = it.trg.scale * tp[2] + it.trg.shift[2];
+        float2 acc = make_float2(0.f, 0.f);
+        for (int s = it.src_begin; s < it.src_end; ++s) {
+            const PtSrc S = srcs[s];
+            const float2* den = reinterpret_cast<const float2*>(S.den);
+            for (int q = 0; q < S.src.n; ++q) {
+                const double* sp = S.src.x + 3 * q;
+                double sx = S.src.scale * sp[0] + S.src.shift[0];
+                double sy = S.src.scale * sp[1] + S.src.shift[1];
+                double sz = S.src.scale * sp[2] + S.src.shift[2];
+                cfma32(acc, kfun32(tx - sx, ty - sy, tz - sz, kernel), den[q]);
+            }
+        }
+        float2 o = out[t];
+        out[t] = make_float2(o.x + acc.x, o.y + acc.y);
+    }
+}
+
+void launch_pt32(const PtItem* items, int nitems, const PtSrc* srcs, int kernel, cudaStream_t s) {
+    if (nitems == 0) return;
+    pt32_kernel<<<(nitems * 32 + 255) / 256, 256, 0, s>>>(items, nitems, srcs, kernel);
+}
+
+// ---------------------------------------------------------------- V list (FP32)
+// The pruned corner-cube transforms of kernels.cu in complex FP32.
+__global__ void vlist_forward32_kernel(VlistLevel L, const int* __restrict__ boxes, const float2* __restrict__ upeq,
+                                       float2* __restrict__ spec, const float2* __restrict__ twf) {
+    extern __shared__ float2 sm32[];
+    const int G = L.G, P = L.P, PP = P * P;
+    float2* cube = sm32;
+    float2* b1 = cube + PP * P;
+    float2* b2 = b1 + G * PP;
+    const int b = boxes[blockIdx.x];
+    for (int e = threadIdx.x; e < PP * P; e += blockDim.x) cube[e] = make_float2(0.f, 0.f);
+    __syncthreads();
+    for (int k = threadIdx.x; k < L.nE; k += blockDim.x) cube[L.cube_idx[k]] = upeq[(size_t)b * L.nE + k];
+    __syncthreads();
+    for (int e = threadIdx.x; e < G * PP; e += blockDim.x) {
+        int ka = e % G, line = e / G;
+        float2 acc = make_float2(0.f, 0.f);
+        for (int a = 0; a < P; ++a) cfma32(acc, cube[line * P + a], twf[((P + a) * ka) % G]);
+        b1[e] = acc;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < G * G * P; e += blockDim.x) {
+        int ka = e % G, kb = (e / G) % G, c = e / (G * G);
+        float2 acc = make_float2(0.f, 0.f);
+        for (int bb = 0; bb < P; ++bb) cfma32(acc, b1[(c * P + bb) * G + ka], twf[((P + bb) * kb) % G]);
+        b2[e] = acc;
+    }
+    __syncthreads();
+    float2* o = spec + (size_t)b * G * G * G;
+    for (int e = threadIdx.x; e < G * G * G; e += blockDim.x) {
+        int kab = e % (G * G), kc = e / (G * G);
+        float2 acc = make_float2(0.f, 0.f);
+        for (int c = 0; c < P; ++c) cfma32(acc, b2[c * G * G + kab], twf[((P + c) * kc) % G]);
+        o[e] = acc;
+    }
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) vlist_accum32_kernel(VlistLevel L, const int* __restrict__ trg,
+                                                            const int* __restrict__ vptr,
+                                                            const int* __restrict__ vsrc,
+                                                            const int* __restrict__ voff,
+                                                            const float2* __restrict__ spec,
+                                                            float2* __restrict__ dnchk,
+                                                            const float2* __restrict__ twb) {
+    extern __shared__ float2 sm32[];
+    constexpr int P = G / 2, PP = P * P, G3 = G * G * G, NE = (G3 + 255) / 256;
+    float2* grid = sm32;
+    float2* c1 = sm32 + G3;
+    const float2* tns = reinterpret_cast<const float2*>(L.tns);
+    const int ti = blockIdx.x, t = trg[ti];
+    float2 acc[NE];
+#pragma unroll
+    for (int q = 0; q < NE; ++q) acc[q] = make_float2(0.f, 0.f);
+    for (int v = vptr[ti]; v < vptr[ti + 1]; ++v) {
+        const float2* sp = spec + (size_t)vsrc[v] * G3;
+        const float2* tn = tns + (size_t)voff[v] * G3;
+#pragma unroll
+        for (int q = 0; q < NE; ++q) {
+            int e = threadIdx.x + 256 * q;
+            if (e < G3) cfma32(acc[q], __ldg(sp + e), __ldg(tn + e));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NE; ++q) {
+        int e = threadIdx.x + 256 * q;
+        if (e < G3) grid[e] = acc[q];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < G * G * P; e += blockDim.x) {
+        int kab = e % (G * G), c = e / (G * G);
+        float2 s = make_float2(0.f, 0.f);
+        for (int kc = 0; kc < G; ++kc) cfma32(s, grid[kc * G * G + kab], twb[((P + c) * kc) % G]);
+        c1[e] = s;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < G * PP; e += blockDim.x) {
+        int ka = e % G, bb = (e / G) % P, c = e / (G * P);
+        float2 s = make_float2(0.f, 0.f);
+        for (int kb = 0; kb < G; ++kb) cfma32(s, c1[(c * G + kb) * G + ka], twb[((P + bb) * kb) % G]);
+        grid[e] = s;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < PP * P; e += blockDim.x) {
+        int a = e % P, line = e / P;
+        float2 s = make_float2(0.f, 0.f);
+        for (int ka = 0; ka < G; ++ka) cfma32(s, grid[line * G + ka], twb[((P + a) * ka) % G]);
+        c1[e] = s;
+    }
+    __syncthreads();
+    const float coef = 1.0f / (float)G3;
+    for (int k = threadIdx.x; k < L.nE; k += blockDim.x) {
+        float2 v = c1[L.cube_idx[k]];
+        float2 o = dnchk[(size_t)t * L.nE + k];
+        dnchk[(size_t)t * L.nE + k] = make_float2(o.x + v.x * coef, o.y + v.y * coef);
+    }
+}
+
+static size_t vfwd32_smem(int G, int P) { return sizeof(float2) * (P * P * P + G * P * P + G * G * P); }
+static size_t vacc32_smem(int G, int P) { return sizeof(float2) * (G * G * G + G * G * P); }
+
+void vlist32_init(int G) {
+    int P = G / 2;
+    cudaFuncSetAttribute(vlist_forward32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vfwd32_smem(G, P));
+    cudaFuncSetAttribute(vlist_accum32_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vacc32_smem(8, 4));
+    cudaFuncSetAttribute(vlist_accum32_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)vacc32_smem(12, 6));
+    cudaFuncSetAttribute(vlist_accum32_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)vacc32_smem(16, 8));
+}
+
+// L.tns, L.twf, L.twb hold float2 data in this form.
+void launch_vlist_forward32(const VlistLevel& L, const int* boxes, int nbox, const void* upeq, void* spec,
+                            cudaStream_t s) {
+    if (nbox == 0) return;
+    vlist_forward32_kernel<<<nbox, 256, vfwd32_smem(L.G, L.P), s>>>(
+        L, boxes, static_cast<const float2*>(upeq), static_cast<float2*>(spec),
+        reinterpret_cast<const float2*>(L.twf));
+}
+
+void launch_vlist_accum32(const VlistLevel& L, const int* trg, int ntrg, const int* vptr, const int* vsrc,
+                          const int* voff, const void* spec, void* dnchk, cudaStream_t s) {
+    if (ntrg == 0) return;
+    size_t sm = vacc32_smem(L.G, L.P);
+    const float2* sp = static_cast<const float2*>(spec);
+    float2* dn = static_cast<float2*>(dnchk);
+    const float2* tw = reinterpret_cast<const float2*>(L.twb);
+    switch (L.G) {
+        case 8: vlist_accum32_kernel<8><<<ntrg, 256, sm, s>>>(L, trg, vptr, vsrc, voff, sp, dn, tw); break;
+        case 12: vlist_accum32_kernel<12><<<ntrg, 256, sm, s>>>(L, trg, vptr, vsrc, voff, sp, dn, tw); break;
+        case 16: vlist_accum32_kernel<16><<<ntrg, 256, sm, s>>>(L, trg, vptr, vsrc, voff, sp, dn, tw); break;
+        default: break;
+    }
+}
+
+// ---------------------------------------------------------------- conversions
+__global__ void gather32_kernel(const double2* __restrict__ den, const int* __restrict__ perm,
+                                float2* __restrict__ out, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        double2 v = den[perm[i]];
+        out[i] = make_float2((float)v.x, (float)v.y);
+    }
+}
+__global__ void gather32c_kernel(const float2* __restrict__ den, const int* __restrict__ perm,
+                                 float2* __restrict__ out, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = den[perm[i]];
+}
+__global__ void scatter32_kernel(const float2* __restrict__ in, const int* __restrict__ perm,
+                                 double2* __restrict__ val, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        float2 v = in[i];
+        val[perm[i]] = make_double2(v.x, v.y);
+    }
+}
+__global__ void scatter32c_kernel(const float2* __restrict__ in, const int* __restrict__ perm,
+                                  float2* __restrict__ val, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) val[perm[i]] = in[i];
+}
+// den / val are complex128 (c64 = 0) or complex64 (c64 = 1) arrays in point-id order
+void launch_gather32(const void* den, const int* perm, void* out, int n, int c64, cudaStream_t s) {
+    if (n <= 0) return;
+    if (c64)
+        gather32c_kernel<<<(n + 255) / 256, 256, 0, s>>>(static_cast<const float2*>(den), perm,
+                                                         static_cast<float2*>(out), n);
+    else
+        gather32_kernel<<<(n + 255) / 256, 256, 0, s>>>(static_cast<const double2*>(den), perm,
+                                                        static_cast<float2*>(out), n);
+}
+void launch_scatter32(const void* in, const int* perm, void* val, int n, int c64, cudaStream_t s) {
+    if (n <= 0) return;
+    if (c64)
+        scatter32c_kernel<<<(n + 255) / 256, 256, 0, s>>>(static_cast<const float2*>(in), perm,
+                                                          static_cast<float2*>(val), n);
+    else
+        scatter32_kernel<<<(n + 255) / 256, 256, 0, s>>>(static_cast<const float2*>(in), perm,
+                                                         static_cast<double2*>(val), n);
+}
+
+__global__ void to_c64_kernel(const double2* __restrict__ a, float2* __restrict__ b, long long n) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = make_float2((float)a[i].x, (float)a[i].y);
+}
+void launch_to_c64(const double2* a, float2* b, long long n, cudaStream_t s) {
+    if (n > 0) to_c64_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, b, n);
+}
+
+}  // namespace ddfmm

@@ -229,6 +229,23 @@ void Session::build() {
     const int nE = P * P * P - (P - 2) * (P - 2) * (P - 2);
     const int kern = prm_.kernel;
     if (kern != KERNEL_HELM && kern != KERNEL_EXPR) throw std::runtime_error("unknown kernel type");
+    // complex state: double2 (plain FP64 form) or float2 (mixed form); plan
+    // offsets are in elements, so both forms share one plan
+    const bool mixed = prm_.precision == PRECISION_MIXED;
+    const size_t es = mixed ? sizeof(float2) : sizeof(double2);
+    auto E = [&](double2* base, size_t elems) { return (double2*)((char*)base + elems * es); };
+    auto salloc = [&](size_t elems) { return (double2*)dalloc<char>(elems * es); };
+    // operators are built in FP64; the mixed form multiplies with FP32 copies
+    std::map<const double2*, const double2*> op32;
+    auto opm = [&](const double2* a, size_t n) -> const double2* {
+        if (!mixed) return a;
+        auto it = op32.find(a);
+        if (it != op32.end()) return it->second;
+        float2* b = dalloc<float2>(n);
+        launch_to_c64(a, b, (long long)n, stream_);
+        CK(cudaGetLastError());
+        return op32[a] = (const double2*)b;
+    };
     Tree& T = tree_;
     const int nb = (int)T.boxes.size();
     stats_.n_points = npts_;
@@ -262,25 +279,25 @@ void Session::build() {
     d_perm_ = upload(perm);
     d_pos_ids_ = upload(pos_);
     d_pos_sorted_ = upload(pos_sorted);
-    d_den_sorted_ = dalloc<double2>(npts_);
-    d_val_sorted_ = dalloc<double2>(npts_);
+    d_den_sorted_ = salloc(npts_);
+    d_val_sorted_ = salloc(npts_);
     d_den_io_ = dalloc<double2>(npts_);
     d_val_io_ = dalloc<double2>(npts_);
-    zero_at_start_.push_back(Memset{d_val_sorted_, sizeof(double2) * npts_});
+    zero_at_start_.push_back(Memset{d_val_sorted_, es * npts_});
 
     std::map<int, std::vector<int> > lflevels;  // level -> lf ids (key order)
     for (int l = 0; l < nLF; ++l) lflevels[T.boxes[lfbox[l]].level].push_back(l);
 
-    double2* lf_upeq = dalloc<double2>((size_t)nLF * nE);
-    double2* lf_upchk = dalloc<double2>((size_t)nLF * nE);
-    double2* lf_mid = dalloc<double2>((size_t)nLF * nE);
-    double2* lf_dnchk = dalloc<double2>((size_t)nLF * nE);
-    double2* lf_dneq = dalloc<double2>((size_t)nLF * nE);
-    double2* lf_spec = dalloc<double2>((size_t)nLF * G3);
+    double2* lf_upeq = salloc((size_t)nLF * nE);
+    double2* lf_upchk = salloc((size_t)nLF * nE);
+    double2* lf_mid = salloc((size_t)nLF * nE);
+    double2* lf_dnchk = salloc((size_t)nLF * nE);
+    double2* lf_dneq = salloc((size_t)nLF * nE);
+    double2* lf_spec = salloc((size_t)nLF * G3);
     spectra_elems_ = (size_t)nLF * G3;
     stats_.fft_spectra_bytes = (long long)nLF * G3 * 16;
-    zero_at_start_.push_back(Memset{lf_upchk, sizeof(double2) * (size_t)nLF * nE});
-    zero_at_start_.push_back(Memset{lf_dnchk, sizeof(double2) * (size_t)nLF * nE});
+    zero_at_start_.push_back(Memset{lf_upchk, es * (size_t)nLF * nE});
+    zero_at_start_.push_back(Memset{lf_dnchk, es * (size_t)nLF * nE});
 
     // per-LF-level device operators
     struct LfLevelOps {
@@ -321,10 +338,12 @@ void Session::build() {
             twb[m] = make_double2((double)cosl(a), (double)sinl(a));
         }
     }
-    double2* d_twf = upload(twf);
-    double2* d_twb = upload(twb);
+    const double2* d_twf = opm(upload(twf), G);
+    const double2* d_twb = opm(upload(twb), G);
     vlist_init(G);
     gemm_init();
+    vlist32_init(G);
+    cgemm_init();
 
     for (auto& kv : lflevels) {
         int level = kv.first;
@@ -358,7 +377,7 @@ void Session::build() {
             if (t.empty()) continue;
             for (int e = 0; e < G3; ++e) tns[(size_t)o * G3 + e] = make_double2(t[e].real(), t[e].imag());
         }
-        L.tns = upload(tns);
+        L.tns = (double2*)opm(upload(tns), tns.size());
         // (src/wave3d_eval.cpp:626-628,655-657): a = round((x + W/2)/step) + P in [P, 2P)
         std::vector<int> cidx(nE);
         double step = W / (P - 1);
@@ -497,11 +516,11 @@ void Session::build() {
     }
     stats_.hf_up_nodes = (long long)up.size();
     stats_.hf_down_nodes = (long long)dn.size();
-    double2* hf_upeq = dalloc<double2>((size_t)upeq_total);
-    double2* hf_dnchk = dalloc<double2>((size_t)dnchk_total);
-    double2* T0 = dalloc<double2>((size_t)tmp_max);
-    double2* T1 = dalloc<double2>((size_t)tmp_max);
-    zero_at_start_.push_back(Memset{hf_dnchk, sizeof(double2) * (size_t)dnchk_total});
+    double2* hf_upeq = salloc((size_t)upeq_total);
+    double2* hf_dnchk = salloc((size_t)dnchk_total);
+    double2* T0 = salloc((size_t)tmp_max);
+    double2* T1 = salloc((size_t)tmp_max);
+    zero_at_start_.push_back(Memset{hf_dnchk, es * (size_t)dnchk_total});
 
     // ---------------------------------------------------------------- HF operators
     // Raw kernel matrices -- M2M ue2uc and L2L de2dc per (W, wedge, child), M2L per
@@ -720,6 +739,8 @@ void Session::build() {
         CK(cudaStreamSynchronize(stream_));
         CK(cudaFree(dscr));
     }
+    const double2* dkeepm = opm(dkeep, keep);
+    auto KP = [&](size_t off) { return E((double2*)dkeepm, off); };
 
     // ---------------------------------------------------------------- steps: LF upward
     auto lf_set = [&](const double* x, int n, Pt3 shift, double scale) {
@@ -748,9 +769,9 @@ void Session::build() {
             if (!B.terminal()) continue;
             PtItem itm;
             itm.trg = lf_set(L.ucp, nE, T.center(B), 1.0);
-            itm.out = lf_upchk + (size_t)l * nE;
+            itm.out = E(lf_upchk, (size_t)l * nE);
             itm.src_begin = (int)srcs.size();
-            srcs.push_back(PtSrc{leaf_set(l), d_den_sorted_ + leaf_off[l]});
+            srcs.push_back(PtSrc{leaf_set(l), E(d_den_sorted_, leaf_off[l])});
             itm.src_end = (int)srcs.size();
             items.push_back(itm);
         }
@@ -767,7 +788,8 @@ void Session::build() {
                     x.push_back((long long)lfidx[c] * nE);
                     y.push_back((long long)l * nE);
                 }
-                single(GemmProblem{L.ue2uc[ind], nE, nE, nE, 0, 0}, x, y, lf_upeq, lf_upchk, GEMM_ADD, "lf_m2m");
+                single(GemmProblem{opm(L.ue2uc[ind], (size_t)nE * nE), nE, nE, nE, 0, 0}, x, y, lf_upeq, lf_upchk, GEMM_ADD,
+                       "lf_m2m");
             }
         // upeqnden = v * (1/sigma .* (U^H * upchk))   (src/wave3d_eval.cpp:466-478)
         std::vector<long long> a, b2;
@@ -775,8 +797,10 @@ void Session::build() {
             a.push_back((long long)l * nE);
             b2.push_back((long long)l * nE);
         }
-        single(GemmProblem{L.up_s, L.r, nE, L.r, 0, 0}, a, b2, lf_upchk, lf_mid, GEMM_SET, "lf_uc2ue");
-        single(GemmProblem{L.v, nE, L.r, nE, 0, 0}, a, b2, lf_mid, lf_upeq, GEMM_SET, "lf_uc2ue");
+        single(GemmProblem{opm(L.up_s, (size_t)L.r * nE), L.r, nE, L.r, 0, 0}, a, b2, lf_upchk, lf_mid, GEMM_SET,
+               "lf_uc2ue");
+        single(GemmProblem{opm(L.v, (size_t)L.r * nE), nE, L.r, nE, 0, 0}, a, b2, lf_mid, lf_upeq, GEMM_SET,
+               "lf_uc2ue");
     }
 
     // ---------------------------------------------------------------- steps: HF upward
@@ -789,7 +813,7 @@ void Session::build() {
         Step ms{};
         ms.kind = 4;
         ms.label = "memset";
-        ms.ms = Memset{T0, sizeof(double2) * (size_t)tmp_max};
+        ms.ms = Memset{T0, es * (size_t)tmp_max};
         steps_.push_back(ms);
         // M2M: E3 upchkval = sum_children [E3 ue2uc E1(child)] w_child (src/wave3d_eval.cpp:796-834)
         for (int ind = 0; ind < 8; ++ind) {
@@ -814,7 +838,7 @@ void Session::build() {
                     const DirMats& M = m2m_mats.at(std::make_pair(W, u.dir));
                     p = (int)probs.size();
                     pid[u.dir] = p;
-                    probs.push_back(GemmProblem{dkeep + M.fin[ind], M.mrows, M.mcols, M.mrows, 0, 0});
+                    probs.push_back(GemmProblem{KP(M.fin[ind]), M.mrows, M.mcols, M.mrows, 0, 0});
                     xo.emplace_back();
                     yo.emplace_back();
                 } else {
@@ -837,7 +861,7 @@ void Session::build() {
                 const Canon& c = hfcanon[u.canon];
                 p = (int)p2.size();
                 cp[u.canon] = p;
-                p2.push_back(GemmProblem{c.E2, c.r1, c.r2, c.r1, 0, 0});
+                p2.push_back(GemmProblem{opm(c.E2, (size_t)c.r1 * c.r2), c.r1, c.r2, c.r1, 0, 0});
                 xa.emplace_back();
                 ya.emplace_back();
             } else {
@@ -861,7 +885,7 @@ void Session::build() {
             std::vector<GemmProblem> probs;
             for (int gid : m2l_probs[level]) {
                 const M2LMat& M = m2l_mats[gid];
-                probs.push_back(GemmProblem{dkeep + M.fin, M.r1, M.r1, M.r1, 0, 0});
+                probs.push_back(GemmProblem{KP(M.fin), M.r1, M.r1, M.r1, 0, 0});
             }
             add_gemm(probs, m2l_x[level], m2l_y[level], hf_upeq, hf_dnchk, GEMM_ATOMIC, width_label("hf_m2l", W));
         }
@@ -877,7 +901,7 @@ void Session::build() {
                 const Canon& c = hfcanon[d.canon];
                 p = (int)p2.size();
                 cp[d.canon] = p;
-                p2.push_back(GemmProblem{c.E2t, c.r2, c.r1, c.r2, 0, 0});
+                p2.push_back(GemmProblem{opm(c.E2t, (size_t)c.r1 * c.r2), c.r2, c.r1, c.r2, 0, 0});
                 xa.emplace_back();
                 xt.emplace_back();
             } else {
@@ -910,7 +934,7 @@ void Session::build() {
                     const DirMats& M = l2l_mats.at(std::make_pair(W, d.dir));
                     p = (int)probs.size();
                     pid[d.dir] = p;
-                    probs.push_back(GemmProblem{dkeep + M.fin[ind], M.mrows, M.mcols, M.mrows, 0, 0});
+                    probs.push_back(GemmProblem{KP(M.fin[ind]), M.mrows, M.mcols, M.mrows, 0, 0});
                     xo.emplace_back();
                     yo.emplace_back();
                 } else {
@@ -963,7 +987,7 @@ void Session::build() {
                 std::vector<int> srcb;
                 for (int l = 0; l < nLF; ++l)
                     if (is_src[l]) srcb.push_back(l);
-                VlistLevel VL{G, P, nE, L.cube_idx, L.tns, d_twf, d_twb};
+                VlistLevel VL{G, P, nE, L.cube_idx, L.tns, d_twf, d_twb};  // FP32 data in the mixed form
                 Step f{};
                 f.kind = 2;
                 f.label = "lf_vlist_fft";
@@ -1002,12 +1026,12 @@ void Session::build() {
                 bool direct = B.terminal() && leaf_cnt[l] < nE;
                 PtItem itm;
                 itm.trg = direct ? leaf_set(l) : lf_set(L.uep, nE, T.center(B), 1.0);
-                itm.out = direct ? d_val_sorted_ + leaf_off[l] : lf_dnchk + (size_t)l * nE;
+                itm.out = direct ? E(d_val_sorted_, leaf_off[l]) : E(lf_dnchk, (size_t)l * nE);
                 auto& S = direct ? srcsA : srcsB;
                 itm.src_begin = (int)S.size();
                 for (int s : B.xlist) {
                     int ls = lfidx[s];
-                    S.push_back(PtSrc{leaf_set(ls), d_den_sorted_ + leaf_off[ls]});
+                    S.push_back(PtSrc{leaf_set(ls), E(d_den_sorted_, leaf_off[ls])});
                     stats_.x_pairs++;
                 }
                 itm.src_end = (int)S.size();
@@ -1025,11 +1049,11 @@ void Session::build() {
                 if (!B.ulist.empty()) {
                     PtItem itm;
                     itm.trg = leaf_set(l);
-                    itm.out = d_val_sorted_ + leaf_off[l];
+                    itm.out = E(d_val_sorted_, leaf_off[l]);
                     itm.src_begin = (int)srcs.size();
                     for (int s : B.ulist) {
                         int ls = lfidx[s];
-                        srcs.push_back(PtSrc{leaf_set(ls), d_den_sorted_ + leaf_off[ls]});
+                        srcs.push_back(PtSrc{leaf_set(ls), E(d_den_sorted_, leaf_off[ls])});
                         stats_.u_pairs++;
                         stats_.u_interactions += (long long)leaf_cnt[l] * leaf_cnt[ls];
                     }
@@ -1039,16 +1063,16 @@ void Session::build() {
                 if (!B.wlist.empty()) {
                     PtItem itm;
                     itm.trg = leaf_set(l);
-                    itm.out = d_val_sorted_ + leaf_off[l];
+                    itm.out = E(d_val_sorted_, leaf_off[l]);
                     itm.src_begin = (int)wsrcs.size();
                     for (int s : B.wlist) {
                         int ls = lfidx[s];
                         const Box& SB = T.boxes[s];
                         if (SB.terminal() && leaf_cnt[ls] < nE) {
-                            wsrcs.push_back(PtSrc{leaf_set(ls), d_den_sorted_ + leaf_off[ls]});
+                            wsrcs.push_back(PtSrc{leaf_set(ls), E(d_den_sorted_, leaf_off[ls])});
                         } else {
                             double coef = T.width(SB.level) / W;
-                            wsrcs.push_back(PtSrc{lf_set(L.uep, nE, T.center(SB), coef), lf_upeq + (size_t)ls * nE});
+                            wsrcs.push_back(PtSrc{lf_set(L.uep, nE, T.center(SB), coef), E(lf_upeq, (size_t)ls * nE)});
                         }
                         stats_.w_pairs++;
                     }
@@ -1062,8 +1086,10 @@ void Session::build() {
         // dneqnden = up^T (1/sigma .* (v^T dnchk))   (src/wave3d_eval.cpp:536-547, src/mlib3d.cpp:147-152)
         std::vector<long long> a;
         for (int l : ids) a.push_back((long long)l * nE);
-        single(GemmProblem{L.vT_s, L.r, nE, L.r, 0, 0}, a, a, lf_dnchk, lf_mid, GEMM_SET, "lf_dc2de");
-        single(GemmProblem{L.upT, nE, L.r, nE, 0, 0}, a, a, lf_mid, lf_dneq, GEMM_SET, "lf_dc2de");
+        single(GemmProblem{opm(L.vT_s, (size_t)L.r * nE), L.r, nE, L.r, 0, 0}, a, a, lf_dnchk, lf_mid, GEMM_SET,
+               "lf_dc2de");
+        single(GemmProblem{opm(L.upT, (size_t)L.r * nE), nE, L.r, nE, 0, 0}, a, a, lf_mid, lf_dneq, GEMM_SET,
+               "lf_dc2de");
         // L2T at leaves (src/wave3d_eval.cpp:550-560)
         {
             std::vector<PtItem> items;
@@ -1073,9 +1099,9 @@ void Session::build() {
                 if (!B.terminal()) continue;
                 PtItem itm;
                 itm.trg = leaf_set(l);
-                itm.out = d_val_sorted_ + leaf_off[l];
+                itm.out = E(d_val_sorted_, leaf_off[l]);
                 itm.src_begin = (int)srcs.size();
-                srcs.push_back(PtSrc{lf_set(L.ucp, nE, T.center(B), 1.0), lf_dneq + (size_t)l * nE});
+                srcs.push_back(PtSrc{lf_set(L.ucp, nE, T.center(B), 1.0), E(lf_dneq, (size_t)l * nE)});
                 itm.src_end = (int)srcs.size();
                 items.push_back(itm);
             }
@@ -1093,7 +1119,8 @@ void Session::build() {
                     x.push_back((long long)l * nE);
                     y.push_back((long long)lfidx[c] * nE);
                 }
-                single(GemmProblem{L.de2dc[ind], nE, nE, nE, 0, 0}, x, y, lf_dneq, lf_dnchk, GEMM_ADD, "lf_l2l");
+                single(GemmProblem{opm(L.de2dc[ind], (size_t)nE * nE), nE, nE, nE, 0, 0}, x, y, lf_dneq, lf_dnchk, GEMM_ADD,
+                       "lf_l2l");
             }
     }
     stats_.kernel_launches = (long long)steps_.size() + 2;
@@ -1109,6 +1136,39 @@ static const char* kernel_name(int kind) {
     }
 }
 
+void Session::launch_step(const Step& st, cudaStream_t s, double2* spec) {
+    const bool m = mixed();
+    switch (st.kind) {
+        case 0:
+            if (m)
+                launch_cgemm(st.g.probs, st.g.tiles, st.g.ntiles, st.g.xoff, st.g.yoff, st.g.X, st.g.Y, st.g.mode, s);
+            else
+                launch_gemm(st.g.probs, st.g.tiles, st.g.ntiles, st.g.xoff, st.g.yoff, st.g.X, st.g.Y, st.g.mode, s);
+            break;
+        case 1:
+            if (m)
+                launch_pt32(st.pt.items, st.pt.nitems, st.pt.srcs, prm_.kernel, s);
+            else
+                launch_pt(st.pt.items, st.pt.nitems, st.pt.srcs, prm_.kernel, s);
+            break;
+        case 2:
+            if (m)
+                launch_vlist_forward32(st.v.L, st.v.src_boxes, st.v.nsrc, st.v.upeq, spec, s);
+            else
+                launch_vlist_forward(st.v.L, st.v.src_boxes, st.v.nsrc, st.v.upeq, spec, s);
+            break;
+        case 3:
+            if (m)
+                launch_vlist_accum32(st.v.L, st.v.trg, st.v.ntrg, st.v.vptr, st.v.vsrc, st.v.voff, spec, st.v.dnchk, s);
+            else
+                launch_vlist_accum(st.v.L, st.v.trg, st.v.ntrg, st.v.vptr, st.v.vsrc, st.v.voff, spec, st.v.dnchk, s);
+            break;
+        case 4:
+            CK(cudaMemsetAsync(st.ms.p, 0, st.ms.bytes, s));
+            break;
+    }
+}
+
 void Session::run_steps(cudaStream_t s) {
     for (const Memset& m : zero_at_start_) CK(cudaMemsetAsync(m.p, 0, m.bytes, s));
     if (profiling_ && ev_.size() < 2 * steps_.size()) {
@@ -1120,24 +1180,7 @@ void Session::run_steps(cudaStream_t s) {
     for (size_t i = 0; i < steps_.size(); ++i) {
         const Step& st = steps_[i];
         if (profiling_) CK(cudaEventRecord(ev_[2 * i], s));
-        switch (st.kind) {
-            case 0:
-                launch_gemm(st.g.probs, st.g.tiles, st.g.ntiles, st.g.xoff, st.g.yoff, st.g.X, st.g.Y, st.g.mode, s);
-                break;
-            case 1:
-                launch_pt(st.pt.items, st.pt.nitems, st.pt.srcs, prm_.kernel, s);
-                break;
-            case 2:
-                launch_vlist_forward(st.v.L, st.v.src_boxes, st.v.nsrc, st.v.upeq, st.v.spec, s);
-                break;
-            case 3:
-                launch_vlist_accum(st.v.L, st.v.trg, st.v.ntrg, st.v.vptr, st.v.vsrc, st.v.voff, st.v.spec,
-                                   st.v.dnchk, s);
-                break;
-            case 4:
-                CK(cudaMemsetAsync(st.ms.p, 0, st.ms.bytes, s));
-                break;
-        }
+        launch_step(st, s, st.v.spec);
         if (profiling_) {
             CK(cudaEventRecord(ev_[2 * i + 1], s));
             ev_pending_.push_back(std::make_pair((int)i, (int)(2 * i)));
@@ -1171,47 +1214,58 @@ std::vector<Session::ProfileEntry> Session::profile_read() {
 }
 
 void Session::eval_device(const double2* den, double2* val, cudaStream_t s) {
-    launch_gather_den(den, d_perm_, d_den_sorted_, npts_, s);
+    if (mixed())
+        launch_gather32(den, d_perm_, d_den_sorted_, npts_, 0, s);
+    else
+        launch_gather_den(den, d_perm_, d_den_sorted_, npts_, s);
     run_steps(s);
-    launch_scatter_val(d_val_sorted_, d_perm_, val, npts_, s);
+    if (mixed())
+        launch_scatter32(d_val_sorted_, d_perm_, val, npts_, 0, s);
+    else
+        launch_scatter_val(d_val_sorted_, d_perm_, val, npts_, s);
     CK(cudaGetLastError());
 }
 
-// A copy of run_steps whose V-list launches use `spec` for the spectra.
+void Session::eval_device_c64(const float2* den, float2* val, cudaStream_t s) {
+    if (!mixed()) throw std::invalid_argument("complex64 evaluation needs a mixed-precision session");
+    launch_gather32(den, d_perm_, d_den_sorted_, npts_, 1, s);
+    run_steps(s);
+    launch_scatter32(d_val_sorted_, d_perm_, val, npts_, 1, s);
+    CK(cudaGetLastError());
+}
+
+void Session::eval_host_c64(const std::complex<float>* den, std::complex<float>* val) {
+    if (!mixed()) throw std::invalid_argument("complex64 evaluation needs a mixed-precision session");
+    CK(cudaMemcpyAsync(d_den_io_, den, sizeof(float2) * npts_, cudaMemcpyHostToDevice, stream_));
+    eval_device_c64((const float2*)d_den_io_, (float2*)d_val_io_, stream_);
+    CK(cudaMemcpyAsync(val, d_val_io_, sizeof(float2) * npts_, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+}
+
+// run_steps with the V-list launches on `spec` for the spectra, no profiling.
 void Session::run_steps_spec(cudaStream_t s, double2* spec) {
     for (const Memset& m : zero_at_start_) CK(cudaMemsetAsync(m.p, 0, m.bytes, s));
-    for (const Step& st : steps_) {
-        switch (st.kind) {
-            case 0:
-                launch_gemm(st.g.probs, st.g.tiles, st.g.ntiles, st.g.xoff, st.g.yoff, st.g.X, st.g.Y, st.g.mode, s);
-                break;
-            case 1:
-                launch_pt(st.pt.items, st.pt.nitems, st.pt.srcs, prm_.kernel, s);
-                break;
-            case 2:
-                launch_vlist_forward(st.v.L, st.v.src_boxes, st.v.nsrc, st.v.upeq, spec, s);
-                break;
-            case 3:
-                launch_vlist_accum(st.v.L, st.v.trg, st.v.ntrg, st.v.vptr, st.v.vsrc, st.v.voff, spec, st.v.dnchk, s);
-                break;
-            case 4:
-                CK(cudaMemsetAsync(st.ms.p, 0, st.ms.bytes, s));
-                break;
-        }
-    }
+    for (const Step& st : steps_) launch_step(st, s, spec);
 }
 
 void Session::eval_device_scratch(const double2* den, double2* val, cudaStream_t s, double2* spec, size_t capacity) {
-    if (spectra_elems_ > capacity) {
+    const size_t es = mixed() ? sizeof(float2) : sizeof(double2);
+    if (spectra_elems_ * es > capacity * sizeof(double2)) {
         char msg[200];
         snprintf(msg, sizeof msg,
                  "the session's V-list spectra need %.1f MiB, more than the %.1f MiB of fixed scratch",
-                 spectra_elems_ * sizeof(double2) / 1048576.0, capacity * sizeof(double2) / 1048576.0);
+                 spectra_elems_ * es / 1048576.0, capacity * sizeof(double2) / 1048576.0);
         throw std::invalid_argument(msg);
     }
-    launch_gather_den(den, d_perm_, d_den_sorted_, npts_, s);
+    if (mixed())
+        launch_gather32(den, d_perm_, d_den_sorted_, npts_, 0, s);
+    else
+        launch_gather_den(den, d_perm_, d_den_sorted_, npts_, s);
     run_steps_spec(s, spec);
-    launch_scatter_val(d_val_sorted_, d_perm_, val, npts_, s);
+    if (mixed())
+        launch_scatter32(d_val_sorted_, d_perm_, val, npts_, 0, s);
+    else
+        launch_scatter_val(d_val_sorted_, d_perm_, val, npts_, s);
     CK(cudaGetLastError());
 }
 

@@ -20,6 +20,7 @@ struct SessionParams {
     int accu = 1;    // -wave3d_ACCU: P = 4/6/8 (src/wave3d.cpp:145-158)
     int kernel = 0;  // KERNEL_HELM / KERNEL_EXPR
     int device = 0;
+    int precision = 0;  // PRECISION_FP64 (plain) / PRECISION_MIXED
 };
 
 struct SessionStats {
@@ -44,6 +45,10 @@ public:
     // val = G * den at every point; arrays in point-id order, complex128.
     void eval_host(const std::complex<double>* den, std::complex<double>* val);
     void eval_device(const double2* den, double2* val, cudaStream_t s);
+    // complex64 densities / values (mixed form only)
+    void eval_device_c64(const float2* den, float2* val, cudaStream_t s);
+    void eval_host_c64(const std::complex<float>* den, std::complex<float>* val);
+    bool mixed() const { return prm_.precision == PRECISION_MIXED; }
     // Same matvec with the V-list spectra in caller-provided scratch of
     // `capacity` double2 (must hold spectra_elems()); nothing is allocated.
     void eval_device_scratch(const double2* den, double2* val, cudaStream_t s, double2* spec, size_t capacity);
@@ -122,6 +127,7 @@ private:
     void build();
     void run_steps(cudaStream_t s);
     void run_steps_spec(cudaStream_t s, double2* spec);
+    void launch_step(const Step& st, cudaStream_t s, double2* spec);
 
     SessionParams prm_;
     int npts_ = 0;

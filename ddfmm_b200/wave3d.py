@@ -55,8 +55,12 @@ class Mlib3d:
 
 
 class Wave3d:
-    def __init__(self, prefix="wave3d_", device=0):
+    """precision: _lib.PLAIN_FP64 (every pass in FP64) or _lib.MIXED (complex
+    FP32 storage, 3xTF32 tensor-core translations, FP32 near field)."""
+
+    def __init__(self, prefix="wave3d_", device=0, precision=0):
         self.prefix = prefix
+        self.precision = precision
         self.posptr = None
         self.kernel = 0
         self.mlibptr = None
@@ -90,10 +94,11 @@ class Wave3d:
         self.close()
         ctr = (C.c_double * 3)(*self.ctr)
         out = C.c_void_p()
-        rc = lib.ddfmm_session_create(pos.ctypes.data_as(C.POINTER(C.c_double)), pos.shape[0], int(self.kernel),
-                                      self.ACCU, self.NPQ, self.K, ctr, self.ptsmax, self.maxlevel, nc,
-                                      self.mlibptr.ldname.encode(), self.mlibptr.hdname.encode(), self.device,
-                                      C.byref(out))
+        rc = lib.ddfmm_session_create_ex(pos.ctypes.data_as(C.POINTER(C.c_double)), pos.shape[0],
+                                         int(self.kernel), self.ACCU, self.NPQ, self.K, ctr, self.ptsmax,
+                                         self.maxlevel, nc, self.mlibptr.ldname.encode(),
+                                         self.mlibptr.hdname.encode(), self.device, int(self.precision),
+                                         C.byref(out))
         _lib.check(rc)
         self._s = out
         self._n = pos.shape[0]
@@ -105,22 +110,33 @@ class Wave3d:
 
     # src/wave3d_eval.cpp:299-415
     def eval(self, den, val):
+        """val[:] = matvec(den).  val's dtype picks the I/O: complex128 always,
+        complex64 on mixed sessions."""
         self._need()
-        d = np.ascontiguousarray(den, dtype=np.complex128)
+        c64 = isinstance(val, np.ndarray) and val.dtype == np.complex64
+        dt = np.complex64 if c64 else np.complex128
+        d = np.ascontiguousarray(den, dtype=dt)
         if d.shape != (self._n,):
             raise _lib.DDFMMError(1, "den must hold %d complex values" % self._n)
-        if not (isinstance(val, np.ndarray) and val.dtype == np.complex128 and val.shape == (self._n,)
+        if not (isinstance(val, np.ndarray) and val.dtype == dt and val.shape == (self._n,)
                 and val.flags.c_contiguous):
-            raise _lib.DDFMMError(1, "val must be a contiguous complex128 array of length %d" % self._n)
-        dp = C.POINTER(C.c_double)
-        _lib.check(_lib.load().ddfmm_eval(self._s, d.ctypes.data_as(dp), val.ctypes.data_as(dp)))
+            raise _lib.DDFMMError(1, "val must be a contiguous complex128 (or, mixed, complex64) array of "
+                                     "length %d" % self._n)
+        if c64:
+            fp = C.POINTER(C.c_float)
+            _lib.check(_lib.load().ddfmm_eval_c64(self._s, d.ctypes.data_as(fp), val.ctypes.data_as(fp)))
+        else:
+            dp = C.POINTER(C.c_double)
+            _lib.check(_lib.load().ddfmm_eval(self._s, d.ctypes.data_as(dp), val.ctypes.data_as(dp)))
         return 0
 
-    def eval_device(self, den_ptr, val_ptr, stream_ptr=None):
-        """den_ptr / val_ptr: device addresses of N complex128 values."""
+    def eval_device(self, den_ptr, val_ptr, stream_ptr=None, c64=False):
+        """den_ptr / val_ptr: device addresses of N complex128 values
+        (complex64 with c64=True, mixed sessions only)."""
         self._need()
-        _lib.check(_lib.load().ddfmm_eval_device(self._s, C.c_void_p(den_ptr), C.c_void_p(val_ptr),
-                                                 C.c_void_p(stream_ptr) if stream_ptr else None))
+        f = _lib.load().ddfmm_eval_device_c64 if c64 else _lib.load().ddfmm_eval_device
+        _lib.check(f(self._s, C.c_void_p(den_ptr), C.c_void_p(val_ptr),
+                     C.c_void_p(stream_ptr) if stream_ptr else None))
 
     def direct(self, den, ids):
         """FP64 direct sum at the given point ids."""
@@ -171,13 +187,13 @@ class Wave3d:
             pass
 
 
-def from_workload(w, device=0):
+def from_workload(w, device=0, precision=0):
     """Set up a Wave3d for a workloads.Workload (operators created on demand)."""
     ld, hd = w.operators()
     mlib = Mlib3d()
     mlib.kernel = w.kernel
     mlib.setup({"-mlib3d_ldname": ld, "-mlib3d_hdname": hd, "-mlib3d_NPQ": str(w.npq)})
-    wave = Wave3d(device=device)
+    wave = Wave3d(device=device, precision=precision)
     wave.posptr = w.points()
     wave.kernel = w.kernel
     wave.mlibptr = mlib

@@ -37,6 +37,14 @@ enum {
 
 enum { DDFMM_KERNEL_HELM = 0, DDFMM_KERNEL_EXPR = 1 }; /* include/kernel3d.hpp:24-27 */
 
+/* Arithmetic of a session.  PLAIN_FP64: every pass in FP64 (the form that
+ * matches the reference to 1e-10).  MIXED: operators still built in FP64,
+ * then stored and applied in complex FP32 -- translations as 3xTF32 products
+ * on the tensor cores with FP32 accumulation, the near field in FP32 on FP64
+ * coordinate differences.  Error vs the FP64 direct sum is then set by FP32
+ * rounding (about 1e-6) on top of the method's own (1e-4 / 1e-6 / 1e-8). */
+enum { DDFMM_PLAIN_FP64 = 0, DDFMM_MIXED = 1 };
+
 typedef struct ddfmm_session ddfmm_session;
 
 typedef struct ddfmm_stats {
@@ -61,10 +69,23 @@ int ddfmm_session_create(const double* pos3n, int n, int kernel, int accu, int n
                          const char* ld_path, const char* hd_path, int device,
                          ddfmm_session** out);
 
+/* ddfmm_session_create with the arithmetic chosen by `precision`
+ * (DDFMM_PLAIN_FP64 or DDFMM_MIXED). */
+int ddfmm_session_create_ex(const double* pos3n, int n, int kernel, int accu, int npq, double K,
+                            const double* ctr3, int ptsmax, int maxlevel, int ncell,
+                            const char* ld_path, const char* hd_path, int device, int precision,
+                            ddfmm_session** out);
+
 /* Wave3d::eval: val[i] = sum_j G(p_i, p_j) den[j] via the directional FMM.
  * den, val: host arrays of n complex128 in point-id order.  Unlike the
  * reference, repeated calls do not accumulate (src/wave3d_eval.cpp:518-521). */
 int ddfmm_eval(ddfmm_session* s, const double* den, double* val);
+
+/* Mixed sessions only: complex64 densities and values (interleaved floats),
+ * host arrays / device arrays of the session's GPU.  ddfmm_eval and
+ * ddfmm_eval_device also work on mixed sessions (complex128 in and out). */
+int ddfmm_eval_c64(ddfmm_session* s, const float* den, float* val);
+int ddfmm_eval_device_c64(ddfmm_session* s, const void* den_dev, void* val_dev, void* stream);
 
 /* Same, with den / val already in device memory of the session's GPU
  * (n complex128 each); stream is a cudaStream_t or NULL for the session's
