@@ -189,7 +189,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws):
+def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws, profile_json=None):
     """The mixed-precision form on the same workload: complex64 densities on
     the device, 3xTF32 translations; reports matvec/s, its error vs the FP64
     direct sum and latency percentiles."""
@@ -217,6 +217,8 @@ def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws):
         torch.distributed.barrier()
     torch.cuda.synchronize(dev)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    if profile_json:
+        m.profile(True)
     for i in range(steps):
         with torch.cuda.stream(stream):
             ev[i][0].record(stream)
@@ -224,6 +226,11 @@ def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws):
         with torch.cuda.stream(stream):
             ev[i][1].record(stream)
     stream.synchronize()
+    if profile_json:
+        prof = m.profile_read(reset=True)
+        m.profile(False)
+        json.dump({k: dict(v, ms_per_step=v["ms"] / steps) for k, v in prof.items()}, open(profile_json, "w"),
+                  indent=1)
     lat = np.array([a.elapsed_time(b) for a, b in ev])
     ms = ev[0][0].elapsed_time(ev[-1][1]) / steps
     if ws > 1:
@@ -351,7 +358,8 @@ def run_ours(args):
             cpu = {"value": None, "unit": "matvec/s", "cores": 1, "kind": "reference", "sample": "unavailable: %s" % ex}
     mixed = None
     if not args.no_mixed:
-        mixed = measure_mixed(w, wave_args=(local,), steps=args.steps, warmup=args.warmup, dev=dev, chk=chk, ws=ws)
+        mixed = measure_mixed(w, wave_args=(local,), steps=args.steps, warmup=args.warmup, dev=dev, chk=chk, ws=ws,
+                              profile_json=(args.profile_json + ".mixed") if args.profile_json else None)
     if args.profile_json and rank == 0:
         json.dump({"passes": passes, "by_kernel": by_kernel, "stats": st}, open(args.profile_json, "w"), indent=1)
     if rank == 0:
