@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-json", default=None, help="write the per-pass profile here")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form measurement")
+    ap.add_argument("--mixed-mma-sync", action="store_true",
+                    help="also measure the mixed form with its translations on the mma.sync path")
     return ap.parse_args()
 
 
@@ -189,15 +191,17 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws, profile_json=None):
+def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws, profile_json=None, precision=None):
     """The mixed-precision form on the same workload: complex64 densities on
-    the device, 3xTF32 translations; reports matvec/s, its error vs the FP64
-    direct sum and latency percentiles."""
+    the device, 3xTF32 translations (tcgen05 by default, or the mma.sync
+    path); reports matvec/s, its error vs the FP64 direct sum and latency
+    percentiles."""
     import torch
     from ddfmm_b200 import _lib, wave3d
     (local,) = wave_args
+    precision = _lib.MIXED if precision is None else precision
     t0 = time.perf_counter()
-    m = wave3d.from_workload(w, device=local, precision=_lib.MIXED)
+    m = wave3d.from_workload(w, device=local, precision=precision)
     setup_s = time.perf_counter() - t0
     den = w.densities(np.complex64)
     rng = np.random.default_rng(7)
@@ -238,7 +242,9 @@ def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws, profile_json=None):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
     m.close()
-    return {"value": ws * 1e3 / ms, "unit": "matvec/s", "ms_per_step": ms, "dtype": "c64 (3xTF32 translations)",
+    gemm = "tcgen05" if precision == _lib.MIXED else "mma.sync"
+    return {"value": ws * 1e3 / ms, "unit": "matvec/s", "ms_per_step": ms,
+            "dtype": "c64 (3xTF32 translations on %s)" % gemm,
             "relerr_vs_fp64_direct": relerr, "setup_s": setup_s,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))}}
 
@@ -360,6 +366,12 @@ def run_ours(args):
     if not args.no_mixed:
         mixed = measure_mixed(w, wave_args=(local,), steps=args.steps, warmup=args.warmup, dev=dev, chk=chk, ws=ws,
                               profile_json=(args.profile_json + ".mixed") if args.profile_json else None)
+    mixed_mma = None
+    if args.mixed_mma_sync:
+        from ddfmm_b200 import _lib
+        mixed_mma = measure_mixed(w, wave_args=(local,), steps=args.steps, warmup=args.warmup, dev=dev, chk=chk,
+                                  ws=ws, precision=_lib.MIXED_MMA_SYNC,
+                                  profile_json=(args.profile_json + ".mma_sync") if args.profile_json else None)
     if args.profile_json and rank == 0:
         json.dump({"passes": passes, "by_kernel": by_kernel, "stats": st}, open(args.profile_json, "w"), indent=1)
     if rank == 0:
@@ -376,6 +388,8 @@ def run_ours(args):
                         "d2h_bytes_per_step": 16 * w.N, "rel_diff_vs_device_path": e2e_relerr},
                 "roofline": roof, "gpu_launches": int(round(launches / args.steps)) * args.steps,
                 "clocks": clocks, "cpu_baseline": cpu, "mixed_form": mixed, "passes": passes}
+        if mixed_mma:
+            line["mixed_form_mma_sync"] = mixed_mma
         print(json.dumps(line), flush=True)
     wave.close()
     if ws > 1:

@@ -17,7 +17,7 @@ EXPORTS = (
     "ddfmm_profile_enable", "ddfmm_profile_read", "ddfmm_eval_device_noalloc",
     "ddfmm_session_create_ex", "ddfmm_eval_c64", "ddfmm_eval_device_c64",
 )
-PLAIN_FP64, MIXED = 0, 1
+PLAIN_FP64, MIXED, MIXED_MMA_SYNC = 0, 1, 2
 
 
 class ddfmm_stats(C.Structure):

@@ -73,8 +73,8 @@ int ddfmm_session_create_ex(const double* pos3n, int n, int kernel, int accu, in
     if (ncell < 1 || (ncell & (ncell - 1)) || K / ncell < 1 - 1e-12)
         return fail(DDFMM_EINVAL, "ncell must be a power of two with K/ncell >= 1");
     if (ptsmax < 1 || maxlevel < 1) return fail(DDFMM_EINVAL, "ptsmax and maxlevel must be positive");
-    if (precision != DDFMM_PLAIN_FP64 && precision != DDFMM_MIXED)
-        return fail(DDFMM_EINVAL, "precision must be DDFMM_PLAIN_FP64 or DDFMM_MIXED");
+    if (precision != DDFMM_PLAIN_FP64 && precision != DDFMM_MIXED && precision != DDFMM_MIXED_MMA_SYNC)
+        return fail(DDFMM_EINVAL, "precision must be DDFMM_PLAIN_FP64, DDFMM_MIXED or DDFMM_MIXED_MMA_SYNC");
     if (!ld_path || !hd_path) return fail(DDFMM_EINVAL, "operator file paths are required");
     for (long long i = 0; i < 3LL * n; ++i)
         if (!std::isfinite(pos3n[i])) return fail(DDFMM_EINVAL, "non-finite point coordinate");

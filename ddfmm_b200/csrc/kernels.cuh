@@ -82,7 +82,9 @@ void launch_vlist_accum(const VlistLevel& L, const int* trg, int ntrg, const int
 // mixed-precision form (kernels_mixed.cu): complex FP32 data behind the same
 // descriptors; GemmProblem::A, PtItem::out, PtSrc::den and VlistLevel::tns /
 // twf / twb then point to float2 data.
-enum Precision { PRECISION_FP64 = 0, PRECISION_MIXED = 1 };
+// PRECISION_MIXED multiplies on tcgen05 (kernels_umma.cu); PRECISION_MIXED_MMA_SYNC
+// is the same form with the warp-level mma.sync GEMM (cgemm_kernel), kept for comparison.
+enum Precision { PRECISION_FP64 = 0, PRECISION_MIXED = 1, PRECISION_MIXED_MMA_SYNC = 2 };
 void cgemm_init();
 void launch_cgemm(const GemmProblem* probs_dev, const GemmTile* tiles_dev, int ntiles, const long long* xoff,
                   const long long* yoff, const void* X, void* Y, int mode, cudaStream_t s);
@@ -95,6 +97,36 @@ void launch_vlist_accum32(const VlistLevel& L, const int* trg, int ntrg, const i
 void launch_gather32(const void* den, const int* perm, void* out, int n, int c64, cudaStream_t s);
 void launch_scatter32(const void* in, const int* perm, void* val, int n, int c64, cudaStream_t s);
 void launch_to_c64(const double2* a, float2* b, long long n, cudaStream_t s);
+
+// mixed-form GEMM on tcgen05 (kernels_umma.cu): 128 gathered columns x up to
+// 128 complex operator rows per tile, operator packed at setup as split TF32.
+struct UmmaProblem {
+    const float* B;      // packed operator (umma_pack_kernel layout)
+    size_t tile_stride;  // floats between 128-row tiles of the packed operator
+    int m, k, nkb;       // complex rows, complex columns, 16-wide real K blocks
+    int col0, ncol;      // gathered columns, as in GemmProblem
+};
+struct UmmaTile {
+    int prob;
+    int rtile;  // 128-row tile of the operator
+    int row0;   // = 128 * rtile
+    int rows;   // complex rows of this tile (<= 128)
+    int col0;   // relative to the problem's first column
+    int pad;
+};
+struct UmmaPackJob {
+    const float2* A;  // complex FP32 operator, column-major
+    float* dst;
+    size_t tile_stride;
+    int m, k, lda, nkb;
+};
+void umma_init();
+int umma_nkb(int k);
+size_t umma_tile_stride(int k);
+size_t umma_packed_floats(int m, int k);
+void launch_umma_pack(const UmmaPackJob* jobs_dev, int njobs, cudaStream_t s);
+void launch_umma_cgemm(const UmmaProblem* probs, const UmmaTile* tiles, int ntiles, const long long* xoff,
+                       const long long* yoff, const void* X, void* Y, int mode, int* err, cudaStream_t s);
 
 // gather/scatter helpers
 void launch_gather_den(const double2* den, const int* perm, double2* out, int n, cudaStream_t s);

@@ -106,6 +106,12 @@ void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<
     st.label = label;
     st.flops = flops;
     st.bytes = bytes;
+    if (umma()) {
+        add_umma(P, xs, ys, X, Y, mode, st);
+        steps_.push_back(st);
+        stats_.gemm_launches++;
+        return;
+    }
     st.g.probs = upload(P);
     st.g.tiles = upload(tiles);
     st.g.xoff = upload(xs);
@@ -116,6 +122,75 @@ void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<
     st.g.mode = mode;
     steps_.push_back(st);
     stats_.gemm_launches++;
+}
+
+const float* Session::packed_operator(const GemmProblem& q) {
+    const auto key = std::make_pair((const void*)q.A, ((long long)q.m << 32) | (long long)q.k);
+    auto it = packed_.find(key);
+    if (it != packed_.end()) return it->second;
+    // packed operators are sub-allocated from 256 MiB chunks (16-byte aligned: they are
+    // read with cp.async.bulk)
+    const size_t nf = (umma_packed_floats(q.m, q.k) + 63) & ~(size_t)63;
+    if (nf > arena_left_) {
+        const size_t chunk = std::max(nf, (size_t)64 << 20);
+        arena_ = dalloc<float>(chunk);
+        arena_left_ = chunk;
+    }
+    float* d = arena_;
+    arena_ += nf;
+    arena_left_ -= nf;
+    pack_jobs_.push_back(UmmaPackJob{(const float2*)q.A, d, umma_tile_stride(q.k), q.m, q.k, q.lda, umma_nkb(q.k)});
+    return packed_[key] = d;
+}
+
+// tcgen05 form of one grouped GEMM launch: tiles of 128 gathered columns x
+// 128 complex operator rows, the tiles of one problem adjacent so that blocks
+// in flight share its packed operator in L2.
+void Session::add_umma(const std::vector<GemmProblem>& P, const std::vector<long long>& xs,
+                       const std::vector<long long>& ys, const double2* X, double2* Y, int mode, Step& st) {
+    std::vector<UmmaProblem> U;
+    std::vector<UmmaTile> tiles;
+    for (size_t i = 0; i < P.size(); ++i) {
+        const GemmProblem& q = P[i];
+        U.push_back(UmmaProblem{packed_operator(q), umma_tile_stride(q.k), q.m, q.k, umma_nkb(q.k), q.col0, q.ncol});
+        for (int rt = 0; rt * 128 < q.m; ++rt)
+            for (int c0 = 0; c0 < q.ncol; c0 += 128)
+                tiles.push_back(UmmaTile{(int)i, rt, rt * 128, std::min(128, q.m - rt * 128), c0, 0});
+    }
+    st.kind = 5;
+    st.u.probs = upload(U);
+    st.u.tiles = upload(tiles);
+    st.u.xoff = upload(xs);
+    st.u.yoff = upload(ys);
+    st.u.ntiles = (int)tiles.size();
+    st.u.X = X;
+    st.u.Y = Y;
+    st.u.mode = mode;
+}
+
+void Session::flush_packs() {
+    if (pack_jobs_.empty()) return;
+    UmmaPackJob* d = nullptr;
+    CK(cudaMalloc(&d, sizeof(UmmaPackJob) * pack_jobs_.size()));
+    CK(cudaMemcpyAsync(d, pack_jobs_.data(), sizeof(UmmaPackJob) * pack_jobs_.size(), cudaMemcpyHostToDevice,
+                       stream_));
+    launch_umma_pack(d, (int)pack_jobs_.size(), stream_);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaFree(d));
+    pack_jobs_.clear();
+}
+
+void Session::check_device_error() {
+    if (!d_err_) return;
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, d_err_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    if (h) {
+        CK(cudaMemsetAsync(d_err_, 0, sizeof(int), stream_));
+        CK(cudaStreamSynchronize(stream_));
+        throw std::runtime_error("CUDA error: a tensor-core GEMM block timed out waiting on its pipeline");
+    }
 }
 
 const char* Session::width_label(const char* pass, double W) {
@@ -231,7 +306,7 @@ void Session::build() {
     if (kern != KERNEL_HELM && kern != KERNEL_EXPR) throw std::runtime_error("unknown kernel type");
     // complex state: double2 (plain FP64 form) or float2 (mixed form); plan
     // offsets are in elements, so both forms share one plan
-    const bool mixed = prm_.precision == PRECISION_MIXED;
+    const bool mixed = this->mixed();
     const size_t es = mixed ? sizeof(float2) : sizeof(double2);
     auto E = [&](double2* base, size_t elems) { return (double2*)((char*)base + elems * es); };
     auto salloc = [&](size_t elems) { return (double2*)dalloc<char>(elems * es); };
@@ -344,6 +419,11 @@ void Session::build() {
     gemm_init();
     vlist32_init(G);
     cgemm_init();
+    if (umma()) {
+        umma_init();
+        d_err_ = dalloc<int>(1);
+        CK(cudaMemsetAsync(d_err_, 0, sizeof(int), stream_));
+    }
 
     for (auto& kv : lflevels) {
         int level = kv.first;
@@ -1123,6 +1203,7 @@ void Session::build() {
                        "lf_l2l");
             }
     }
+    flush_packs();
     stats_.kernel_launches = (long long)steps_.size() + 2;
 }
 
@@ -1132,6 +1213,7 @@ static const char* kernel_name(int kind) {
         case 1: return "pt_kernel";
         case 2: return "vlist_forward_kernel";
         case 3: return "vlist_accum_kernel";
+        case 5: return "umma_cgemm_kernel";
         default: return "memset";
     }
 }
@@ -1165,6 +1247,10 @@ void Session::launch_step(const Step& st, cudaStream_t s, double2* spec) {
             break;
         case 4:
             CK(cudaMemsetAsync(st.ms.p, 0, st.ms.bytes, s));
+            break;
+        case 5:
+            launch_umma_cgemm(st.u.probs, st.u.tiles, st.u.ntiles, st.u.xoff, st.u.yoff, st.u.X, st.u.Y, st.u.mode,
+                              d_err_, s);
             break;
     }
 }
@@ -1240,6 +1326,7 @@ void Session::eval_host_c64(const std::complex<float>* den, std::complex<float>*
     eval_device_c64((const float2*)d_den_io_, (float2*)d_val_io_, stream_);
     CK(cudaMemcpyAsync(val, d_val_io_, sizeof(float2) * npts_, cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
+    check_device_error();
 }
 
 // run_steps with the V-list launches on `spec` for the spectra, no profiling.
@@ -1274,6 +1361,7 @@ void Session::eval_host(const std::complex<double>* den, std::complex<double>* v
     eval_device(d_den_io_, d_val_io_, stream_);
     CK(cudaMemcpyAsync(val, d_val_io_, sizeof(double2) * npts_, cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
+    check_device_error();
 }
 
 void Session::direct_host(const std::complex<double>* den, const int* ids, int nids, std::complex<double>* out) {

@@ -20,7 +20,7 @@ struct SessionParams {
     int accu = 1;    // -wave3d_ACCU: P = 4/6/8 (src/wave3d.cpp:145-158)
     int kernel = 0;  // KERNEL_HELM / KERNEL_EXPR
     int device = 0;
-    int precision = 0;  // PRECISION_FP64 (plain) / PRECISION_MIXED
+    int precision = 0;  // PRECISION_FP64 (plain) / PRECISION_MIXED / PRECISION_MIXED_MMA_SYNC
 };
 
 struct SessionStats {
@@ -48,7 +48,13 @@ public:
     // complex64 densities / values (mixed form only)
     void eval_device_c64(const float2* den, float2* val, cudaStream_t s);
     void eval_host_c64(const std::complex<float>* den, std::complex<float>* val);
-    bool mixed() const { return prm_.precision == PRECISION_MIXED; }
+    bool mixed() const {
+        return prm_.precision == PRECISION_MIXED || prm_.precision == PRECISION_MIXED_MMA_SYNC;
+    }
+    bool umma() const { return prm_.precision == PRECISION_MIXED; }
+    // Throws if a tensor-core GEMM gave up waiting on its pipeline since the last
+    // check (the flag is reset); synchronises the session's stream.
+    void check_device_error();
     // Same matvec with the V-list spectra in caller-provided scratch of
     // `capacity` double2 (must hold spectra_elems()); nothing is allocated.
     void eval_device_scratch(const double2* den, double2* val, cudaStream_t s, double2* spec, size_t capacity);
@@ -82,6 +88,16 @@ private:
         double2* Y = nullptr;
         int mode = 0;
     };
+    struct UmmaLaunch {
+        UmmaProblem* probs = nullptr;
+        UmmaTile* tiles = nullptr;
+        long long* xoff = nullptr;
+        long long* yoff = nullptr;
+        int ntiles = 0;
+        const double2* X = nullptr;
+        double2* Y = nullptr;
+        int mode = 0;
+    };
     struct PtLaunch {
         PtItem* items = nullptr;
         PtSrc* srcs = nullptr;
@@ -106,11 +122,12 @@ private:
     };
     // one step of the eval: exactly one of these is used
     struct Step {
-        int kind;  // 0 gemm, 1 pt, 2 vfwd, 3 vacc, 4 memset
+        int kind;  // 0 gemm, 1 pt, 2 vfwd, 3 vacc, 4 memset, 5 tcgen05 gemm
         const char* label;  // pass name for profiling
         double flops;       // algorithmic flops of the launch
         double bytes;       // algorithmic DRAM bytes of the launch
         GemmLaunch g;
+        UmmaLaunch u;
         PtLaunch pt;
         VLaunch v;
         Memset ms;
@@ -123,6 +140,10 @@ private:
     void add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<long long> >& xo,
                   std::vector<std::vector<long long> >& yo, const double2* X, double2* Y, int mode,
                   const char* label);
+    const float* packed_operator(const GemmProblem& q);
+    void add_umma(const std::vector<GemmProblem>& P, const std::vector<long long>& xs,
+                  const std::vector<long long>& ys, const double2* X, double2* Y, int mode, Step& st);
+    void flush_packs();
     void add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>& srcs, const char* label);
     void build();
     void run_steps(cudaStream_t s);
@@ -148,6 +169,11 @@ private:
     double2* d_den_io_ = nullptr;
     double2* d_val_io_ = nullptr;
     std::vector<Memset> zero_at_start_;
+    int* d_err_ = nullptr;  // set by a tensor-core GEMM that timed out
+    std::map<std::pair<const void*, long long>, const float*> packed_;  // (operator, m k) -> packed copy
+    std::vector<UmmaPackJob> pack_jobs_;                                 // packing still to launch
+    float* arena_ = nullptr;  // current chunk for packed operators
+    size_t arena_left_ = 0;   // floats left in it
     size_t spectra_elems_ = 0;
     bool profiling_ = false;
     std::vector<cudaEvent_t> ev_;

@@ -55,8 +55,9 @@ class Mlib3d:
 
 
 class Wave3d:
-    """precision: _lib.PLAIN_FP64 (every pass in FP64) or _lib.MIXED (complex
-    FP32 storage, 3xTF32 tensor-core translations, FP32 near field)."""
+    """precision: _lib.PLAIN_FP64 (every pass in FP64), _lib.MIXED (complex
+    FP32 storage, 3xTF32 translations on tcgen05, FP32 near field) or
+    _lib.MIXED_MMA_SYNC (the same with the translations on mma.sync)."""
 
     def __init__(self, prefix="wave3d_", device=0, precision=0):
         self.prefix = prefix

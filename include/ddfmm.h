@@ -40,10 +40,12 @@ enum { DDFMM_KERNEL_HELM = 0, DDFMM_KERNEL_EXPR = 1 }; /* include/kernel3d.hpp:2
 /* Arithmetic of a session.  PLAIN_FP64: every pass in FP64 (the form that
  * matches the reference to 1e-10).  MIXED: operators still built in FP64,
  * then stored and applied in complex FP32 -- translations as 3xTF32 products
- * on the tensor cores with FP32 accumulation, the near field in FP32 on FP64
- * coordinate differences.  Error vs the FP64 direct sum is then set by FP32
- * rounding (about 1e-6) on top of the method's own (1e-4 / 1e-6 / 1e-8). */
-enum { DDFMM_PLAIN_FP64 = 0, DDFMM_MIXED = 1 };
+ * on the tensor cores (tcgen05, accumulators in tensor memory) with FP32
+ * accumulation, the near field in FP32 on FP64 coordinate differences.  Error
+ * vs the FP64 direct sum is then set by FP32 rounding (about 1e-6) on top of
+ * the method's own (1e-4 / 1e-6 / 1e-8).  MIXED_MMA_SYNC: the same form with
+ * the translations on the warp-level mma.sync path instead (for comparison). */
+enum { DDFMM_PLAIN_FP64 = 0, DDFMM_MIXED = 1, DDFMM_MIXED_MMA_SYNC = 2 };
 
 typedef struct ddfmm_session ddfmm_session;
 
@@ -70,7 +72,7 @@ int ddfmm_session_create(const double* pos3n, int n, int kernel, int accu, int n
                          ddfmm_session** out);
 
 /* ddfmm_session_create with the arithmetic chosen by `precision`
- * (DDFMM_PLAIN_FP64 or DDFMM_MIXED). */
+ * (DDFMM_PLAIN_FP64, DDFMM_MIXED or DDFMM_MIXED_MMA_SYNC). */
 int ddfmm_session_create_ex(const double* pos3n, int n, int kernel, int accu, int npq, double K,
                             const double* ctr3, int ptsmax, int maxlevel, int ncell,
                             const char* ld_path, const char* hd_path, int device, int precision,

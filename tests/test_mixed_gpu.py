@@ -1,5 +1,7 @@
 """Mixed-precision form: complex FP32 storage, 3xTF32 tensor-core
 translations with FP32 accumulation, FP32 near field on FP64 differences.
+MIXED runs the translations on tcgen05 (accumulators in tensor memory),
+MIXED_MMA_SYNC on the warp-level mma.sync path; both are held to the bar.
 
 Tolerance: the mixed result differs from the reference's FP64 result by FP32
 rounding through ~10 chained translations; bar 2e-5 relative l2 (the method
@@ -50,6 +52,26 @@ def test_mixed_close_to_reference(name, tmp_path):
     print("mixed %s: complex64 I/O vs complex128 I/O %.3e" % (name, d))
     assert d <= TOL_MIXED
     w.close()
+
+
+@pytest.mark.parametrize("name", ["sphere_k8_n5000_p4_helm", "sphere_k4_n1500_p6_helm", "cluster_k4_n1500_p4_helm_m8"])
+def test_tcgen05_and_mma_sync_translations_agree(name, tmp_path):
+    """Same FP32 form, two tensor-core paths: they differ only by FP32
+    accumulation order (both 3xTF32 products with FP32 sums)."""
+    c = fixtures.Case(name)
+    vals = {}
+    for prec in (_lib.MIXED, _lib.MIXED_MMA_SYNC):
+        w = _session(c, tmp_path, prec)
+        v = np.zeros_like(c.den)
+        w.eval(c.den, v)
+        vals[prec] = v
+        rel = np.linalg.norm(v - c.val) / np.linalg.norm(c.val)
+        print("precision %d %s: rel l2 vs reference %.3e" % (prec, name, rel))
+        assert rel <= TOL_MIXED, rel
+        w.close()
+    d = np.linalg.norm(vals[_lib.MIXED] - vals[_lib.MIXED_MMA_SYNC]) / np.linalg.norm(c.val)
+    print("tcgen05 vs mma.sync %s: %.3e" % (name, d))
+    assert d <= TOL_MIXED
 
 
 def test_c64_entry_points_refuse_plain_sessions(tmp_path):
