@@ -12,16 +12,33 @@
 // TMEM column = real output row).
 //
 // Operands sit in shared memory in the no-swizzle K-major core-matrix layout:
-// a core matrix is 8 rows x 16 bytes (4 TF32 along K), K-adjacent core
-// matrices are 128 B apart (descriptor LBO) and 8-row groups 512 B apart
-// (SBO) within a 16-element K block.  The operator is packed into exactly
-// this layout, already split, at session setup (umma_pack_kernel) and copied
-// per K block with cp.async.bulk; the gathered columns are split and stored
-// by the block's threads.  One thread issues the MMAs of block kb while all
-// threads prefetch block kb+1; tcgen05.commit arrives on an mbarrier when
-// the MMAs are done reading a stage.  Every mbarrier wait is bounded in time
-// and iterations: on timeout the block drains what it has in flight (again
-// bounded), records an error in *err, skips its output and frees its TMEM.
+// a core matrix is 8 rows x 16 bytes (4 TF32 along K); the two core matrices
+// of an 8-wide K block are 128 B apart (descriptor LBO) and 8-row groups 256 B
+// apart (SBO).  The operator is packed into exactly this layout, already
+// split, at session setup (umma_pack_kernel).
+//
+// Persistent: one block per SM walks the tile list (tiles of one
+// problem adjacent, so the blocks in flight share its packed operator in L2)
+// with two TMEM accumulators of 256 columns, so the epilogue of one tile
+// overlaps the main loop of the next.  Warp roles, over a USTAGES-deep ring of
+// K blocks that runs on across tiles:
+//   producers  UPSETS sets of 4 warps, set j taking every UPSETS-th K block from
+//              j on; 32 gathered columns per warp: load the 4 complex of a K block
+//              of each column (8-lane groups, 32 contiguous bytes; zero past k
+//              or ncol), UPREF blocks ahead in registers; when a ring slot is
+//              free, split (hi = the top 19 bits, lo = TF32(x - hi)) into it,
+//              fence to the async proxy, arrive on full[s] (one elected lane
+//              per warp after __syncwarp).
+//   W_LOAD_B   one thread: operator hi/lo blocks by cp.async.bulk onto full[s].
+//   W_MMA      one thread: per tile waits until its accumulator is drained
+//              (tmem_empty), then per block waits full[s], issues the three
+//              MMAs, commits to empty[s]; after the tile commits tmem_full.
+//   W_EPI..+3  epilogue, warp w on TMEM lanes 32 (w % 4) ..: TMEM -> a parking
+//              area -> global, one column at a time in 256-byte coalesced
+//              rows; then arrive on tmem_empty.
+// Every mbarrier wait is bounded (1 s, or sooner once another role failed):
+// a block that gives up stops issuing work, lets its MMAs and copies drain
+// (bounded), frees its TMEM and sets *err.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -31,22 +48,52 @@
 namespace ddfmm {
 
 constexpr int UM = 128;      // gathered columns per tile (MMA M)
-constexpr int UBK = 16;      // real K elements per block (two K=8 MMAs)
+#ifndef DDFMM_UMMA_BK
+#define DDFMM_UMMA_BK 16
+#endif
+constexpr int UBK = DDFMM_UMMA_BK;  // real K per block: UBK / 8 MMA K-steps
+constexpr int CPB = UBK / 2;        // complex per gathered column per block
+static_assert(UBK == 8 || UBK == 16, "K block of 8 or 16");
 constexpr int UNMAX = 256;   // max real rows per tile (MMA N)
-constexpr int UTHREADS = 128;
-// per stage: A hi + lo (128 x 16 TF32 each), B hi + lo (up to 256 x 16 each)
+#ifndef DDFMM_UMMA_STAGES
+#define DDFMM_UMMA_STAGES (UBK == 16 ? 3 : 6)
+#endif
+#ifndef DDFMM_UMMA_PREF
+#define DDFMM_UMMA_PREF (UBK == 16 ? 4 : 8)
+#endif
+#ifndef DDFMM_UMMA_PCH
+#define DDFMM_UMMA_PCH 32
+#endif
+constexpr int USTAGES = DDFMM_UMMA_STAGES;  // ring depth
+constexpr int UPREF = DDFMM_UMMA_PREF;      // gathered-column blocks prefetched into registers
+#ifndef DDFMM_UMMA_PSETS
+#define DDFMM_UMMA_PSETS 2
+#endif
+#ifndef DDFMM_UMMA_ELECT
+#define DDFMM_UMMA_ELECT 0
+#endif
+constexpr int UPSETS = DDFMM_UMMA_PSETS;     // producer sets (4 warps each), alternating K blocks
+constexpr bool UELECT = DDFMM_UMMA_ELECT;    // one mbarrier arrival per warp instead of per thread
+constexpr int W_LOAD_B = 4 * UPSETS, W_MMA = W_LOAD_B + 1, W_EPI = W_LOAD_B + 2;  // warp roles
+constexpr int UTHREADS = 32 * (W_EPI + 4);
+constexpr int U_FULL_COUNT = (UELECT ? 4 : UM) + 1;  // producer arrivals + the operator loader's
+constexpr int U_EMPTY_ACC_COUNT = UELECT ? 4 : UM;   // epilogue arrivals
 constexpr int U_A_BYTES = UM * UBK * 4;
 constexpr int U_B_BYTES = UNMAX * UBK * 4;
 constexpr int U_STAGE_BYTES = 2 * U_A_BYTES + 2 * U_B_BYTES;
-// two stages + alignment slack: ~101 KB per block with the static part, so at
-// most two blocks share an SM and their 2 x 256 TMEM columns always fit
-constexpr int UGEMM_SMEM = 2 * U_STAGE_BYTES + 1024;
+constexpr int PCH = DDFMM_UMMA_PCH;  // epilogue chunk: complex rows parked per column
+static_assert(PCH == 16 || PCH == 32, "epilogue chunk of 16 or 32 rows");
+constexpr int U_PARK_BYTES = 4 * 32 * (PCH + 1) * 8;  // 32 columns x PCH complex (+1 pad) per warp
+// ring + parking area + alignment slack: one block per SM (also what the 512
+// TMEM columns need)
+constexpr int UGEMM_SMEM = USTAGES * U_STAGE_BYTES + U_PARK_BYTES + 1024;
+static_assert(UGEMM_SMEM + 4096 <= 232448, "shared memory per block");
 constexpr unsigned long long U_WAIT_NS = 1000000000ull;  // 1 s
 constexpr uint32_t U_WAIT_ITERS = 1u << 26;
 
-// byte offset of element (r, kk) of a K block in the core-matrix layout
+// byte offset of element (r, kk), kk < UBK, of a K block in the core-matrix layout
 __host__ __device__ __forceinline__ int core_off(int r, int kk) {
-    return (r >> 3) * 512 + (kk >> 2) * 128 + (r & 7) * 16 + (kk & 3) * 4;
+    return (r >> 3) * (UBK * 32) + (kk >> 2) * 128 + (r & 7) * 16 + (kk & 3) * 4;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -54,8 +101,8 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)_
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);        // start address
-    d |= (uint64_t)((128 >> 4) & 0x3FFF) << 16;    // LBO: K-adjacent core matrices
-    d |= (uint64_t)((512 >> 4) & 0x3FFF) << 32;    // SBO: 8-row groups
+    d |= (uint64_t)((128 >> 4) & 0x3FFF) << 16;         // LBO: K-adjacent core matrices
+    d |= (uint64_t)(((UBK * 32) >> 4) & 0x3FFF) << 32;  // SBO: 8-row groups
     d |= (uint64_t)1 << 46;                        // descriptor version 1; layout type 0 (no swizzle)
     return d;
 }
@@ -76,8 +123,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
-// wait for the phase of parity `parity` to complete; false after 1 s or 2^26 polls
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Wait for the phase of parity `parity`; false after 1 s, 2^26 polls, or once
+// *failed is set by another role.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* failed) {
     const uint32_t addr = smem_u32(bar);
     unsigned long long t0 = 0;
     for (uint32_t it = 0; it < U_WAIT_ITERS; ++it) {
@@ -91,7 +139,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
             : "memory");
         if (done) return true;
         if ((it & 255) == 255) {
-            unsigned long long t = gtimer();
+            if (failed && *failed) return false;
+            const unsigned long long t = gtimer();
             if (t0 == 0)
                 t0 = t;
             else if (t - t0 > U_WAIT_NS)
@@ -99,6 +148,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         }
     }
     return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
@@ -135,16 +188,25 @@ __device__ __forceinline__ uint32_t tf32_bits(float x) {
     return r;
 }
 
+// operator split: hi = TF32 rounding of x, lo = TF32 rounding of the rest
 __device__ __forceinline__ void split2(float x, uint32_t& hi, uint32_t& lo) {
     hi = tf32_bits(x);
     lo = tf32_bits(x - __uint_as_float(hi));
+}
+
+// gathered-column split in place: hi = x with the 13 low mantissa bits cleared
+// (exact), lo = TF32 rounding of x - hi
+__device__ __forceinline__ void split_mask(uint32_t& w, uint32_t& lo) {
+    const uint32_t hi = w & 0xFFFFE000u;
+    lo = tf32_bits(__uint_as_float(w) - __uint_as_float(hi));
+    w = hi;
 }
 
 // ---------------------------------------------------------------- packing
 // Real, interleaved, split, blocked copy of a complex operator (setup only).
 // Row tile t (complex rows 128t .. 128t+rows_t, N_t = round_up(2 rows_t, 16)
 // real rows) starts at dst + t * tile_stride floats and holds, per K block b,
-// the hi block (N_t x 16 TF32 in core-matrix order) then the lo block.
+// the hi block (N_t x 8 TF32 in core-matrix order) then the lo block.
 __global__ void umma_pack_kernel(const UmmaPackJob* __restrict__ jobs, int njobs) {
     for (int j = blockIdx.y; j < njobs; j += gridDim.y) {
         const UmmaPackJob J = jobs[j];
@@ -184,55 +246,60 @@ void launch_umma_pack(const UmmaPackJob* jobs_dev, int njobs, cudaStream_t s) {
     umma_pack_kernel<<<grid, 256, 0, s>>>(jobs_dev, njobs);
 }
 
-size_t umma_tile_stride(int k) { return (size_t)((2 * k + UBK - 1) / UBK) * 2 * UNMAX * UBK; }
-
-size_t umma_packed_floats(int m, int k) {
-    const int nkb = (2 * k + UBK - 1) / UBK;
-    const int nt = (m + 127) / 128;
-    const int last = m - (nt - 1) * 128;
-    return (size_t)(nt - 1) * umma_tile_stride(k) + (size_t)nkb * 2 * (((2 * last + 15) / 16) * 16) * UBK;
-}
-
 int umma_nkb(int k) { return (2 * k + UBK - 1) / UBK; }
 
+size_t umma_tile_stride(int k) { return (size_t)umma_nkb(k) * 2 * UNMAX * UBK; }
+
+size_t umma_packed_floats(int m, int k) {
+    const int nt = (m + 127) / 128;
+    const int last = m - (nt - 1) * 128;
+    return (size_t)(nt - 1) * umma_tile_stride(k) + (size_t)umma_nkb(k) * 2 * (((2 * last + 15) / 16) * 16) * UBK;
+}
+
 // ---------------------------------------------------------------- GEMM
-__global__ void __launch_bounds__(UTHREADS) umma_cgemm_kernel(const UmmaProblem* __restrict__ probs,
-                                                              const UmmaTile* __restrict__ tiles,
-                                                              const long long* __restrict__ xoff,
-                                                              const long long* __restrict__ yoff,
-                                                              const float2* __restrict__ X, float2* Y, int mode,
-                                                              int* err) {
+struct TileInfo {
+    UmmaTile t;
+    UmmaProblem p;
+};
+__device__ __forceinline__ TileInfo tile_info(const UmmaProblem* probs, const UmmaTile* tiles, int ti) {
+    TileInfo r;
+    r.t = tiles[ti];
+    r.p = probs[r.t.prob];
+    return r;
+}
+__device__ __forceinline__ int tile_n(int rows) { return ((2 * rows + 15) / 16) * 16; }
+
+__global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaProblem* __restrict__ probs,
+                                                                 const UmmaTile* __restrict__ tiles, int ntiles,
+                                                                 const long long* __restrict__ xoff,
+                                                                 const long long* __restrict__ yoff,
+                                                                 const float2* __restrict__ X, float2* Y, int mode,
+                                                                 int* err) {
     extern __shared__ __align__(1024) unsigned char usm_raw[];
-    __shared__ __align__(8) uint64_t bar_b[2], bar_mma[2];
+    __shared__ __align__(8) uint64_t full[USTAGES], empty[USTAGES], tmem_full[2], tmem_empty[2];
     __shared__ uint32_t tmem_base;
-    __shared__ long long xo[UM], yo[UM];
-    __shared__ int failed;
+    __shared__ int failed_s;
+    volatile int* failed = &failed_s;
     unsigned char* usm = (unsigned char*)(((uintptr_t)usm_raw + 1023) & ~(uintptr_t)1023);
+    float2* park_all = reinterpret_cast<float2*>(usm + USTAGES * U_STAGE_BYTES);
 
-    const UmmaTile t = tiles[blockIdx.x];
-    const UmmaProblem p = probs[t.prob];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int ncol = min(UM, p.ncol - t.col0);
-    const int rows = t.rows;                     // complex rows of this tile
-    const int N = ((2 * rows + 15) / 16) * 16;   // real rows (MMA N)
-    const int nkb = p.nkb;
-    const char* Bt = reinterpret_cast<const char*>(p.B + (size_t)t.rtile * p.tile_stride);
-    const uint32_t blk_bytes = (uint32_t)N * UBK * 4;
-
-    xo[tid] = tid < ncol ? xoff[p.col0 + t.col0 + tid] : -1;
-    yo[tid] = tid < ncol ? yoff[p.col0 + t.col0 + tid] : -1;
     if (tid == 0) {
-        failed = 0;
-        for (int s = 0; s < 2; ++s) {
-            mbar_init(&bar_b[s], 1);
-            mbar_init(&bar_mma[s], 1);
+        failed_s = 0;
+        for (int s = 0; s < USTAGES; ++s) {
+            mbar_init(&full[s], U_FULL_COUNT);
+            mbar_init(&empty[s], 1);      // tcgen05.commit
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&tmem_full[a], 1);    // tcgen05.commit
+            mbar_init(&tmem_empty[a], U_EMPTY_ACC_COUNT);
         }
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    if (warp == 0) {  // 256 TMEM columns: 128 lanes x 256 FP32 accumulators
+    if (warp == 0) {  // 512 TMEM columns: two accumulators of 128 lanes x 256 FP32
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                          smem_u32(&tmem_base)),
-                     "r"(256)
+                     "r"(512)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
@@ -241,145 +308,257 @@ __global__ void __launch_bounds__(UTHREADS) umma_cgemm_kernel(const UmmaProblem*
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = tmem_base;
 
-    // gathered columns: per K block each thread handles 4 (column, 2 complex) pieces;
-    // a warp instruction covers 8 columns x 4 pieces -> 16-byte conflict-free stores
-    const int q4 = lane & 3;
-    float2 pre[4][2];
-    auto fetch_a = [&](int kb) {
+    if (warp < W_LOAD_B) {
+        // ------------------------------------------------ gathered columns
+        // producer set `set` takes the blocks g = set, set + UPSETS, ... of the block
+        // sequence of this block's tiles; within a set, warp cw covers columns 32cw ..
+        // 32cw + 31, load i columns 32cw + 8i .. +7, lane = (column, complex q); blocks
+        // are prefetched UPREF deep into registers and split into a ring slot once free
+        const int set = warp >> 2, cw = warp & 3;
+        // load i covers columns 32cw + i (32 / CPB) .., CPB lanes per column
+        const int q = lane % CPB;
+        int coff[CPB];  // core_off(column, 2q)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int r = warp * 32 + c * 8 + (lane >> 2);
-            const int kc = kb * (UBK / 2) + 2 * q4;
-            const long long o = xo[r];
-            pre[c][0] = (o >= 0 && kc < p.k) ? X[o + kc] : make_float2(0.f, 0.f);
-            pre[c][1] = (o >= 0 && kc + 1 < p.k) ? X[o + kc + 1] : make_float2(0.f, 0.f);
-        }
-    };
-    auto store_a = [&](int s) {
-        unsigned char* ahi = usm + s * U_STAGE_BYTES;
-        unsigned char* alo = ahi + U_A_BYTES;
+        for (int i = 0; i < CPB; ++i) coff[i] = core_off(cw * 32 + i * (32 / CPB) + lane / CPB, 2 * q);
+        // load cursor: tile ti_i, block kb_i of nkb_i, its columns' offsets xr[]
+        int ti_i = blockIdx.x, kb_i = 0, nkb_i = 0, k_i = 0;
+        long long xr[CPB];
+        auto load_tile = [&]() {
+            if (ti_i >= ntiles) return;
+            const TileInfo T = tile_info(probs, tiles, ti_i);
+            nkb_i = T.p.nkb;
+            k_i = T.p.k;
+            const int ncol = min(UM, T.p.ncol - T.t.col0);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int r = warp * 32 + c * 8 + (lane >> 2);
-            uint4 h, l;
-            split2(pre[c][0].x, h.x, l.x);
-            split2(pre[c][0].y, h.y, l.y);
-            split2(pre[c][1].x, h.z, l.z);
-            split2(pre[c][1].y, h.w, l.w);
-            const int off = core_off(r, 4 * q4);
-            *reinterpret_cast<uint4*>(ahi + off) = h;
-            *reinterpret_cast<uint4*>(alo + off) = l;
-        }
-    };
-    // operator K block (hi and lo) into stage s: one thread, two bulk copies
-    auto load_b = [&](int s, int kb) {
-        unsigned char* bhi = usm + s * U_STAGE_BYTES + 2 * U_A_BYTES;
-        const char* src = Bt + (size_t)kb * 2 * blk_bytes;
-        mbar_expect_tx(&bar_b[s], 2 * blk_bytes);
-        bulk_g2s(bhi, src, blk_bytes, &bar_b[s]);
-        bulk_g2s(bhi + U_B_BYTES, src + blk_bytes, blk_bytes, &bar_b[s]);
-    };
-
-    int last_load = -1, last_commit = -1;  // tracked by thread 0
-    if (tid == 0) {
-        load_b(0, 0);
-        last_load = 0;
-    }
-    fetch_a(0);
-    store_a(0);
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    __syncthreads();
-    const uint32_t idesc = idesc_tf32(N);
-    for (int kb = 0; kb < nkb; ++kb) {
-        const int s = kb & 1;
-        if (kb + 1 < nkb) fetch_a(kb + 1);  // global loads in flight during the MMA issue
-        if (tid == 0 && !failed) {
-            if (!mbar_wait(&bar_b[s], (kb >> 1) & 1)) {
-                failed = 1;
-            } else {
-                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                const uint32_t ahi = smem_u32(usm + s * U_STAGE_BYTES), alo = ahi + U_A_BYTES;
-                const uint32_t bhi = ahi + 2 * U_A_BYTES, blo = bhi + U_B_BYTES;
+            for (int i = 0; i < CPB; ++i) {
+                const int c = cw * 32 + i * (32 / CPB) + lane / CPB;
+                xr[i] = c < ncol ? xoff[T.p.col0 + T.t.col0 + c] : -1;
+            }
+        };
+        auto advance = [&]() {
+            if (++kb_i == nkb_i) {
+                kb_i = 0;
+                ti_i += gridDim.x;
+                load_tile();
+            }
+        };
+        auto fetch = [&](float2(&dst)[CPB]) {  // the block at the cursor, then advance it
+            const int kc = kb_i * CPB + q;
 #pragma unroll
-                for (int ks = 0; ks < UBK / 8; ++ks) {  // K = 8 per MMA: two core-matrix columns, 256 B
-                    const uint32_t o = ks * 256;
-                    umma_tf32(tmem, sdesc(ahi + o), sdesc(bhi + o), idesc, (kb > 0 || ks > 0) ? 1u : 0u);
-                    umma_tf32(tmem, sdesc(alo + o), sdesc(bhi + o), idesc, 1u);
-                    umma_tf32(tmem, sdesc(ahi + o), sdesc(blo + o), idesc, 1u);
+            for (int i = 0; i < CPB; ++i)
+                dst[i] = (xr[i] >= 0 && kc < k_i) ? X[xr[i] + kc] : make_float2(0.f, 0.f);
+            for (int a = 0; a < UPSETS && ti_i < ntiles; ++a) advance();
+        };
+        load_tile();
+        for (int a = 0; a < set && ti_i < ntiles; ++a) advance();
+        float2 pre[UPREF][CPB];
+        int loaded = 0;
+#pragma unroll
+        for (int d = 0; d < UPREF; ++d)
+            if (ti_i < ntiles) {
+                fetch(pre[d]);
+                ++loaded;
+            }
+        int n = 0;  // this set's blocks done; block n sits in pre[n % UPREF]
+        while (n < loaded && !*failed) {
+#pragma unroll
+            for (int d = 0; d < UPREF; ++d) {
+                if (n >= loaded || *failed) break;
+                const int g = n * UPSETS + set;
+                const int s = g % USTAGES;
+                if (g >= USTAGES && !mbar_wait(&empty[s], ((g / USTAGES) - 1) & 1, failed)) {
+                    *failed = 1;
+                    break;
                 }
-                umma_commit(&bar_mma[s]);
-                last_commit = kb;
-            }
-        }
-        if (kb + 1 < nkb) {
-            const int ns = s ^ 1;
-            if (kb >= 1) {  // the MMAs of block kb-1 must be done reading stage ns
-                if (tid == 0 && !failed && !mbar_wait(&bar_mma[ns], ((kb - 1) >> 1) & 1)) failed = 1;
-                __syncthreads();
-            }
-            if (tid == 0 && !failed) {
-                load_b(ns, kb + 1);
-                last_load = kb + 1;
-            }
-            store_a(ns);
-            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        }
-        __syncthreads();
-    }
-    // the last commit tracks completion of every MMA issued before it
-    if (tid == 0 && !failed && !mbar_wait(&bar_mma[(nkb - 1) & 1], ((nkb - 1) >> 1) & 1)) failed = 1;
-    if (tid == 0 && failed) {  // drain what is still in flight, bounded
-        if (last_commit >= 0) mbar_wait(&bar_mma[last_commit & 1], (last_commit >> 1) & 1);
-        if (last_load >= 0) mbar_wait(&bar_b[last_load & 1], (last_load >> 1) & 1);
-        atomicExch(err, 1);
-    }
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    if (!failed) {
-        // warp w reads TMEM lanes 32w..32w+31: each thread one gathered column, N FP32 values
-        const int col = warp * 32 + lane;
-        float2* y = (col < ncol) ? Y + yo[col] + t.row0 : nullptr;
-        for (int c0 = 0; c0 < N; c0 += 8) {
-            uint32_t v[8];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0)
-                : "memory");
-            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-            if (!y) continue;
+                unsigned char* ahi = usm + s * U_STAGE_BYTES;
+                unsigned char* alo = ahi + U_A_BYTES;
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int i = (c0 >> 1) + e;  // complex row within the tile
-                if (i >= rows) break;
-                const float2 val = make_float2(__uint_as_float(v[2 * e]), __uint_as_float(v[2 * e + 1]));
-                if (mode == GEMM_SET) {
-                    y[i] = val;
-                } else if (mode == GEMM_ADD) {
-                    const float2 o = y[i];
-                    y[i] = make_float2(o.x + val.x, o.y + val.y);
+                for (int i = 0; i < CPB; ++i) {
+                    uint2 w = make_uint2(__float_as_uint(pre[d][i].x), __float_as_uint(pre[d][i].y));
+                    uint2 l;
+                    split_mask(w.x, l.x);
+                    split_mask(w.y, l.y);
+                    *reinterpret_cast<uint2*>(ahi + coff[i]) = w;
+                    *reinterpret_cast<uint2*>(alo + coff[i]) = l;
+                }
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                if (UELECT) {
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&full[s]);
                 } else {
-                    atomicAdd(&y[i].x, val.x);
-                    atomicAdd(&y[i].y, val.y);
+                    mbar_arrive(&full[s]);
+                }
+                if (ti_i < ntiles) {
+                    fetch(pre[d]);
+                    ++loaded;
+                }
+                ++n;
+            }
+        }
+    } else if (warp == W_LOAD_B) {
+        // ------------------------------------------------ operator blocks
+        if (lane == 0) {
+            int g = 0;
+            for (int ti = blockIdx.x; ti < ntiles && !*failed; ti += gridDim.x) {
+                const TileInfo T = tile_info(probs, tiles, ti);
+                const char* Bt = reinterpret_cast<const char*>(T.p.B + (size_t)T.t.rtile * T.p.tile_stride);
+                const uint32_t blk = (uint32_t)tile_n(T.t.rows) * UBK * 4;
+                for (int kb = 0; kb < T.p.nkb; ++kb, ++g) {
+                    const int s = g % USTAGES;
+                    if (g >= USTAGES && !mbar_wait(&empty[s], ((g / USTAGES) - 1) & 1, failed)) {
+                        *failed = 1;
+                        break;
+                    }
+                    unsigned char* bhi = usm + s * U_STAGE_BYTES + 2 * U_A_BYTES;
+                    const char* src = Bt + (size_t)kb * 2 * blk;
+                    mbar_expect_tx(&full[s], 2 * blk);
+                    bulk_g2s(bhi, src, blk, &full[s]);
+                    bulk_g2s(bhi + U_B_BYTES, src + blk, blk, &full[s]);
                 }
             }
         }
+    } else if (warp == W_MMA) {
+        // ------------------------------------------------ MMA issue
+        if (lane == 0) {
+            int g = 0, it = 0, last = -1;
+            for (int ti = blockIdx.x; ti < ntiles && !*failed; ti += gridDim.x, ++it) {
+                const TileInfo T = tile_info(probs, tiles, ti);
+                const uint32_t idesc = idesc_tf32(tile_n(T.t.rows));
+                const int acc = it & 1;
+                if (it >= 2 && !mbar_wait(&tmem_empty[acc], ((it >> 1) - 1) & 1, failed)) {
+                    *failed = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t d = tmem + (uint32_t)(acc * 256);
+                for (int kb = 0; kb < T.p.nkb; ++kb, ++g) {
+                    const int s = g % USTAGES;
+                    if (!mbar_wait(&full[s], (g / USTAGES) & 1, failed)) {
+                        *failed = 1;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                    const uint32_t ahi = smem_u32(usm + s * U_STAGE_BYTES), alo = ahi + U_A_BYTES;
+                    const uint32_t bhi = ahi + 2 * U_A_BYTES, blo = bhi + U_B_BYTES;
+#pragma unroll
+                    for (int ks = 0; ks < UBK / 8; ++ks) {  // K = 8 per MMA: two core matrices, 256 B
+                        const uint32_t o = ks * 256;
+                        umma_tf32(d, sdesc(ahi + o), sdesc(bhi + o), idesc, (kb > 0 || ks > 0) ? 1u : 0u);
+                        umma_tf32(d, sdesc(alo + o), sdesc(bhi + o), idesc, 1u);
+                        umma_tf32(d, sdesc(ahi + o), sdesc(blo + o), idesc, 1u);
+                    }
+                    umma_commit(&empty[s]);
+                    last = g;
+                }
+                if (*failed) break;
+                umma_commit(&tmem_full[acc]);
+            }
+            if (*failed && last >= 0)  // let the MMAs already issued finish before TMEM is freed
+                mbar_wait(&empty[last % USTAGES], (last / USTAGES) & 1, nullptr);
+        }
+    } else {
+        // ------------------------------------------------ epilogue
+        const int qw = warp & 3;  // TMEM lanes 32 qw .. 32 qw + 31 = tile columns
+        float2* park = park_all + qw * (32 * (PCH + 1));
+        int it = 0;
+        for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x, ++it) {
+            const TileInfo T = tile_info(probs, tiles, ti);
+            const int ncol = min(UM, T.p.ncol - T.t.col0);
+            const int rows = T.t.rows, N = tile_n(rows);
+            const int acc = it & 1;
+            const int mycol = qw * 32 + lane;
+            const long long my_yo = mycol < ncol ? yoff[T.p.col0 + T.t.col0 + mycol] + T.t.row0 : 0;
+            bool ok = !*failed && mbar_wait(&tmem_full[acc], (it >> 1) & 1, failed);
+            ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld is warp-collective
+            if (!ok) {
+                *failed = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t src = tmem + ((uint32_t)(qw * 32) << 16) + (uint32_t)(acc * 256);
+            for (int c0 = 0; c0 < N; c0 += 2 * PCH) {
+#pragma unroll
+                for (int h = 0; h < 2 * PCH; h += 16) {
+                    if (c0 + h < N) {  // N is a multiple of 16
+                        uint32_t v[16];
+                        asm volatile(
+                            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+                            "%15}, [%16];\n"
+                            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                              "=r"(v[14]), "=r"(v[15])
+                            : "r"(src + (uint32_t)(c0 + h))
+                            : "memory");
+                        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+                        for (int e = 0; e < 8; ++e)
+                            park[lane * (PCH + 1) + (h >> 1) + e] =
+                                make_float2(__uint_as_float(v[2 * e]), __uint_as_float(v[2 * e + 1]));
+                    }
+                }
+                if (c0 + 2 * PCH >= N) {  // accumulator fully read: hand it back to the MMA issuer
+                    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+                    if (UELECT) {
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&tmem_empty[acc]);
+                    } else {
+                        mbar_arrive(&tmem_empty[acc]);
+                    }
+                }
+                __syncwarp();
+                // 32 / PCH columns per store instruction, PCH consecutive rows each
+                const int sub = lane / PCH, r = lane % PCH;
+                const int i = (c0 >> 1) + r;  // complex row of this lane
+                for (int cc = 0; cc < 32; cc += 32 / PCH) {
+                    const int col = cc + sub;
+                    const long long yb = __shfl_sync(0xffffffffu, my_yo, col);
+                    if (qw * 32 + cc >= ncol) break;
+                    if (i >= rows || qw * 32 + col >= ncol) continue;
+                    const float2 val = park[col * (PCH + 1) + r];
+                    float2* y = Y + yb + i;
+                    if (mode == GEMM_SET) {
+                        *y = val;
+                    } else if (mode == GEMM_ADD) {
+                        const float2 o = *y;
+                        *y = make_float2(o.x + val.x, o.y + val.y);
+                    } else {
+                        atomicAdd(y, val);
+                    }
+                }
+                __syncwarp();
+            }
+        }
+    }
+    __syncthreads();
+    if (*failed && tid == 0) {
+        // bounded drain of operator copies still in flight, then report
+        const unsigned long long t0 = gtimer();
+        while (gtimer() - t0 < 200000ull) __nanosleep(1000);
+        atomicExch(err, 1);
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(256) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512) : "memory");
 }
+
+static int g_umma_sms = 0;
 
 void umma_init() {
     cudaFuncSetAttribute(umma_cgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, UGEMM_SMEM);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_umma_sms, cudaDevAttrMultiProcessorCount, dev);
 }
 
 void launch_umma_cgemm(const UmmaProblem* probs, const UmmaTile* tiles, int ntiles, const long long* xoff,
                        const long long* yoff, const void* X, void* Y, int mode, int* err, cudaStream_t s) {
     if (ntiles == 0) return;
-    umma_cgemm_kernel<<<ntiles, UTHREADS, UGEMM_SMEM, s>>>(probs, tiles, xoff, yoff, static_cast<const float2*>(X),
-                                                          static_cast<float2*>(Y), mode, err);
+    const int sms = g_umma_sms > 0 ? g_umma_sms : 148;
+    const int grid = ntiles < sms ? ntiles : sms;
+    umma_cgemm_kernel<<<grid, UTHREADS, UGEMM_SMEM, s>>>(probs, tiles, ntiles, xoff, yoff,
+                                                        static_cast<const float2*>(X), static_cast<float2*>(Y), mode,
+                                                        err);
 }
 
 }  // namespace ddfmm
