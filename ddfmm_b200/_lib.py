@@ -16,6 +16,8 @@ EXPORTS = (
     "ddfmm_session_stats", "ddfmm_session_destroy", "ddfmm_last_error", "ddfmm_tree_stats",
     "ddfmm_profile_enable", "ddfmm_profile_read", "ddfmm_eval_device_noalloc",
     "ddfmm_session_create_ex", "ddfmm_eval_c64", "ddfmm_eval_device_c64",
+    "ddfmm_batch_create", "ddfmm_batch_eval_c64", "ddfmm_batch_eval_device_c64", "ddfmm_batch_launches",
+    "ddfmm_batch_destroy",
 )
 PLAIN_FP64, MIXED, MIXED_MMA_SYNC = 0, 1, 2
 
@@ -95,6 +97,17 @@ def load():
     lib.ddfmm_profile_read.restype = C.c_int
     lib.ddfmm_last_error.argtypes = []
     lib.ddfmm_last_error.restype = C.c_char_p
+    vpp = C.POINTER(C.c_void_p)
+    lib.ddfmm_batch_create.argtypes = [vpp, C.c_int, vpp]
+    lib.ddfmm_batch_create.restype = C.c_int
+    lib.ddfmm_batch_eval_c64.argtypes = [C.c_void_p, vpp, vpp]
+    lib.ddfmm_batch_eval_c64.restype = C.c_int
+    lib.ddfmm_batch_eval_device_c64.argtypes = [C.c_void_p, vpp, vpp, C.c_void_p]
+    lib.ddfmm_batch_eval_device_c64.restype = C.c_int
+    lib.ddfmm_batch_launches.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+    lib.ddfmm_batch_launches.restype = C.c_int
+    lib.ddfmm_batch_destroy.argtypes = [C.c_void_p]
+    lib.ddfmm_batch_destroy.restype = C.c_int
     _lib = lib
     return lib
 

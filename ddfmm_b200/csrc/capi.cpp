@@ -9,10 +9,20 @@
 #include <string>
 
 #include "../../include/ddfmm.h"
+#include "batch.hpp"
 #include "session.hpp"
 
 struct ddfmm_session {
     ddfmm::Session* impl;
+};
+
+struct ddfmm_batch {
+    ddfmm::Batch* impl = nullptr;
+    int* d_active = nullptr;  // device mask of the sessions a call computes
+    int* h_active = nullptr;  // pinned host copy
+    cudaEvent_t copied = nullptr;  // the last mask copy has left h_active
+    cudaStream_t stream = nullptr;
+    int device = 0;
 };
 
 namespace ddfmm {
@@ -21,6 +31,26 @@ double2* noalloc_scratch(size_t* capacity);  // noalloc.cu
 
 namespace {
 thread_local std::string g_err;
+
+#define CKA(x)                                                                                     \
+    do {                                                                                           \
+        cudaError_t e_ = (x);                                                                      \
+        if (e_ != cudaSuccess)                                                                     \
+            throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e_) + " (" + \
+                                     #x + ")");                                                    \
+    } while (0)
+
+// makes `device` current for a scope and restores the caller's device after
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        CKA(cudaSetDevice(device));
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
 
 int fail(int code, const std::string& msg) {
     g_err = msg;
@@ -266,6 +296,107 @@ int ddfmm_session_destroy(ddfmm_session* s) {
     int rc = guarded([&] { delete s->impl; });
     delete s;
     return rc;
+}
+
+static void batch_free(ddfmm_batch* b) {
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    delete b->impl;
+    if (b->d_active) cudaFree(b->d_active);
+    if (b->h_active) cudaFreeHost(b->h_active);
+    if (b->copied) cudaEventDestroy(b->copied);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+int ddfmm_batch_create(ddfmm_session* const* sessions, int n, ddfmm_batch** out) {
+    if (!out) return fail(DDFMM_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!sessions || n <= 0) return fail(DDFMM_EINVAL, "need at least one session");
+    std::vector<ddfmm::Session*> v;
+    for (int i = 0; i < n; ++i) {
+        if (!sessions[i]) return fail(DDFMM_EINVAL, "session is NULL");
+        v.push_back(sessions[i]->impl);
+    }
+    ddfmm_batch* b = new (std::nothrow) ddfmm_batch();
+    if (!b) return fail(DDFMM_ENOMEM, "host out of memory");
+    int rc = guarded([&] {
+        b->device = v[0]->device();
+        DeviceGuard dg(b->device);
+        b->impl = new ddfmm::Batch(v);
+        CKA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        CKA(cudaMalloc(&b->d_active, sizeof(int) * n));
+        CKA(cudaMallocHost(&b->h_active, sizeof(int) * n));
+        CKA(cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming));
+        CKA(cudaEventRecord(b->copied, b->stream));
+    });
+    if (rc != DDFMM_OK) {
+        batch_free(b);
+        return rc;
+    }
+    *out = b;
+    return DDFMM_OK;
+}
+
+// mask from the non-NULL inputs, copied to the device on st; then the graph
+static void batch_launch(ddfmm_batch* b, const void* const* den, cudaStream_t st) {
+    const int n = b->impl->size();
+    CKA(cudaEventSynchronize(b->copied));
+    for (int i = 0; i < n; ++i) b->h_active[i] = den[i] != nullptr;
+    CKA(cudaMemcpyAsync(b->d_active, b->h_active, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    CKA(cudaEventRecord(b->copied, st));
+    b->impl->run_graph(b->d_active, st);
+}
+
+int ddfmm_batch_eval_c64(ddfmm_batch* b, const float* const* den, float* const* val) {
+    if (!b || !den || !val) return fail(DDFMM_EINVAL, "NULL argument");
+    return guarded([&] {
+        DeviceGuard dg(b->device);
+        const int n = b->impl->size();
+        for (int i = 0; i < n; ++i) {
+            if (den[i] && !val[i]) throw std::invalid_argument("val[i] is NULL for a computed session");
+            if (den[i])
+                CKA(cudaMemcpyAsync(b->impl->den(i), den[i], sizeof(float2) * b->impl->session(i)->npts(),
+                                    cudaMemcpyHostToDevice, b->stream));
+        }
+        batch_launch(b, reinterpret_cast<const void* const*>(den), b->stream);
+        for (int i = 0; i < n; ++i)
+            if (den[i])
+                CKA(cudaMemcpyAsync(val[i], b->impl->val(i), sizeof(float2) * b->impl->session(i)->npts(),
+                                    cudaMemcpyDeviceToHost, b->stream));
+        b->impl->check_error(b->stream);
+    });
+}
+
+int ddfmm_batch_eval_device_c64(ddfmm_batch* b, const void* const* den_dev, void* const* val_dev, void* stream) {
+    if (!b || !den_dev || !val_dev) return fail(DDFMM_EINVAL, "NULL argument");
+    return guarded([&] {
+        DeviceGuard dg(b->device);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+        const int n = b->impl->size();
+        for (int i = 0; i < n; ++i) {
+            if (den_dev[i] && !val_dev[i]) throw std::invalid_argument("val_dev[i] is NULL for a computed session");
+            if (den_dev[i])
+                CKA(cudaMemcpyAsync(b->impl->den(i), den_dev[i], sizeof(float2) * b->impl->session(i)->npts(),
+                                    cudaMemcpyDeviceToDevice, st));
+        }
+        batch_launch(b, den_dev, st);
+        for (int i = 0; i < n; ++i)
+            if (den_dev[i])
+                CKA(cudaMemcpyAsync(val_dev[i], b->impl->val(i), sizeof(float2) * b->impl->session(i)->npts(),
+                                    cudaMemcpyDeviceToDevice, st));
+        CKA(cudaGetLastError());
+    });
+}
+
+int ddfmm_batch_launches(ddfmm_batch* b, int* launches) {
+    if (!b || !launches) return fail(DDFMM_EINVAL, "NULL argument");
+    *launches = b->impl->launches();
+    return DDFMM_OK;
+}
+
+int ddfmm_batch_destroy(ddfmm_batch* b) {
+    if (!b) return DDFMM_OK;
+    return guarded([&] { batch_free(b); });
 }
 
 }  // extern "C"

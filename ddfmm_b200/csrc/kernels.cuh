@@ -88,12 +88,61 @@ enum Precision { PRECISION_FP64 = 0, PRECISION_MIXED = 1, PRECISION_MIXED_MMA_SY
 void cgemm_init();
 void launch_cgemm(const GemmProblem* probs_dev, const GemmTile* tiles_dev, int ntiles, const long long* xoff,
                   const long long* yoff, const void* X, void* Y, int mode, cudaStream_t s);
-void launch_pt32(const PtItem* items_dev, int nitems, const PtSrc* srcs_dev, int kernel, cudaStream_t s);
+
+// Multi-instance launches of the mixed form.  A launch is a device array of
+// per-instance sub-launches plus the prefix sums of their work items (nsub + 1
+// entries); a sub-launch is skipped when `active` (indexed by `inst`) is given
+// and holds 0.  A single session is a launch with one sub-launch.
+struct PtSub {
+    const PtItem* items;
+    const PtSrc* srcs;
+    int nitems;
+    int kernel;  // KERNEL_HELM / KERNEL_EXPR
+    int inst;
+    int pad;
+};
+struct VfSub {  // V-list source spectra, one work item per source box
+    VlistLevel L;
+    const int* boxes;
+    const float2* upeq;
+    float2* spec;
+    int nbox;
+    int inst;
+};
+struct VaSub {  // V-list accumulation, one work item per target box
+    VlistLevel L;
+    const int* trg;
+    const int* vptr;
+    const int* vsrc;
+    const int* voff;
+    const float2* spec;
+    float2* dnchk;
+    int ntrg;
+    int inst;
+};
+struct MoveSub {  // complex64 point data between point-id and leaf order
+    const void* in;
+    const int* perm;
+    void* out;
+    int n;
+    int inst;
+};
+struct ZeroSub {
+    void* p;
+    long long n8;  // 8-byte words
+    int inst;
+    int pad;
+};
+void launch_pt32(const PtSub* subs, const int* prefix, int nsub, int nitems, const int* active, cudaStream_t s);
 void vlist32_init(int G);
-void launch_vlist_forward32(const VlistLevel& L, const int* boxes, int nbox, const void* upeq, void* spec,
-                            cudaStream_t s);
-void launch_vlist_accum32(const VlistLevel& L, const int* trg, int ntrg, const int* vptr, const int* vsrc,
-                          const int* voff, const void* spec, void* dnchk, cudaStream_t s);
+void launch_vlist_forward32(const VfSub* subs, const int* prefix, int nsub, int nbox, int G, const int* active,
+                            void* spec_override, cudaStream_t s);
+void launch_vlist_accum32(const VaSub* subs, const int* prefix, int nsub, int ntrg, int G, const int* active,
+                          const void* spec_override, cudaStream_t s);
+void launch_move32(const MoveSub* subs, const int* prefix, int nsub, int n, const int* active, int scatter,
+                   cudaStream_t s);
+void launch_zero(const ZeroSub* subs, const long long* prefix, int nsub, long long n8, const int* active,
+                 cudaStream_t s);
 void launch_gather32(const void* den, const int* perm, void* out, int n, int c64, cudaStream_t s);
 void launch_scatter32(const void* in, const int* perm, void* val, int n, int c64, cudaStream_t s);
 void launch_to_c64(const double2* a, float2* b, long long n, cudaStream_t s);
@@ -114,6 +163,18 @@ struct UmmaTile {
     int col0;   // relative to the problem's first column
     int pad;
 };
+struct UmmaSub {  // one instance's part of a multi-instance GEMM launch
+    const UmmaProblem* probs;
+    const UmmaTile* tiles;
+    const long long* xoff;
+    const long long* yoff;
+    const float2* X;
+    float2* Y;
+    int ntiles;
+    int mode;
+    int inst;
+    int pad;
+};
 struct UmmaPackJob {
     const float2* A;  // complex FP32 operator, column-major
     float* dst;
@@ -125,8 +186,8 @@ int umma_nkb(int k);
 size_t umma_tile_stride(int k);
 size_t umma_packed_floats(int m, int k);
 void launch_umma_pack(const UmmaPackJob* jobs_dev, int njobs, cudaStream_t s);
-void launch_umma_cgemm(const UmmaProblem* probs, const UmmaTile* tiles, int ntiles, const long long* xoff,
-                       const long long* yoff, const void* X, void* Y, int mode, int* err, cudaStream_t s);
+void launch_umma_cgemm(const UmmaSub* subs, const int* prefix, int nsub, int ntiles, const int* active, int* err,
+                       cudaStream_t s);
 
 // gather/scatter helpers
 void launch_gather_den(const double2* den, const int* perm, double2* out, int n, cudaStream_t s);

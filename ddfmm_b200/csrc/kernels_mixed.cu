@@ -222,14 +222,35 @@ void launch_cgemm(const GemmProblem* probs, const GemmTile* tiles, int ntiles, c
 }
 
 // ---------------------------------------------------------------- points (FP32)
+// ---------------------------------------------------------------- multi-instance launches
+// Every mixed-form launch below walks a list of per-instance sub-launches
+// (one entry for a single session, one per session for a batch): work item i
+// of the launch belongs to sub-launch j with prefix[j] <= i < prefix[j+1], and
+// is skipped when active != nullptr and active[sub.inst] == 0.
+template <class T>
+__device__ __forceinline__ int find_sub(const T* __restrict__ prefix, int nsub, T i) {
+    int lo = 0, hi = nsub - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= i)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
 // One warp per item as pt_kernel; densities / outputs are float2 (the
 // descriptors' double2 pointers are reinterpreted).  Differences of the FP64
 // coordinates are taken in FP64, the kernel is evaluated in FP32.
-__global__ void pt32_kernel(const PtItem* __restrict__ items, int nitems, const PtSrc* __restrict__ srcs,
-                            int kernel) {
-    int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+__global__ void pt32_kernel(const PtSub* __restrict__ subs, const int* __restrict__ prefix, int nsub, int nitems,
+                            const int* __restrict__ active) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (w >= nitems) return;
-    const PtItem it = items[w];
+    const int j = find_sub(prefix, nsub, w);
+    const PtSub S = subs[j];
+    if (active && !active[S.inst]) return;
+    const PtItem it = S.items[w - prefix[j]];
     float2* out = reinterpret_cast<float2*>(it.out);
     for (int t = lane; t < it.trg.n; t += 32) {
         const double* tp = it.trg.x + 3 * t;
@@ -238,14 +259,14 @@ __global__ void pt32_kernel(const PtItem* __restrict__ items, int nitems, const 
         double tz = it.trg.scale * tp[2] + it.trg.shift[2];
         float2 acc = make_float2(0.f, 0.f);
         for (int s = it.src_begin; s < it.src_end; ++s) {
-            const PtSrc S = srcs[s];
-            const float2* den = reinterpret_cast<const float2*>(S.den);
-            for (int q = 0; q < S.src.n; ++q) {
-                const double* sp = S.src.x + 3 * q;
-                double sx = S.src.scale * sp[0] + S.src.shift[0];
-                double sy = S.src.scale * sp[1] + S.src.shift[1];
-                double sz = S.src.scale * sp[2] + S.src.shift[2];
-                cfma32(acc, kfun32(tx - sx, ty - sy, tz - sz, kernel), den[q]);
+            const PtSrc Q = S.srcs[s];
+            const float2* den = reinterpret_cast<const float2*>(Q.den);
+            for (int q = 0; q < Q.src.n; ++q) {
+                const double* sp = Q.src.x + 3 * q;
+                double sx = Q.src.scale * sp[0] + Q.src.shift[0];
+                double sy = Q.src.scale * sp[1] + Q.src.shift[1];
+                double sz = Q.src.scale * sp[2] + Q.src.shift[2];
+                cfma32(acc, kfun32(tx - sx, ty - sy, tz - sz, S.kernel), den[q]);
             }
         }
         float2 o = out[t];
@@ -253,21 +274,31 @@ __global__ void pt32_kernel(const PtItem* __restrict__ items, int nitems, const 
     }
 }
 
-void launch_pt32(const PtItem* items, int nitems, const PtSrc* srcs, int kernel, cudaStream_t s) {
+void launch_pt32(const PtSub* subs, const int* prefix, int nsub, int nitems, const int* active, cudaStream_t s) {
     if (nitems == 0) return;
-    pt32_kernel<<<(nitems * 32 + 255) / 256, 256, 0, s>>>(items, nitems, srcs, kernel);
+    pt32_kernel<<<(nitems * 32 + 255) / 256, 256, 0, s>>>(subs, prefix, nsub, nitems, active);
 }
 
 // ---------------------------------------------------------------- V list (FP32)
-// The pruned corner-cube transforms of kernels.cu in complex FP32.
-__global__ void vlist_forward32_kernel(VlistLevel L, const int* __restrict__ boxes, const float2* __restrict__ upeq,
-                                       float2* __restrict__ spec, const float2* __restrict__ twf) {
+// The pruned corner-cube transforms of kernels.cu in complex FP32; one block
+// per source box (forward) or target box (accumulate).  All sub-launches of a
+// launch share G = 2P; spec_override, when set, replaces every sub-launch's
+// spectra array (fixed-scratch entry point, single instance).
+__global__ void vlist_forward32_kernel(const VfSub* __restrict__ subs, const int* __restrict__ prefix, int nsub,
+                                       const int* __restrict__ active, float2* spec_override) {
     extern __shared__ float2 sm32[];
+    const int j = find_sub(prefix, nsub, (int)blockIdx.x);
+    const VfSub S = subs[j];
+    if (active && !active[S.inst]) return;
+    const VlistLevel& L = S.L;
+    const float2* twf = reinterpret_cast<const float2*>(L.twf);
+    const float2* upeq = S.upeq;
+    float2* spec = spec_override ? spec_override : S.spec;
     const int G = L.G, P = L.P, PP = P * P;
     float2* cube = sm32;
     float2* b1 = cube + PP * P;
     float2* b2 = b1 + G * PP;
-    const int b = boxes[blockIdx.x];
+    const int b = S.boxes[blockIdx.x - prefix[j]];
     for (int e = threadIdx.x; e < PP * P; e += blockDim.x) cube[e] = make_float2(0.f, 0.f);
     __syncthreads();
     for (int k = threadIdx.x; k < L.nE; k += blockDim.x) cube[L.cube_idx[k]] = upeq[(size_t)b * L.nE + k];
@@ -296,25 +327,29 @@ __global__ void vlist_forward32_kernel(VlistLevel L, const int* __restrict__ box
 }
 
 template <int G>
-__global__ void __launch_bounds__(256) vlist_accum32_kernel(VlistLevel L, const int* __restrict__ trg,
-                                                            const int* __restrict__ vptr,
-                                                            const int* __restrict__ vsrc,
-                                                            const int* __restrict__ voff,
-                                                            const float2* __restrict__ spec,
-                                                            float2* __restrict__ dnchk,
-                                                            const float2* __restrict__ twb) {
+__global__ void __launch_bounds__(256) vlist_accum32_kernel(const VaSub* __restrict__ subs,
+                                                            const int* __restrict__ prefix, int nsub,
+                                                            const int* __restrict__ active,
+                                                            const float2* spec_override) {
     extern __shared__ float2 sm32[];
     constexpr int P = G / 2, PP = P * P, G3 = G * G * G, NE = (G3 + 255) / 256;
+    const int j = find_sub(prefix, nsub, (int)blockIdx.x);
+    const VaSub S = subs[j];
+    if (active && !active[S.inst]) return;
+    const VlistLevel& L = S.L;
+    const float2* twb = reinterpret_cast<const float2*>(L.twb);
+    const float2* spec = spec_override ? spec_override : S.spec;
+    float2* dnchk = S.dnchk;
     float2* grid = sm32;
     float2* c1 = sm32 + G3;
     const float2* tns = reinterpret_cast<const float2*>(L.tns);
-    const int ti = blockIdx.x, t = trg[ti];
+    const int ti = blockIdx.x - prefix[j], t = S.trg[ti];
     float2 acc[NE];
 #pragma unroll
     for (int q = 0; q < NE; ++q) acc[q] = make_float2(0.f, 0.f);
-    for (int v = vptr[ti]; v < vptr[ti + 1]; ++v) {
-        const float2* sp = spec + (size_t)vsrc[v] * G3;
-        const float2* tn = tns + (size_t)voff[v] * G3;
+    for (int v = S.vptr[ti]; v < S.vptr[ti + 1]; ++v) {
+        const float2* sp = spec + (size_t)S.vsrc[v] * G3;
+        const float2* tn = tns + (size_t)S.voff[v] * G3;
 #pragma unroll
         for (int q = 0; q < NE; ++q) {
             int e = threadIdx.x + 256 * q;
@@ -370,27 +405,65 @@ void vlist32_init(int G) {
 }
 
 // L.tns, L.twf, L.twb hold float2 data in this form.
-void launch_vlist_forward32(const VlistLevel& L, const int* boxes, int nbox, const void* upeq, void* spec,
-                            cudaStream_t s) {
+void launch_vlist_forward32(const VfSub* subs, const int* prefix, int nsub, int nbox, int G, const int* active,
+                            void* spec_override, cudaStream_t s) {
     if (nbox == 0) return;
-    vlist_forward32_kernel<<<nbox, 256, vfwd32_smem(L.G, L.P), s>>>(
-        L, boxes, static_cast<const float2*>(upeq), static_cast<float2*>(spec),
-        reinterpret_cast<const float2*>(L.twf));
+    vlist_forward32_kernel<<<nbox, 256, vfwd32_smem(G, G / 2), s>>>(subs, prefix, nsub, active,
+                                                                     static_cast<float2*>(spec_override));
 }
 
-void launch_vlist_accum32(const VlistLevel& L, const int* trg, int ntrg, const int* vptr, const int* vsrc,
-                          const int* voff, const void* spec, void* dnchk, cudaStream_t s) {
+void launch_vlist_accum32(const VaSub* subs, const int* prefix, int nsub, int ntrg, int G, const int* active,
+                          const void* spec_override, cudaStream_t s) {
     if (ntrg == 0) return;
-    size_t sm = vacc32_smem(L.G, L.P);
-    const float2* sp = static_cast<const float2*>(spec);
-    float2* dn = static_cast<float2*>(dnchk);
-    const float2* tw = reinterpret_cast<const float2*>(L.twb);
-    switch (L.G) {
-        case 8: vlist_accum32_kernel<8><<<ntrg, 256, sm, s>>>(L, trg, vptr, vsrc, voff, sp, dn, tw); break;
-        case 12: vlist_accum32_kernel<12><<<ntrg, 256, sm, s>>>(L, trg, vptr, vsrc, voff, sp, dn, tw); break;
-        case 16: vlist_accum32_kernel<16><<<ntrg, 256, sm, s>>>(L, trg, vptr, vsrc, voff, sp, dn, tw); break;
+    const size_t sm = vacc32_smem(G, G / 2);
+    const float2* so = static_cast<const float2*>(spec_override);
+    switch (G) {
+        case 8: vlist_accum32_kernel<8><<<ntrg, 256, sm, s>>>(subs, prefix, nsub, active, so); break;
+        case 12: vlist_accum32_kernel<12><<<ntrg, 256, sm, s>>>(subs, prefix, nsub, active, so); break;
+        case 16: vlist_accum32_kernel<16><<<ntrg, 256, sm, s>>>(subs, prefix, nsub, active, so); break;
         default: break;
     }
+}
+
+// Batch I/O: complex64 densities in point-id order into leaf order (gather),
+// leaf-order values back to point-id order (scatter); one thread per point.
+__global__ void move32_kernel(const MoveSub* __restrict__ subs, const int* __restrict__ prefix, int nsub, int n,
+                              const int* __restrict__ active, int scatter) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int j = find_sub(prefix, nsub, i);
+    const MoveSub S = subs[j];
+    if (active && !active[S.inst]) return;
+    const int l = i - prefix[j];
+    const float2* in = static_cast<const float2*>(S.in);
+    float2* out = static_cast<float2*>(S.out);
+    if (scatter)
+        out[S.perm[l]] = in[l];
+    else
+        out[l] = in[S.perm[l]];
+}
+void launch_move32(const MoveSub* subs, const int* prefix, int nsub, int n, const int* active, int scatter,
+                   cudaStream_t s) {
+    if (n > 0) move32_kernel<<<(n + 255) / 256, 256, 0, s>>>(subs, prefix, nsub, n, active, scatter);
+}
+
+// Zeroing of several instances' arrays, 8-byte words.
+__global__ void zero_kernel(const ZeroSub* __restrict__ subs, const long long* __restrict__ prefix, int nsub,
+                            long long n, const int* __restrict__ active) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int j = find_sub(prefix, nsub, i);
+        const ZeroSub S = subs[j];
+        if (active && !active[S.inst]) continue;
+        static_cast<unsigned long long*>(S.p)[i - prefix[j]] = 0ull;
+    }
+}
+void launch_zero(const ZeroSub* subs, const long long* prefix, int nsub, long long n8, const int* active,
+                 cudaStream_t s) {
+    if (n8 <= 0) return;
+    long long blocks = (n8 + 255) / 256;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    zero_kernel<<<(unsigned)blocks, 256, 0, s>>>(subs, prefix, nsub, n8, active);
 }
 
 // ---------------------------------------------------------------- conversions

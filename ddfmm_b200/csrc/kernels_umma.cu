@@ -257,23 +257,45 @@ size_t umma_packed_floats(int m, int k) {
 }
 
 // ---------------------------------------------------------------- GEMM
+// Tile ti of a launch: its sub-launch (prefix[j] <= ti < prefix[j+1]), tile and
+// problem; `on` is false when the sub-launch's instance is inactive.
 struct TileInfo {
     UmmaTile t;
     UmmaProblem p;
+    const float2* X;
+    float2* Y;
+    const long long* xoff;
+    const long long* yoff;
+    int mode;
+    bool on;
 };
-__device__ __forceinline__ TileInfo tile_info(const UmmaProblem* probs, const UmmaTile* tiles, int ti) {
+__device__ __forceinline__ TileInfo tile_info(const UmmaSub* __restrict__ subs, const int* __restrict__ prefix,
+                                              int nsub, const int* __restrict__ active, int ti) {
+    int lo = 0, hi = nsub - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= ti)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const UmmaSub& S = subs[lo];
     TileInfo r;
-    r.t = tiles[ti];
-    r.p = probs[r.t.prob];
+    r.on = !active || active[S.inst];
+    r.t = S.tiles[ti - __ldg(prefix + lo)];
+    r.p = S.probs[r.t.prob];
+    r.X = S.X;
+    r.Y = S.Y;
+    r.xoff = S.xoff;
+    r.yoff = S.yoff;
+    r.mode = S.mode;
     return r;
 }
 __device__ __forceinline__ int tile_n(int rows) { return ((2 * rows + 15) / 16) * 16; }
 
-__global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaProblem* __restrict__ probs,
-                                                                 const UmmaTile* __restrict__ tiles, int ntiles,
-                                                                 const long long* __restrict__ xoff,
-                                                                 const long long* __restrict__ yoff,
-                                                                 const float2* __restrict__ X, float2* Y, int mode,
+__global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub* __restrict__ subs,
+                                                                 const int* __restrict__ prefix, int nsub,
+                                                                 int ntiles, const int* __restrict__ active,
                                                                  int* err) {
     extern __shared__ __align__(1024) unsigned char usm_raw[];
     __shared__ __align__(8) uint64_t full[USTAGES], empty[USTAGES], tmem_full[2], tmem_empty[2];
@@ -323,16 +345,21 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaProbl
         // load cursor: tile ti_i, block kb_i of nkb_i, its columns' offsets xr[]
         int ti_i = blockIdx.x, kb_i = 0, nkb_i = 0, k_i = 0;
         long long xr[CPB];
-        auto load_tile = [&]() {
-            if (ti_i >= ntiles) return;
-            const TileInfo T = tile_info(probs, tiles, ti_i);
-            nkb_i = T.p.nkb;
-            k_i = T.p.k;
-            const int ncol = min(UM, T.p.ncol - T.t.col0);
+        const float2* X = nullptr;
+        auto load_tile = [&]() {  // the first active tile from ti_i on
+            for (; ti_i < ntiles; ti_i += gridDim.x) {
+                const TileInfo T = tile_info(subs, prefix, nsub, active, ti_i);
+                if (!T.on) continue;
+                nkb_i = T.p.nkb;
+                k_i = T.p.k;
+                X = T.X;
+                const int ncol = min(UM, T.p.ncol - T.t.col0);
 #pragma unroll
-            for (int i = 0; i < CPB; ++i) {
-                const int c = cw * 32 + i * (32 / CPB) + lane / CPB;
-                xr[i] = c < ncol ? xoff[T.p.col0 + T.t.col0 + c] : -1;
+                for (int i = 0; i < CPB; ++i) {
+                    const int c = cw * 32 + i * (32 / CPB) + lane / CPB;
+                    xr[i] = c < ncol ? T.xoff[T.p.col0 + T.t.col0 + c] : -1;
+                }
+                return;
             }
         };
         auto advance = [&]() {
@@ -400,7 +427,8 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaProbl
         if (lane == 0) {
             int g = 0;
             for (int ti = blockIdx.x; ti < ntiles && !*failed; ti += gridDim.x) {
-                const TileInfo T = tile_info(probs, tiles, ti);
+                const TileInfo T = tile_info(subs, prefix, nsub, active, ti);
+                if (!T.on) continue;
                 const char* Bt = reinterpret_cast<const char*>(T.p.B + (size_t)T.t.rtile * T.p.tile_stride);
                 const uint32_t blk = (uint32_t)tile_n(T.t.rows) * UBK * 4;
                 for (int kb = 0; kb < T.p.nkb; ++kb, ++g) {
@@ -421,8 +449,9 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaProbl
         // ------------------------------------------------ MMA issue
         if (lane == 0) {
             int g = 0, it = 0, last = -1;
-            for (int ti = blockIdx.x; ti < ntiles && !*failed; ti += gridDim.x, ++it) {
-                const TileInfo T = tile_info(probs, tiles, ti);
+            for (int ti = blockIdx.x; ti < ntiles && !*failed; ti += gridDim.x) {
+                const TileInfo T = tile_info(subs, prefix, nsub, active, ti);
+                if (!T.on) continue;
                 const uint32_t idesc = idesc_tf32(tile_n(T.t.rows));
                 const int acc = it & 1;
                 if (it >= 2 && !mbar_wait(&tmem_empty[acc], ((it >> 1) - 1) & 1, failed)) {
@@ -452,6 +481,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaProbl
                 }
                 if (*failed) break;
                 umma_commit(&tmem_full[acc]);
+                ++it;
             }
             if (*failed && last >= 0)  // let the MMAs already issued finish before TMEM is freed
                 mbar_wait(&empty[last % USTAGES], (last / USTAGES) & 1, nullptr);
@@ -461,13 +491,16 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaProbl
         const int qw = warp & 3;  // TMEM lanes 32 qw .. 32 qw + 31 = tile columns
         float2* park = park_all + qw * (32 * (PCH + 1));
         int it = 0;
-        for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x, ++it) {
-            const TileInfo T = tile_info(probs, tiles, ti);
+        for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+            const TileInfo T = tile_info(subs, prefix, nsub, active, ti);
+            if (!T.on) continue;
             const int ncol = min(UM, T.p.ncol - T.t.col0);
             const int rows = T.t.rows, N = tile_n(rows);
             const int acc = it & 1;
             const int mycol = qw * 32 + lane;
-            const long long my_yo = mycol < ncol ? yoff[T.p.col0 + T.t.col0 + mycol] + T.t.row0 : 0;
+            const long long my_yo = mycol < ncol ? T.yoff[T.p.col0 + T.t.col0 + mycol] + T.t.row0 : 0;
+            float2* const Y = T.Y;
+            const int mode = T.mode;
             bool ok = !*failed && mbar_wait(&tmem_full[acc], (it >> 1) & 1, failed);
             ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld is warp-collective
             if (!ok) {
@@ -527,6 +560,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaProbl
                 }
                 __syncwarp();
             }
+            ++it;
         }
     }
     __syncthreads();
@@ -551,14 +585,12 @@ void umma_init() {
     cudaDeviceGetAttribute(&g_umma_sms, cudaDevAttrMultiProcessorCount, dev);
 }
 
-void launch_umma_cgemm(const UmmaProblem* probs, const UmmaTile* tiles, int ntiles, const long long* xoff,
-                       const long long* yoff, const void* X, void* Y, int mode, int* err, cudaStream_t s) {
+void launch_umma_cgemm(const UmmaSub* subs, const int* prefix, int nsub, int ntiles, const int* active, int* err,
+                       cudaStream_t s) {
     if (ntiles == 0) return;
     const int sms = g_umma_sms > 0 ? g_umma_sms : 148;
     const int grid = ntiles < sms ? ntiles : sms;
-    umma_cgemm_kernel<<<grid, UTHREADS, UGEMM_SMEM, s>>>(probs, tiles, ntiles, xoff, yoff,
-                                                        static_cast<const float2*>(X), static_cast<float2*>(Y), mode,
-                                                        err);
+    umma_cgemm_kernel<<<grid, UTHREADS, UGEMM_SMEM, s>>>(subs, prefix, nsub, ntiles, active, err);
 }
 
 }  // namespace ddfmm

@@ -14,6 +14,7 @@
 #include "session.hpp"
 
 #include <algorithm>
+#include <cctype>
 #include <cstdio>
 #include <chrono>
 #include <cmath>
@@ -108,7 +109,7 @@ void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<
     st.bytes = bytes;
     if (umma()) {
         add_umma(P, xs, ys, X, Y, mode, st);
-        steps_.push_back(st);
+        push_step(st);
         stats_.gemm_launches++;
         return;
     }
@@ -120,7 +121,7 @@ void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<
     st.g.X = X;
     st.g.Y = Y;
     st.g.mode = mode;
-    steps_.push_back(st);
+    push_step(st);
     stats_.gemm_launches++;
 }
 
@@ -158,14 +159,44 @@ void Session::add_umma(const std::vector<GemmProblem>& P, const std::vector<long
                 tiles.push_back(UmmaTile{(int)i, rt, rt * 128, std::min(128, q.m - rt * 128), c0, 0});
     }
     st.kind = 5;
-    st.u.probs = upload(U);
-    st.u.tiles = upload(tiles);
-    st.u.xoff = upload(xs);
-    st.u.yoff = upload(ys);
-    st.u.ntiles = (int)tiles.size();
-    st.u.X = X;
-    st.u.Y = Y;
-    st.u.mode = mode;
+    st.hu = UmmaSub{upload(U), upload(tiles), upload(xs), upload(ys), reinterpret_cast<const float2*>(X),
+                    reinterpret_cast<float2*>(Y), (int)tiles.size(), mode, 0, 0};
+    set_multi(st, st.hu, (int)tiles.size());
+}
+
+template <class Sub>
+void Session::set_multi(Step& st, const Sub& sub, int total) {
+    st.msubs = upload(std::vector<Sub>(1, sub));
+    st.mpre = upload(std::vector<int>{0, total});
+    st.mtotal = total;
+}
+
+// Steps are emitted in blocks (phase, width): LF upward and HF upward by
+// ascending width, HF downward and LF downward by descending width.
+void Session::begin_block(int phase, double W) {
+    cur_phase_ = phase;
+    const long long w = std::lround(std::log2(W));
+    cur_wkey_ = phase < 2 ? 1000 + w : 1000 - w;
+    block_counts_.clear();
+}
+
+void Session::push_step(Step st) {
+    // step types in the order the blocks emit them
+    static const char* const order[] = {"lf_s2m",   "lf_m2m",       "lf_uc2ue",     "memset",   "hf_m2m",
+                                        "hf_uc2ue", "hf_m2l",       "hf_dc2de",     "hf_l2l",   "lf_vlist_fft",
+                                        "lf_vlist_m2l", "lf_xlist", "lf_ulist",     "lf_wlist", "lf_dc2de",
+                                        "lf_l2t",   "lf_l2l"};
+    std::string base(st.label);
+    const size_t u = base.rfind("_w");
+    if (u != std::string::npos && u + 2 < base.size() && std::isdigit((unsigned char)base[u + 2]))
+        base = base.substr(0, u);  // per-width label "pass_w<W>"
+
+    long long rank = 63;
+    for (size_t i = 0; i < sizeof(order) / sizeof(order[0]); ++i)
+        if (base == order[i]) rank = (long long)i;
+    const long long occ = block_counts_[base]++;
+    st.key = ((long long)cur_phase_ << 48) | (cur_wkey_ << 32) | (rank << 16) | occ;
+    steps_.push_back(st);
 }
 
 void Session::flush_packs() {
@@ -219,7 +250,11 @@ void Session::add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>&
     st.pt.items = upload(items);
     st.pt.srcs = upload(srcs);
     st.pt.nitems = (int)items.size();
-    steps_.push_back(st);
+    if (mixed()) {
+        st.hp = PtSub{st.pt.items, st.pt.srcs, st.pt.nitems, prm_.kernel, 0, 0};
+        set_multi(st, st.hp, st.pt.nitems);
+    }
+    push_step(st);
 }
 
 namespace {
@@ -841,6 +876,7 @@ void Session::build() {
     for (auto it = lflevels.rbegin(); it != lflevels.rend(); ++it) {
         const LfLevelOps& L = lfops[it->first];
         const auto& ids = it->second;
+        begin_block(0, L.W);
         // S2M at leaves (src/wave3d_eval.cpp:441-451)
         std::vector<PtItem> items;
         std::vector<PtSrc> srcs;
@@ -890,11 +926,12 @@ void Session::build() {
         double W = T.width(level);
         auto ur = uprange[level];
         if (ur.first == ur.second) continue;
+        begin_block(1, W);
         Step ms{};
         ms.kind = 4;
         ms.label = "memset";
         ms.ms = Memset{T0, es * (size_t)tmp_max};
-        steps_.push_back(ms);
+        push_step(ms);
         // M2M: E3 upchkval = sum_children [E3 ue2uc E1(child)] w_child (src/wave3d_eval.cpp:796-834)
         for (int ind = 0; ind < 8; ++ind) {
             std::map<Idx3, int> pid;
@@ -960,6 +997,7 @@ void Session::build() {
         double W = T.width(level);
         auto dr = dnrange[level];
         if (dr.first == dr.second) continue;
+        begin_block(2, W);
         // M2L (src/wave3d_eval.cpp:876-928)
         {
             std::vector<GemmProblem> probs;
@@ -1033,6 +1071,7 @@ void Session::build() {
         const LfLevelOps& L = lfops[level];
         const auto& ids = kv.second;
         double W = L.W;
+        begin_block(3, W);
         // V list: FFT M2L (src/wave3d_eval.cpp:602-661)
         {
             std::vector<int> trg, vptr(1, 0), vsrc, voff;
@@ -1078,7 +1117,12 @@ void Session::build() {
                 f.v.nsrc = (int)srcb.size();
                 f.v.upeq = lf_upeq;
                 f.v.spec = lf_spec;
-                steps_.push_back(f);
+                if (mixed) {
+                    f.hvf = VfSub{VL, f.v.src_boxes, reinterpret_cast<const float2*>(lf_upeq),
+                                  reinterpret_cast<float2*>(lf_spec), f.v.nsrc, 0};
+                    set_multi(f, f.hvf, f.v.nsrc);
+                }
+                push_step(f);
                 Step a{};
                 a.kind = 3;
                 a.label = "lf_vlist_m2l";
@@ -1093,7 +1137,12 @@ void Session::build() {
                 a.v.ntrg = (int)trg.size();
                 a.v.spec = lf_spec;
                 a.v.dnchk = lf_dnchk;
-                steps_.push_back(a);
+                if (mixed) {
+                    a.hva = VaSub{VL, a.v.trg, a.v.vptr, a.v.vsrc, a.v.voff, reinterpret_cast<const float2*>(lf_spec),
+                                  reinterpret_cast<float2*>(lf_dnchk), a.v.ntrg, 0};
+                    set_multi(a, a.hva, a.v.ntrg);
+                }
+                push_step(a);
             }
         }
         // X list (src/wave3d_eval.cpp:663-686), into dnchk or, for small leaves, into extval
@@ -1229,19 +1278,21 @@ void Session::launch_step(const Step& st, cudaStream_t s, double2* spec) {
             break;
         case 1:
             if (m)
-                launch_pt32(st.pt.items, st.pt.nitems, st.pt.srcs, prm_.kernel, s);
+                launch_pt32(static_cast<const PtSub*>(st.msubs), st.mpre, 1, st.mtotal, nullptr, s);
             else
                 launch_pt(st.pt.items, st.pt.nitems, st.pt.srcs, prm_.kernel, s);
             break;
         case 2:
             if (m)
-                launch_vlist_forward32(st.v.L, st.v.src_boxes, st.v.nsrc, st.v.upeq, spec, s);
+                launch_vlist_forward32(static_cast<const VfSub*>(st.msubs), st.mpre, 1, st.mtotal, st.v.L.G, nullptr,
+                                       spec != st.v.spec ? spec : nullptr, s);
             else
                 launch_vlist_forward(st.v.L, st.v.src_boxes, st.v.nsrc, st.v.upeq, spec, s);
             break;
         case 3:
             if (m)
-                launch_vlist_accum32(st.v.L, st.v.trg, st.v.ntrg, st.v.vptr, st.v.vsrc, st.v.voff, spec, st.v.dnchk, s);
+                launch_vlist_accum32(static_cast<const VaSub*>(st.msubs), st.mpre, 1, st.mtotal, st.v.L.G, nullptr,
+                                     spec != st.v.spec ? spec : nullptr, s);
             else
                 launch_vlist_accum(st.v.L, st.v.trg, st.v.ntrg, st.v.vptr, st.v.vsrc, st.v.voff, spec, st.v.dnchk, s);
             break;
@@ -1249,8 +1300,7 @@ void Session::launch_step(const Step& st, cudaStream_t s, double2* spec) {
             CK(cudaMemsetAsync(st.ms.p, 0, st.ms.bytes, s));
             break;
         case 5:
-            launch_umma_cgemm(st.u.probs, st.u.tiles, st.u.ntiles, st.u.xoff, st.u.yoff, st.u.X, st.u.Y, st.u.mode,
-                              d_err_, s);
+            launch_umma_cgemm(static_cast<const UmmaSub*>(st.msubs), st.mpre, 1, st.mtotal, nullptr, d_err_, s);
             break;
     }
 }

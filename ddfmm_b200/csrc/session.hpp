@@ -88,16 +88,6 @@ private:
         double2* Y = nullptr;
         int mode = 0;
     };
-    struct UmmaLaunch {
-        UmmaProblem* probs = nullptr;
-        UmmaTile* tiles = nullptr;
-        long long* xoff = nullptr;
-        long long* yoff = nullptr;
-        int ntiles = 0;
-        const double2* X = nullptr;
-        double2* Y = nullptr;
-        int mode = 0;
-    };
     struct PtLaunch {
         PtItem* items = nullptr;
         PtSrc* srcs = nullptr;
@@ -127,11 +117,24 @@ private:
         double flops;       // algorithmic flops of the launch
         double bytes;       // algorithmic DRAM bytes of the launch
         GemmLaunch g;
-        UmmaLaunch u;
         PtLaunch pt;
         VLaunch v;
         Memset ms;
+        // Position of the step in the pass structure, equal across sessions for steps
+        // that play the same part (phase, width, step type, occurrence): a Batch
+        // merges the steps of its sessions that share a key into one launch.
+        long long key;
+        // mixed form: the step as a one-instance launch (device sub-launch array and
+        // prefix sums) and the host copy of its sub-launch
+        void* msubs;
+        int* mpre;
+        int mtotal;
+        UmmaSub hu;
+        PtSub hp;
+        VfSub hvf;
+        VaSub hva;
     };
+    friend class Batch;
 
     template <class T>
     T* dalloc(size_t count);
@@ -145,6 +148,10 @@ private:
                   const std::vector<long long>& ys, const double2* X, double2* Y, int mode, Step& st);
     void flush_packs();
     void add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>& srcs, const char* label);
+    template <class Sub>
+    void set_multi(Step& st, const Sub& sub, int total);
+    void begin_block(int phase, double W);
+    void push_step(Step st);
     void build();
     void run_steps(cudaStream_t s);
     void run_steps_spec(cudaStream_t s, double2* spec);
@@ -180,6 +187,9 @@ private:
     std::vector<std::pair<int, int> > ev_pending_;  // (step, event index) recorded, not yet read
     std::map<std::string, ProfileEntry> prof_;
     std::vector<std::string> label_store_;  // per-width pass labels (Step::label points here)
+    int cur_phase_ = 0;
+    long long cur_wkey_ = 0;
+    std::map<std::string, int> block_counts_;  // occurrences of each step type in the current block
     const char* width_label(const char* pass, double W);
 };
 

@@ -188,6 +188,64 @@ class Wave3d:
             pass
 
 
+class Batch:
+    """Several mixed-form Wave3d instances evaluated together (merged
+    multi-instance launches replayed as one CUDA graph).  The instances must
+    stay open while the batch is used."""
+
+    def __init__(self, waves):
+        self.waves = list(waves)
+        for w in self.waves:
+            w._need()
+        arr = (C.c_void_p * len(self.waves))(*[w._s for w in self.waves])
+        out = C.c_void_p()
+        _lib.check(_lib.load().ddfmm_batch_create(arr, len(self.waves), C.byref(out)))
+        self._b = out
+
+    def launches(self):
+        n = C.c_int()
+        _lib.check(_lib.load().ddfmm_batch_launches(self._b, C.byref(n)))
+        return n.value
+
+    def eval(self, dens, vals):
+        """vals[i][:] = matvec_i(dens[i]) for every i with dens[i] is not None
+        (complex64 arrays); the others are not computed."""
+        n = len(self.waves)
+        keep = []
+        dp = (C.c_void_p * n)()
+        vp = (C.c_void_p * n)()
+        for i, (d, v) in enumerate(zip(dens, vals)):
+            if d is None:
+                continue
+            d = np.ascontiguousarray(d, dtype=np.complex64)
+            if d.shape != (self.waves[i]._n,) or v.dtype != np.complex64 or v.shape != d.shape:
+                raise _lib.DDFMMError(1, "instance %d needs complex64 arrays of %d entries" % (i, self.waves[i]._n))
+            if not v.flags.c_contiguous:
+                raise _lib.DDFMMError(1, "val arrays must be contiguous")
+            keep.append(d)
+            dp[i] = d.ctypes.data
+            vp[i] = v.ctypes.data
+        _lib.check(_lib.load().ddfmm_batch_eval_c64(self._b, dp, vp))
+
+    def eval_device(self, den_ptrs, val_ptrs, stream=None):
+        """Device complex64 arrays (integer pointers, None = not computed)."""
+        n = len(self.waves)
+        dp = (C.c_void_p * n)(*[p if p else None for p in den_ptrs])
+        vp = (C.c_void_p * n)(*[p if p else None for p in val_ptrs])
+        _lib.check(_lib.load().ddfmm_batch_eval_device_c64(self._b, dp, vp, C.c_void_p(stream) if stream else None))
+
+    def close(self):
+        if getattr(self, "_b", None) is not None:
+            _lib.load().ddfmm_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def from_workload(w, device=0, precision=0):
     """Set up a Wave3d for a workloads.Workload (operators created on demand)."""
     ld, hd = w.operators()

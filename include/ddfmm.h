@@ -159,6 +159,29 @@ int ddfmm_profile_read(ddfmm_session* s, ddfmm_profile_entry* out, int max_entri
 int ddfmm_session_destroy(ddfmm_session* s);
 const char* ddfmm_last_error(void);
 
+/* ---------------------------------------------------------------- batches
+ * No counterpart in the reference (one Wave3d per process there).  A batch
+ * evaluates many independent sessions together: their launch sequences are
+ * merged pass by pass (same pass, width and step type) into multi-instance
+ * launches and replayed as one CUDA graph, so one matvec of every session
+ * costs as many launches as the deepest single session.  Sessions must be
+ * DDFMM_MIXED sessions of one device and one ACCU, must outlive the batch,
+ * and must not be evaluated on their own while a batch call on them is in
+ * flight (the batch uses their device buffers). */
+typedef struct ddfmm_batch ddfmm_batch;
+int ddfmm_batch_create(ddfmm_session* const* sessions, int n, ddfmm_batch** out);
+/* One matvec of every session i with den[i] != NULL (complex64 host arrays of
+ * that session's n points, interleaved floats); val[i] receives it.  Entries
+ * with den[i] == NULL are not computed and val[i] is not touched.  Returns
+ * when every val[i] is filled. */
+int ddfmm_batch_eval_c64(ddfmm_batch* b, const float* const* den, float* const* val);
+/* The same with device arrays, enqueued on `stream` (a cudaStream_t, or NULL
+ * for the batch's own stream); returns after enqueueing. */
+int ddfmm_batch_eval_device_c64(ddfmm_batch* b, const void* const* den_dev, void* const* val_dev, void* stream);
+/* Launches per batch matvec (the merged sequence). */
+int ddfmm_batch_launches(ddfmm_batch* b, int* launches);
+int ddfmm_batch_destroy(ddfmm_batch* b);
+
 #ifdef __cplusplus
 }
 #endif
