@@ -17,9 +17,20 @@ EXPORTS = (
     "ddfmm_profile_enable", "ddfmm_profile_read", "ddfmm_eval_device_noalloc",
     "ddfmm_session_create_ex", "ddfmm_eval_c64", "ddfmm_eval_device_c64",
     "ddfmm_batch_create", "ddfmm_batch_eval_c64", "ddfmm_batch_eval_device_c64", "ddfmm_batch_launches",
-    "ddfmm_batch_destroy",
+    "ddfmm_batch_destroy", "ddfmm_server_create", "ddfmm_server_add_session", "ddfmm_server_session_state",
+    "ddfmm_server_remove_session", "ddfmm_server_submit", "ddfmm_server_wait", "ddfmm_server_poll",
+    "ddfmm_server_get_stats", "ddfmm_server_destroy",
 )
 PLAIN_FP64, MIXED, MIXED_MMA_SYNC = 0, 1, 2
+
+
+class ddfmm_server_stats(C.Structure):
+    _fields_ = [("requests", C.c_longlong), ("ticks", C.c_longlong), ("mean_batch", C.c_double),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double), ("busy_s", C.c_double),
+                ("used_bytes", C.c_longlong), ("admitted", C.c_int), ("waiting", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class ddfmm_stats(C.Structure):
@@ -108,6 +119,21 @@ def load():
     lib.ddfmm_batch_launches.restype = C.c_int
     lib.ddfmm_batch_destroy.argtypes = [C.c_void_p]
     lib.ddfmm_batch_destroy.restype = C.c_int
+    lib.ddfmm_server_create.argtypes = [C.c_int, C.c_double, vpp]
+    lib.ddfmm_server_add_session.argtypes = [C.c_void_p, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, dp,
+                                             C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p,
+                                             C.POINTER(C.c_int)]
+    lib.ddfmm_server_session_state.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    lib.ddfmm_server_remove_session.argtypes = [C.c_void_p, C.c_int]
+    lib.ddfmm_server_submit.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong)]
+    lib.ddfmm_server_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_double, C.POINTER(C.c_int)]
+    lib.ddfmm_server_poll.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(C.c_int)]
+    lib.ddfmm_server_get_stats.argtypes = [C.c_void_p, C.POINTER(ddfmm_server_stats), C.c_int]
+    lib.ddfmm_server_destroy.argtypes = [C.c_void_p]
+    for f in ("ddfmm_server_create", "ddfmm_server_add_session", "ddfmm_server_session_state",
+              "ddfmm_server_remove_session", "ddfmm_server_submit", "ddfmm_server_wait", "ddfmm_server_poll",
+              "ddfmm_server_get_stats", "ddfmm_server_destroy"):
+        getattr(lib, f).restype = C.c_int
     _lib = lib
     return lib
 

@@ -10,10 +10,15 @@
 
 #include "../../include/ddfmm.h"
 #include "batch.hpp"
+#include "server.hpp"
 #include "session.hpp"
 
 struct ddfmm_session {
     ddfmm::Session* impl;
+};
+
+struct ddfmm_server {
+    ddfmm::Server* impl;
 };
 
 struct ddfmm_batch {
@@ -90,11 +95,13 @@ int ddfmm_session_create(const double* pos3n, int n, int kernel, int accu, int n
                                    device, DDFMM_PLAIN_FP64, out);
 }
 
-int ddfmm_session_create_ex(const double* pos3n, int n, int kernel, int accu, int npq, double K, const double* ctr3,
-                            int ptsmax, int maxlevel, int ncell, const char* ld_path, const char* hd_path, int device,
-                            int precision, ddfmm_session** out) {
-    if (!out) return fail(DDFMM_EINVAL, "out is NULL");
-    *out = nullptr;
+}  // extern "C"
+
+// Validation shared by session creation and server admission (the reference's
+// option checks, src/wave3d.cpp:145-158 and src/wave3d_setup.cpp:21-97).
+static int make_params(const double* pos3n, int n, int kernel, int accu, int npq, double K, const double* ctr3,
+                       int ptsmax, int maxlevel, int ncell, const char* ld_path, const char* hd_path, int device,
+                       int precision, ddfmm::SessionParams* out) {
     if (!pos3n || n <= 0) return fail(DDFMM_EINVAL, "need n > 0 points");
     if (kernel != DDFMM_KERNEL_HELM && kernel != DDFMM_KERNEL_EXPR) return fail(DDFMM_EINVAL, "unknown kernel type");
     if (accu < 1 || accu > 3) return fail(DDFMM_EINVAL, "ACCU must be 1, 2 or 3");
@@ -114,7 +121,7 @@ int ddfmm_session_create_ex(const double* pos3n, int n, int kernel, int accu, in
         return fail(DDFMM_ECUDA, "no CUDA device available");
     }
     if (device < 0 || device >= ndev) return fail(DDFMM_EINVAL, "device ordinal out of range");
-    ddfmm::SessionParams p;
+    ddfmm::SessionParams& p = *out;
     p.tree.K = K;
     p.tree.ctr = {{ctr3 ? ctr3[0] : 0.0, ctr3 ? ctr3[1] : 0.0, ctr3 ? ctr3[2] : 0.0}};
     p.tree.ptsmax = ptsmax;
@@ -125,8 +132,22 @@ int ddfmm_session_create_ex(const double* pos3n, int n, int kernel, int accu, in
     p.kernel = kernel;
     p.device = device;
     p.precision = precision;
+    return DDFMM_OK;
+}
+
+extern "C" {
+
+int ddfmm_session_create_ex(const double* pos3n, int n, int kernel, int accu, int npq, double K, const double* ctr3,
+                            int ptsmax, int maxlevel, int ncell, const char* ld_path, const char* hd_path, int device,
+                            int precision, ddfmm_session** out) {
+    if (!out) return fail(DDFMM_EINVAL, "out is NULL");
+    *out = nullptr;
+    ddfmm::SessionParams p;
+    int rc = make_params(pos3n, n, kernel, accu, npq, K, ctr3, ptsmax, maxlevel, ncell, ld_path, hd_path, device,
+                         precision, &p);
+    if (rc != DDFMM_OK) return rc;
     ddfmm::Session* impl = nullptr;
-    int rc = guarded([&] { impl = new ddfmm::Session(pos3n, n, p, ld_path, hd_path); });
+    rc = guarded([&] { impl = new ddfmm::Session(pos3n, n, p, ld_path, hd_path); });
     if (rc != DDFMM_OK) return rc;
     *out = new ddfmm_session{impl};
     return DDFMM_OK;
@@ -397,6 +418,107 @@ int ddfmm_batch_launches(ddfmm_batch* b, int* launches) {
 int ddfmm_batch_destroy(ddfmm_batch* b) {
     if (!b) return DDFMM_OK;
     return guarded([&] { batch_free(b); });
+}
+
+int ddfmm_server_create(int device, double budget_bytes, ddfmm_server** out) {
+    if (!out) return fail(DDFMM_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!(budget_bytes > 0)) return fail(DDFMM_EINVAL, "the device-memory budget must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(DDFMM_ECUDA, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return fail(DDFMM_EINVAL, "device ordinal out of range");
+    ddfmm::Server* impl = nullptr;
+    int rc = guarded([&] {
+        DeviceGuard dg(device);
+        impl = new ddfmm::Server(device, (size_t)budget_bytes);
+    });
+    if (rc != DDFMM_OK) return rc;
+    *out = new ddfmm_server{impl};
+    return DDFMM_OK;
+}
+
+int ddfmm_server_add_session(ddfmm_server* sv, const double* pos3n, int n, int kernel, int accu, int npq, double K,
+                             const double* ctr3, int ptsmax, int maxlevel, int ncell, const char* ld_path,
+                             const char* hd_path, int* sid) {
+    if (!sv || !sid) return fail(DDFMM_EINVAL, "NULL argument");
+    ddfmm::SessionParams p;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int rc = make_params(pos3n, n, kernel, accu, npq, K, ctr3, ptsmax, maxlevel, ncell, ld_path, hd_path, dev,
+                         DDFMM_MIXED, &p);
+    if (rc != DDFMM_OK) return rc;
+    return guarded([&] {
+        ddfmm::SessionSpec spec;
+        spec.pos.assign(pos3n, pos3n + 3 * (size_t)n);
+        spec.n = n;
+        spec.params = p;
+        spec.ld = ld_path;
+        spec.hd = hd_path;
+        *sid = sv->impl->add_session(std::move(spec));
+    });
+}
+
+int ddfmm_server_session_state(ddfmm_server* sv, int sid, int* state) {
+    if (!sv || !state) return fail(DDFMM_EINVAL, "NULL argument");
+    std::string why;
+    const int st = sv->impl->state(sid, &why);
+    if (st < 0) return fail(DDFMM_EINVAL, "unknown session");
+    *state = st;
+    if (!why.empty()) g_err = why;
+    return DDFMM_OK;
+}
+
+int ddfmm_server_remove_session(ddfmm_server* sv, int sid) {
+    if (!sv) return fail(DDFMM_EINVAL, "NULL server");
+    return guarded([&] { sv->impl->remove_session(sid); });
+}
+
+int ddfmm_server_submit(ddfmm_server* sv, int sid, const float* den, float* val, long long* ticket) {
+    if (!sv || !den || !val || !ticket) return fail(DDFMM_EINVAL, "NULL argument");
+    return guarded([&] {
+        *ticket = sv->impl->submit(sid, reinterpret_cast<const std::complex<float>*>(den),
+                                   reinterpret_cast<std::complex<float>*>(val));
+    });
+}
+
+int ddfmm_server_wait(ddfmm_server* sv, long long ticket, double timeout_s, int* done) {
+    if (!sv || !done) return fail(DDFMM_EINVAL, "NULL argument");
+    return guarded([&] { *done = sv->impl->wait(ticket, timeout_s) == 0; });
+}
+
+int ddfmm_server_poll(ddfmm_server* sv, long long ticket, int* done) {
+    if (!sv || !done) return fail(DDFMM_EINVAL, "NULL argument");
+    const int r = sv->impl->poll(ticket);
+    if (r < 0) return fail(DDFMM_ECUDA, "request failed (ddfmm_server_wait gives the reason)");
+    *done = r == 0;
+    return DDFMM_OK;
+}
+
+int ddfmm_server_get_stats(ddfmm_server* sv, ddfmm_server_stats* out, int reset) {
+    if (!sv || !out) return fail(DDFMM_EINVAL, "NULL argument");
+    return guarded([&] {
+        const ddfmm::ServerStats s = sv->impl->stats(reset != 0);
+        out->requests = s.requests;
+        out->ticks = s.ticks;
+        out->mean_batch = s.mean_batch;
+        out->p50_ms = s.p50_ms;
+        out->p99_ms = s.p99_ms;
+        out->max_ms = s.max_ms;
+        out->busy_s = s.busy_s;
+        out->used_bytes = (long long)s.used_bytes;
+        out->admitted = s.admitted;
+        out->waiting = s.waiting;
+    });
+}
+
+int ddfmm_server_destroy(ddfmm_server* sv) {
+    if (!sv) return DDFMM_OK;
+    int rc = guarded([&] { delete sv->impl; });
+    delete sv;
+    return rc;
 }
 
 }  // extern "C"

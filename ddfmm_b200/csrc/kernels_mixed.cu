@@ -287,8 +287,14 @@ void launch_pt32(const PtSub* subs, const int* prefix, int nsub, int nitems, con
 __global__ void vlist_forward32_kernel(const VfSub* __restrict__ subs, const int* __restrict__ prefix, int nsub,
                                        const int* __restrict__ active, float2* spec_override) {
     extern __shared__ float2 sm32[];
-    const int j = find_sub(prefix, nsub, (int)blockIdx.x);
-    const VfSub S = subs[j];
+    __shared__ VfSub S;
+    __shared__ int local;
+    if (threadIdx.x == 0) {
+        const int j = find_sub(prefix, nsub, (int)blockIdx.x);
+        S = subs[j];
+        local = blockIdx.x - prefix[j];
+    }
+    __syncthreads();
     if (active && !active[S.inst]) return;
     const VlistLevel& L = S.L;
     const float2* twf = reinterpret_cast<const float2*>(L.twf);
@@ -298,7 +304,7 @@ __global__ void vlist_forward32_kernel(const VfSub* __restrict__ subs, const int
     float2* cube = sm32;
     float2* b1 = cube + PP * P;
     float2* b2 = b1 + G * PP;
-    const int b = S.boxes[blockIdx.x - prefix[j]];
+    const int b = S.boxes[local];
     for (int e = threadIdx.x; e < PP * P; e += blockDim.x) cube[e] = make_float2(0.f, 0.f);
     __syncthreads();
     for (int k = threadIdx.x; k < L.nE; k += blockDim.x) cube[L.cube_idx[k]] = upeq[(size_t)b * L.nE + k];
@@ -333,8 +339,14 @@ __global__ void __launch_bounds__(256) vlist_accum32_kernel(const VaSub* __restr
                                                             const float2* spec_override) {
     extern __shared__ float2 sm32[];
     constexpr int P = G / 2, PP = P * P, G3 = G * G * G, NE = (G3 + 255) / 256;
-    const int j = find_sub(prefix, nsub, (int)blockIdx.x);
-    const VaSub S = subs[j];
+    __shared__ VaSub S;
+    __shared__ int local;
+    if (threadIdx.x == 0) {
+        const int j = find_sub(prefix, nsub, (int)blockIdx.x);
+        S = subs[j];
+        local = blockIdx.x - prefix[j];
+    }
+    __syncthreads();
     if (active && !active[S.inst]) return;
     const VlistLevel& L = S.L;
     const float2* twb = reinterpret_cast<const float2*>(L.twb);
@@ -343,7 +355,7 @@ __global__ void __launch_bounds__(256) vlist_accum32_kernel(const VaSub* __restr
     float2* grid = sm32;
     float2* c1 = sm32 + G3;
     const float2* tns = reinterpret_cast<const float2*>(L.tns);
-    const int ti = blockIdx.x - prefix[j], t = S.trg[ti];
+    const int ti = local, t = S.trg[ti];
     float2 acc[NE];
 #pragma unroll
     for (int q = 0; q < NE; ++q) acc[q] = make_float2(0.f, 0.f);

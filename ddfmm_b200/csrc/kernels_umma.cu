@@ -269,12 +269,14 @@ struct TileInfo {
     int mode;
     bool on;
 };
-__device__ __forceinline__ TileInfo tile_info(const UmmaSub* __restrict__ subs, const int* __restrict__ prefix,
-                                              int nsub, const int* __restrict__ active, int ti) {
+// subs / prefix: the block's shared-memory copies (U_SUBS_SMEM entries at most)
+// or the global arrays
+__device__ __forceinline__ TileInfo tile_info(const UmmaSub* subs, const int* prefix, int nsub,
+                                              const int* __restrict__ active, int ti) {
     int lo = 0, hi = nsub - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(prefix + mid) <= ti)
+        if (prefix[mid] <= ti)
             lo = mid;
         else
             hi = mid - 1;
@@ -282,7 +284,7 @@ __device__ __forceinline__ TileInfo tile_info(const UmmaSub* __restrict__ subs, 
     const UmmaSub& S = subs[lo];
     TileInfo r;
     r.on = !active || active[S.inst];
-    r.t = S.tiles[ti - __ldg(prefix + lo)];
+    r.t = S.tiles[ti - prefix[lo]];
     r.p = S.probs[r.t.prob];
     r.X = S.X;
     r.Y = S.Y;
@@ -293,11 +295,22 @@ __device__ __forceinline__ TileInfo tile_info(const UmmaSub* __restrict__ subs, 
 }
 __device__ __forceinline__ int tile_n(int rows) { return ((2 * rows + 15) / 16) * 16; }
 
-__global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub* __restrict__ subs,
-                                                                 const int* __restrict__ prefix, int nsub,
+constexpr int U_SUBS_SMEM = 64;  // sub-launches cached in shared memory
+
+__global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub* __restrict__ gsubs,
+                                                                 const int* __restrict__ gprefix, int nsub,
                                                                  int ntiles, const int* __restrict__ active,
                                                                  int* err) {
     extern __shared__ __align__(1024) unsigned char usm_raw[];
+    __shared__ UmmaSub ssubs[U_SUBS_SMEM];
+    __shared__ int sprefix[U_SUBS_SMEM + 1];
+    const bool cached = nsub <= U_SUBS_SMEM;
+    if (cached) {
+        for (int i = threadIdx.x; i < nsub; i += blockDim.x) ssubs[i] = gsubs[i];
+        for (int i = threadIdx.x; i <= nsub; i += blockDim.x) sprefix[i] = gprefix[i];
+    }
+    const UmmaSub* subs = cached ? ssubs : gsubs;
+    const int* prefix = cached ? sprefix : gprefix;
     __shared__ __align__(8) uint64_t full[USTAGES], empty[USTAGES], tmem_full[2], tmem_empty[2];
     __shared__ uint32_t tmem_base;
     __shared__ int failed_s;

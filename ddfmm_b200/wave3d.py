@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import time
 
 import numpy as np
 
@@ -238,6 +239,99 @@ class Batch:
         if getattr(self, "_b", None) is not None:
             _lib.load().ddfmm_batch_destroy(self._b)
             self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Matvec server (ddfmm_server_*): mixed-form sessions admitted against a
+    device-memory budget, pending requests batched across sessions each tick."""
+    WAITING, ADMITTED, REJECTED, REMOVED, FAILED = range(5)
+
+    def __init__(self, budget_bytes, device=0):
+        out = C.c_void_p()
+        _lib.check(_lib.load().ddfmm_server_create(device, float(budget_bytes), C.byref(out)))
+        self._sv = out
+        self._n = {}
+        self._inflight = {}
+
+    def add_session(self, pos, kernel, ldname, hdname, opts, geomprtn, prefix="wave3d_"):
+        """Arguments as Wave3d/Mlib3d: points (n x 3), kernel type, operator files,
+        the -wave3d_* options and geomprtn (cells per edge)."""
+        p = "-" + prefix
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        ctr = _opt(opts, p + "ctr", (0.0, 0.0, 0.0), lambda s: tuple(float(x) for x in s.split()))
+        maxlevel = _opt(opts, p + "maxlevel", None, int)
+        if maxlevel is None:
+            raise _lib.DDFMMError(1, "-%smaxlevel is required" % prefix)
+        nc = geomprtn if isinstance(geomprtn, int) else int(np.asarray(geomprtn).shape[0])
+        c3 = (C.c_double * 3)(*ctr)
+        sid = C.c_int()
+        dp = C.POINTER(C.c_double)
+        _lib.check(_lib.load().ddfmm_server_add_session(
+            self._sv, pos.ctypes.data_as(dp), pos.shape[0], int(kernel), _opt(opts, p + "ACCU", 1, int),
+            _opt(opts, p + "NPQ", 4, int), _opt(opts, p + "K", 64.0, float), c3, _opt(opts, p + "ptsmax", 100, int),
+            maxlevel, nc, ldname.encode(), hdname.encode(), C.byref(sid)))
+        self._n[sid.value] = pos.shape[0]
+        return sid.value
+
+    def add_workload(self, w):
+        ld, hd = w.operators()
+        return self.add_session(w.points(), w.kernel, ld, hd, w.options(), w.nc)
+
+    def state(self, sid):
+        st = C.c_int()
+        _lib.check(_lib.load().ddfmm_server_session_state(self._sv, sid, C.byref(st)))
+        return st.value
+
+    def wait_admitted(self, sids, timeout=600.0):
+        """Block until none of sids is waiting; returns their states."""
+        t0 = time.time()
+        while True:
+            st = [self.state(s) for s in sids]
+            if all(x != self.WAITING for x in st) or time.time() - t0 > timeout:
+                return st
+            time.sleep(0.01)
+
+    def remove(self, sid):
+        _lib.check(_lib.load().ddfmm_server_remove_session(self._sv, sid))
+
+    def submit(self, sid, den, val):
+        """Queue val[:] = matvec_sid(den) (complex64 arrays); returns a ticket."""
+        d = np.ascontiguousarray(den, dtype=np.complex64)
+        if d.shape != (self._n[sid],) or val.dtype != np.complex64 or val.shape != d.shape or \
+                not val.flags.c_contiguous:
+            raise _lib.DDFMMError(1, "session %d needs complex64 arrays of %d entries" % (sid, self._n[sid]))
+        t = C.c_longlong()
+        _lib.check(_lib.load().ddfmm_server_submit(self._sv, sid, d.ctypes.data, val.ctypes.data, C.byref(t)))
+        self._inflight[t.value] = (d, val)  # keep the arrays alive until completion
+        return t.value
+
+    def wait(self, ticket, timeout=60.0):
+        done = C.c_int()
+        try:
+            _lib.check(_lib.load().ddfmm_server_wait(self._sv, ticket, float(timeout), C.byref(done)))
+        except _lib.DDFMMError:
+            self._inflight.pop(ticket, None)
+            raise
+        if done.value:
+            self._inflight.pop(ticket, None)
+        return bool(done.value)
+
+    def stats(self, reset=False):
+        st = _lib.ddfmm_server_stats()
+        _lib.check(_lib.load().ddfmm_server_get_stats(self._sv, C.byref(st), 1 if reset else 0))
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "_sv", None) is not None:
+            _lib.load().ddfmm_server_destroy(self._sv)
+            self._sv = None
+            self._inflight.clear()
 
     def __del__(self):
         try:

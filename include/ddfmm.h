@@ -182,6 +182,53 @@ int ddfmm_batch_eval_device_c64(ddfmm_batch* b, const void* const* den_dev, void
 int ddfmm_batch_launches(ddfmm_batch* b, int* launches);
 int ddfmm_batch_destroy(ddfmm_batch* b);
 
+/* ---------------------------------------------------------------- server
+ * No counterpart in the reference.  A matvec server for callers that issue
+ * matvecs on many geometries at once (iterative boundary-integral solvers):
+ * sessions (DDFMM_MIXED) are admitted against a device-memory budget and a
+ * serving thread batches pending requests across sessions.  Each tick takes
+ * the oldest pending request of every admitted session and evaluates them
+ * together (one masked batch matvec); requests arriving meanwhile go to the
+ * next tick.  Sessions are created by an admission thread; one that does not
+ * fit the budget waits, in order, until a removal frees memory, and one
+ * larger than the whole budget is rejected. */
+typedef struct ddfmm_server ddfmm_server;
+enum {
+    DDFMM_SESSION_WAITING = 0,
+    DDFMM_SESSION_ADMITTED = 1,
+    DDFMM_SESSION_REJECTED = 2,
+    DDFMM_SESSION_REMOVED = 3,
+    DDFMM_SESSION_FAILED = 4
+};
+typedef struct ddfmm_server_stats {
+    long long requests;       /* completed since the last reset */
+    long long ticks;
+    double mean_batch;        /* requests per tick */
+    double p50_ms, p99_ms, max_ms;  /* submit -> completion */
+    double busy_s;            /* time spent in ticks */
+    long long used_bytes;     /* device bytes of the admitted sessions */
+    int admitted, waiting;
+} ddfmm_server_stats;
+int ddfmm_server_create(int device, double budget_bytes, ddfmm_server** out);
+/* Arguments as ddfmm_session_create; the session is queued for admission on
+ * the server's device.  *sid identifies it. */
+int ddfmm_server_add_session(ddfmm_server* sv, const double* pos3n, int n, int kernel, int accu, int npq, double K,
+                             const double* ctr3, int ptsmax, int maxlevel, int ncell, const char* ld_path,
+                             const char* hd_path, int* sid);
+/* *state = DDFMM_SESSION_*; for REJECTED / FAILED ddfmm_last_error gives why. */
+int ddfmm_server_session_state(ddfmm_server* sv, int sid, int* state);
+/* Queued requests of a removed session fail; its memory is released between ticks. */
+int ddfmm_server_remove_session(ddfmm_server* sv, int sid);
+/* Queue one matvec: den / val are complex64 host arrays of the session's n
+ * points (interleaved floats) that must stay valid until it completes. */
+int ddfmm_server_submit(ddfmm_server* sv, int sid, const float* den, float* val, long long* ticket);
+/* *done = 1 when the request completed (val filled), 0 after timeout_s;
+ * a failed request returns an error status with the reason. */
+int ddfmm_server_wait(ddfmm_server* sv, long long ticket, double timeout_s, int* done);
+int ddfmm_server_poll(ddfmm_server* sv, long long ticket, int* done);
+int ddfmm_server_get_stats(ddfmm_server* sv, ddfmm_server_stats* out, int reset);
+int ddfmm_server_destroy(ddfmm_server* sv);
+
 #ifdef __cplusplus
 }
 #endif
