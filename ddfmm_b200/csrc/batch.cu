@@ -1,6 +1,8 @@
 // Merged multi-instance launch sequence (see batch.hpp).
 #include "batch.hpp"
 
+#include <algorithm>
+#include <cstring>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -36,6 +38,8 @@ void Batch::add(Kind kind, const std::vector<Sub>& subs, const std::vector<Pre>&
     L.nsub = (int)subs.size();
     L.total = (long long)prefix.back();
     L.G = G;
+    static_assert(sizeof(Sub) <= sizeof(L.one), "sub-launch larger than its host copy");
+    std::memcpy(L.one, subs.data(), sizeof(Sub));
     if (L.total > 0) launches_.push_back(L);
 }
 
@@ -181,7 +185,8 @@ void Batch::run(const int* active, cudaStream_t s) {
                 break;
             case GEMM:
                 launch_umma_cgemm(static_cast<const UmmaSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub,
-                                  (int)L.total, active, d_err_, s);
+                                  (int)L.total, active, d_err_, s,
+                                  L.nsub == 1 ? reinterpret_cast<const UmmaSub*>(L.one) : nullptr);
                 break;
             case PT:
                 launch_pt32(static_cast<const PtSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub, (int)L.total,
@@ -189,11 +194,11 @@ void Batch::run(const int* active, cudaStream_t s) {
                 break;
             case VFWD:
                 launch_vlist_forward32(static_cast<const VfSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub,
-                                       (int)L.total, L.G, active, nullptr, s);
+                                       (int)L.total, L.G, active, nullptr, s, L.nsub == 1 ? reinterpret_cast<const VfSub*>(L.one) : nullptr);
                 break;
             case VACC:
                 launch_vlist_accum32(static_cast<const VaSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub,
-                                     (int)L.total, L.G, active, nullptr, s);
+                                     (int)L.total, L.G, active, nullptr, s, L.nsub == 1 ? reinterpret_cast<const VaSub*>(L.one) : nullptr);
                 break;
         }
     }

@@ -49,6 +49,7 @@ private:
         int nsub;
         long long total;
         int G;
+        alignas(16) unsigned char one[256];  // host copy of the first sub-launch
     };
     template <class Sub, class Pre>
     void add(Kind kind, const std::vector<Sub>& subs, const std::vector<Pre>& counts, int G = 0);

@@ -135,10 +135,12 @@ struct ZeroSub {
 };
 void launch_pt32(const PtSub* subs, const int* prefix, int nsub, int nitems, const int* active, cudaStream_t s);
 void vlist32_init(int G);
+// A launch with nsub == 1 passes its sub-launch as `one` (host copy, sent as
+// a kernel parameter); `subs` / `prefix` are then not read.
 void launch_vlist_forward32(const VfSub* subs, const int* prefix, int nsub, int nbox, int G, const int* active,
-                            void* spec_override, cudaStream_t s);
+                            void* spec_override, cudaStream_t s, const VfSub* one);
 void launch_vlist_accum32(const VaSub* subs, const int* prefix, int nsub, int ntrg, int G, const int* active,
-                          const void* spec_override, cudaStream_t s);
+                          const void* spec_override, cudaStream_t s, const VaSub* one);
 void launch_move32(const MoveSub* subs, const int* prefix, int nsub, int n, const int* active, int scatter,
                    cudaStream_t s);
 void launch_zero(const ZeroSub* subs, const long long* prefix, int nsub, long long n8, const int* active,
@@ -186,8 +188,9 @@ int umma_nkb(int k);
 size_t umma_tile_stride(int k);
 size_t umma_packed_floats(int m, int k);
 void launch_umma_pack(const UmmaPackJob* jobs_dev, int njobs, cudaStream_t s);
+// nsub == 1: `one` is that sub-launch (host copy, sent as a kernel parameter)
 void launch_umma_cgemm(const UmmaSub* subs, const int* prefix, int nsub, int ntiles, const int* active, int* err,
-                       cudaStream_t s);
+                       cudaStream_t s, const UmmaSub* one);
 
 // gather/scatter helpers
 void launch_gather_den(const double2* den, const int* perm, double2* out, int n, cudaStream_t s);

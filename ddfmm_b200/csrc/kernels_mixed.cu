@@ -284,18 +284,34 @@ void launch_pt32(const PtSub* subs, const int* prefix, int nsub, int nitems, con
 // per source box (forward) or target box (accumulate).  All sub-launches of a
 // launch share G = 2P; spec_override, when set, replaces every sub-launch's
 // spectra array (fixed-scratch entry point, single instance).
-__global__ void vlist_forward32_kernel(const VfSub* __restrict__ subs, const int* __restrict__ prefix, int nsub,
-                                       const int* __restrict__ active, float2* spec_override) {
-    extern __shared__ float2 sm32[];
-    __shared__ VfSub S;
-    __shared__ int local;
+// MULTI = false: the single sub-launch `one` (kernel parameter space, as a
+// one-instance launch); MULTI = true: the block's sub-launch from `subs`.
+template <bool MULTI>
+__device__ __forceinline__ void vlist_forward32_body(const VfSub& S, int local, float2* spec_override);
+
+template <bool MULTI>
+__global__ void __launch_bounds__(256) vlist_forward32_kernel(const VfSub one, const VfSub* __restrict__ subs,
+                                                              const int* __restrict__ prefix, int nsub,
+                                                              const int* __restrict__ active, float2* spec_override) {
+    if (!MULTI) {
+        vlist_forward32_body<MULTI>(one, blockIdx.x, spec_override);
+        return;
+    }
+    __shared__ VfSub Sm;
+    __shared__ int lm;
     if (threadIdx.x == 0) {
         const int j = find_sub(prefix, nsub, (int)blockIdx.x);
-        S = subs[j];
-        local = blockIdx.x - prefix[j];
+        Sm = subs[j];
+        lm = blockIdx.x - prefix[j];
     }
     __syncthreads();
-    if (active && !active[S.inst]) return;
+    if (active && !active[Sm.inst]) return;
+    vlist_forward32_body<MULTI>(Sm, lm, spec_override);
+}
+
+template <bool MULTI>
+__device__ __forceinline__ void vlist_forward32_body(const VfSub& S, int local, float2* spec_override) {
+    extern __shared__ float2 sm32[];
     const VlistLevel& L = S.L;
     const float2* twf = reinterpret_cast<const float2*>(L.twf);
     const float2* upeq = S.upeq;
@@ -333,21 +349,33 @@ __global__ void vlist_forward32_kernel(const VfSub* __restrict__ subs, const int
 }
 
 template <int G>
-__global__ void __launch_bounds__(256) vlist_accum32_kernel(const VaSub* __restrict__ subs,
+__device__ __forceinline__ void vlist_accum32_body(const VaSub& S, int local, const float2* spec_override);
+
+template <int G, bool MULTI>
+__global__ void __launch_bounds__(256) vlist_accum32_kernel(const VaSub one, const VaSub* __restrict__ subs,
                                                             const int* __restrict__ prefix, int nsub,
                                                             const int* __restrict__ active,
                                                             const float2* spec_override) {
-    extern __shared__ float2 sm32[];
-    constexpr int P = G / 2, PP = P * P, G3 = G * G * G, NE = (G3 + 255) / 256;
-    __shared__ VaSub S;
-    __shared__ int local;
+    if (!MULTI) {
+        vlist_accum32_body<G>(one, blockIdx.x, spec_override);
+        return;
+    }
+    __shared__ VaSub Sm;
+    __shared__ int lm;
     if (threadIdx.x == 0) {
         const int j = find_sub(prefix, nsub, (int)blockIdx.x);
-        S = subs[j];
-        local = blockIdx.x - prefix[j];
+        Sm = subs[j];
+        lm = blockIdx.x - prefix[j];
     }
     __syncthreads();
-    if (active && !active[S.inst]) return;
+    if (active && !active[Sm.inst]) return;
+    vlist_accum32_body<G>(Sm, lm, spec_override);
+}
+
+template <int G>
+__device__ __forceinline__ void vlist_accum32_body(const VaSub& S, int local, const float2* spec_override) {
+    extern __shared__ float2 sm32[];
+    constexpr int P = G / 2, PP = P * P, G3 = G * G * G, NE = (G3 + 255) / 256;
     const VlistLevel& L = S.L;
     const float2* twb = reinterpret_cast<const float2*>(L.twb);
     const float2* spec = spec_override ? spec_override : S.spec;
@@ -408,33 +436,57 @@ static size_t vacc32_smem(int G, int P) { return sizeof(float2) * (G * G * G + G
 
 void vlist32_init(int G) {
     int P = G / 2;
-    cudaFuncSetAttribute(vlist_forward32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vfwd32_smem(G, P));
-    cudaFuncSetAttribute(vlist_accum32_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vacc32_smem(8, 4));
-    cudaFuncSetAttribute(vlist_accum32_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)vacc32_smem(12, 6));
-    cudaFuncSetAttribute(vlist_accum32_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)vacc32_smem(16, 8));
+    const int fs = (int)vfwd32_smem(G, P);
+    cudaFuncSetAttribute(vlist_forward32_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, fs);
+    cudaFuncSetAttribute(vlist_forward32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, fs);
+    const int a8 = (int)vacc32_smem(8, 4), a12 = (int)vacc32_smem(12, 6), a16 = (int)vacc32_smem(16, 8);
+    cudaFuncSetAttribute(vlist_accum32_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a8);
+    cudaFuncSetAttribute(vlist_accum32_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, a8);
+    cudaFuncSetAttribute(vlist_accum32_kernel<12, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a12);
+    cudaFuncSetAttribute(vlist_accum32_kernel<12, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, a12);
+    cudaFuncSetAttribute(vlist_accum32_kernel<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a16);
+    cudaFuncSetAttribute(vlist_accum32_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, a16);
 }
 
 // L.tns, L.twf, L.twb hold float2 data in this form.
 void launch_vlist_forward32(const VfSub* subs, const int* prefix, int nsub, int nbox, int G, const int* active,
-                            void* spec_override, cudaStream_t s) {
+                            void* spec_override, cudaStream_t s, const VfSub* one) {
     if (nbox == 0) return;
-    vlist_forward32_kernel<<<nbox, 256, vfwd32_smem(G, G / 2), s>>>(subs, prefix, nsub, active,
-                                                                     static_cast<float2*>(spec_override));
+    VfSub o{};
+    if (nsub == 1) {
+        if (!one) return;  // a single sub-launch is passed by value
+        o = *one;
+    }
+    const size_t sm = vfwd32_smem(G, G / 2);
+    float2* so = static_cast<float2*>(spec_override);
+    if (nsub == 1)
+        vlist_forward32_kernel<false><<<nbox, 256, sm, s>>>(o, subs, prefix, nsub, active, so);
+    else
+        vlist_forward32_kernel<true><<<nbox, 256, sm, s>>>(o, subs, prefix, nsub, active, so);
 }
 
 void launch_vlist_accum32(const VaSub* subs, const int* prefix, int nsub, int ntrg, int G, const int* active,
-                          const void* spec_override, cudaStream_t s) {
+                          const void* spec_override, cudaStream_t s, const VaSub* one) {
     if (ntrg == 0) return;
+    VaSub o{};
+    if (nsub == 1) {
+        if (!one) return;  // a single sub-launch is passed by value
+        o = *one;
+    }
     const size_t sm = vacc32_smem(G, G / 2);
     const float2* so = static_cast<const float2*>(spec_override);
+#define DDFMM_VACC(g)                                                                          \
+    if (nsub == 1)                                                                             \
+        vlist_accum32_kernel<g, false><<<ntrg, 256, sm, s>>>(o, subs, prefix, nsub, active, so); \
+    else                                                                                       \
+        vlist_accum32_kernel<g, true><<<ntrg, 256, sm, s>>>(o, subs, prefix, nsub, active, so);
     switch (G) {
-        case 8: vlist_accum32_kernel<8><<<ntrg, 256, sm, s>>>(subs, prefix, nsub, active, so); break;
-        case 12: vlist_accum32_kernel<12><<<ntrg, 256, sm, s>>>(subs, prefix, nsub, active, so); break;
-        case 16: vlist_accum32_kernel<16><<<ntrg, 256, sm, s>>>(subs, prefix, nsub, active, so); break;
+        case 8: DDFMM_VACC(8) break;
+        case 12: DDFMM_VACC(12) break;
+        case 16: DDFMM_VACC(16) break;
         default: break;
     }
+#undef DDFMM_VACC
 }
 
 // Batch I/O: complex64 densities in point-id order into leaf order (gather),

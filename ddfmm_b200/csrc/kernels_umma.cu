@@ -257,6 +257,30 @@ size_t umma_packed_floats(int m, int k) {
 }
 
 // ---------------------------------------------------------------- GEMM
+// Epilogue stores of one parked chunk: 32 / PCH columns per instruction, PCH
+// consecutive rows each; column c of the warp's 32 writes at Y + (c's yoff) + i.
+template <int MODE>
+__device__ __forceinline__ void store_chunk(const float2* park, float2* Y, long long my_yo, int col_base, int ncol,
+                                            int i, int rows, int lane) {
+    const int sub = lane / PCH, r = lane % PCH;
+    for (int cc = 0; cc < 32; cc += 32 / PCH) {
+        const int col = cc + sub;
+        const long long yb = __shfl_sync(0xffffffffu, my_yo, col);
+        if (col_base + cc >= ncol) break;
+        if (i >= rows || col_base + col >= ncol) continue;
+        const float2 val = park[col * (PCH + 1) + r];
+        float2* y = Y + yb + i;
+        if (MODE == GEMM_SET) {
+            *y = val;
+        } else if (MODE == GEMM_ADD) {
+            const float2 o = *y;
+            *y = make_float2(o.x + val.x, o.y + val.y);
+        } else {
+            atomicAdd(y, val);
+        }
+    }
+}
+
 // Tile ti of a launch: its sub-launch (prefix[j] <= ti < prefix[j+1]), tile and
 // problem; `on` is false when the sub-launch's instance is inactive.
 struct TileInfo {
@@ -269,22 +293,27 @@ struct TileInfo {
     int mode;
     bool on;
 };
-// subs / prefix: the block's shared-memory copies (U_SUBS_SMEM entries at most)
-// or the global arrays
-__device__ __forceinline__ TileInfo tile_info(const UmmaSub* subs, const int* prefix, int nsub,
+// MULTI = false: the launch's only sub-launch `one` (kernel parameter space);
+// else subs / prefix: the block's shared-memory copies (U_SUBS_SMEM entries at
+// most) or the global arrays
+template <bool MULTI>
+__device__ __forceinline__ TileInfo tile_info(const UmmaSub& one, const UmmaSub* subs, const int* prefix, int nsub,
                                               const int* __restrict__ active, int ti) {
-    int lo = 0, hi = nsub - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (prefix[mid] <= ti)
-            lo = mid;
-        else
-            hi = mid - 1;
+    int lo = 0;
+    if (MULTI) {
+        int hi = nsub - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= ti)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
     }
-    const UmmaSub& S = subs[lo];
+    const UmmaSub& S = MULTI ? subs[lo] : one;
     TileInfo r;
     r.on = !active || active[S.inst];
-    r.t = S.tiles[ti - prefix[lo]];
+    r.t = S.tiles[MULTI ? ti - prefix[lo] : ti];
     r.p = S.probs[r.t.prob];
     r.X = S.X;
     r.Y = S.Y;
@@ -297,14 +326,16 @@ __device__ __forceinline__ int tile_n(int rows) { return ((2 * rows + 15) / 16) 
 
 constexpr int U_SUBS_SMEM = 64;  // sub-launches cached in shared memory
 
-__global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub* __restrict__ gsubs,
+template <bool MULTI>
+__global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub one,
+                                                                 const UmmaSub* __restrict__ gsubs,
                                                                  const int* __restrict__ gprefix, int nsub,
                                                                  int ntiles, const int* __restrict__ active,
                                                                  int* err) {
     extern __shared__ __align__(1024) unsigned char usm_raw[];
-    __shared__ UmmaSub ssubs[U_SUBS_SMEM];
-    __shared__ int sprefix[U_SUBS_SMEM + 1];
-    const bool cached = nsub <= U_SUBS_SMEM;
+    __shared__ UmmaSub ssubs[MULTI ? U_SUBS_SMEM : 1];
+    __shared__ int sprefix[MULTI ? U_SUBS_SMEM + 1 : 1];
+    const bool cached = MULTI && nsub <= U_SUBS_SMEM;
     if (cached) {
         for (int i = threadIdx.x; i < nsub; i += blockDim.x) ssubs[i] = gsubs[i];
         for (int i = threadIdx.x; i <= nsub; i += blockDim.x) sprefix[i] = gprefix[i];
@@ -361,7 +392,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub* 
         const float2* X = nullptr;
         auto load_tile = [&]() {  // the first active tile from ti_i on
             for (; ti_i < ntiles; ti_i += gridDim.x) {
-                const TileInfo T = tile_info(subs, prefix, nsub, active, ti_i);
+                const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, active, ti_i);
                 if (!T.on) continue;
                 nkb_i = T.p.nkb;
                 k_i = T.p.k;
@@ -370,7 +401,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub* 
 #pragma unroll
                 for (int i = 0; i < CPB; ++i) {
                     const int c = cw * 32 + i * (32 / CPB) + lane / CPB;
-                    xr[i] = c < ncol ? T.xoff[T.p.col0 + T.t.col0 + c] : -1;
+                    xr[i] = c < ncol ? __ldg(T.xoff + T.p.col0 + T.t.col0 + c) : -1;
                 }
                 return;
             }
@@ -386,7 +417,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub* 
             const int kc = kb_i * CPB + q;
 #pragma unroll
             for (int i = 0; i < CPB; ++i)
-                dst[i] = (xr[i] >= 0 && kc < k_i) ? X[xr[i] + kc] : make_float2(0.f, 0.f);
+                dst[i] = (xr[i] >= 0 && kc < k_i) ? __ldg(X + xr[i] + kc) : make_float2(0.f, 0.f);
             for (int a = 0; a < UPSETS && ti_i < ntiles; ++a) advance();
         };
         load_tile();
@@ -440,7 +471,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub* 
         if (lane == 0) {
             int g = 0;
             for (int ti = blockIdx.x; ti < ntiles && !*failed; ti += gridDim.x) {
-                const TileInfo T = tile_info(subs, prefix, nsub, active, ti);
+                const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, active, ti);
                 if (!T.on) continue;
                 const char* Bt = reinterpret_cast<const char*>(T.p.B + (size_t)T.t.rtile * T.p.tile_stride);
                 const uint32_t blk = (uint32_t)tile_n(T.t.rows) * UBK * 4;
@@ -463,7 +494,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub* 
         if (lane == 0) {
             int g = 0, it = 0, last = -1;
             for (int ti = blockIdx.x; ti < ntiles && !*failed; ti += gridDim.x) {
-                const TileInfo T = tile_info(subs, prefix, nsub, active, ti);
+                const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, active, ti);
                 if (!T.on) continue;
                 const uint32_t idesc = idesc_tf32(tile_n(T.t.rows));
                 const int acc = it & 1;
@@ -505,13 +536,13 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub* 
         float2* park = park_all + qw * (32 * (PCH + 1));
         int it = 0;
         for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
-            const TileInfo T = tile_info(subs, prefix, nsub, active, ti);
+            const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, active, ti);
             if (!T.on) continue;
             const int ncol = min(UM, T.p.ncol - T.t.col0);
             const int rows = T.t.rows, N = tile_n(rows);
             const int acc = it & 1;
             const int mycol = qw * 32 + lane;
-            const long long my_yo = mycol < ncol ? T.yoff[T.p.col0 + T.t.col0 + mycol] + T.t.row0 : 0;
+            const long long my_yo = mycol < ncol ? __ldg(T.yoff + T.p.col0 + T.t.col0 + mycol) + T.t.row0 : 0;
             float2* const Y = T.Y;
             const int mode = T.mode;
             bool ok = !*failed && mbar_wait(&tmem_full[acc], (it >> 1) & 1, failed);
@@ -552,25 +583,13 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub* 
                     }
                 }
                 __syncwarp();
-                // 32 / PCH columns per store instruction, PCH consecutive rows each
-                const int sub = lane / PCH, r = lane % PCH;
-                const int i = (c0 >> 1) + r;  // complex row of this lane
-                for (int cc = 0; cc < 32; cc += 32 / PCH) {
-                    const int col = cc + sub;
-                    const long long yb = __shfl_sync(0xffffffffu, my_yo, col);
-                    if (qw * 32 + cc >= ncol) break;
-                    if (i >= rows || qw * 32 + col >= ncol) continue;
-                    const float2 val = park[col * (PCH + 1) + r];
-                    float2* y = Y + yb + i;
-                    if (mode == GEMM_SET) {
-                        *y = val;
-                    } else if (mode == GEMM_ADD) {
-                        const float2 o = *y;
-                        *y = make_float2(o.x + val.x, o.y + val.y);
-                    } else {
-                        atomicAdd(y, val);
-                    }
-                }
+                const int i = (c0 >> 1) + lane % PCH;  // complex row of this lane
+                if (mode == GEMM_SET)
+                    store_chunk<GEMM_SET>(park, Y, my_yo, qw * 32, ncol, i, rows, lane);
+                else if (mode == GEMM_ADD)
+                    store_chunk<GEMM_ADD>(park, Y, my_yo, qw * 32, ncol, i, rows, lane);
+                else
+                    store_chunk<GEMM_ATOMIC>(park, Y, my_yo, qw * 32, ncol, i, rows, lane);
                 __syncwarp();
             }
             ++it;
@@ -592,18 +611,24 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub* 
 static int g_umma_sms = 0;
 
 void umma_init() {
-    cudaFuncSetAttribute(umma_cgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, UGEMM_SMEM);
+    cudaFuncSetAttribute(umma_cgemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, UGEMM_SMEM);
+    cudaFuncSetAttribute(umma_cgemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, UGEMM_SMEM);
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_umma_sms, cudaDevAttrMultiProcessorCount, dev);
 }
 
 void launch_umma_cgemm(const UmmaSub* subs, const int* prefix, int nsub, int ntiles, const int* active, int* err,
-                       cudaStream_t s) {
+                       cudaStream_t s, const UmmaSub* one) {
     if (ntiles == 0) return;
     const int sms = g_umma_sms > 0 ? g_umma_sms : 148;
     const int grid = ntiles < sms ? ntiles : sms;
-    umma_cgemm_kernel<<<grid, UTHREADS, UGEMM_SMEM, s>>>(subs, prefix, nsub, ntiles, active, err);
+    if (nsub == 1) {
+        if (!one) return;  // a single sub-launch is passed by value
+        umma_cgemm_kernel<false><<<grid, UTHREADS, UGEMM_SMEM, s>>>(*one, subs, prefix, nsub, ntiles, active, err);
+    } else {
+        umma_cgemm_kernel<true><<<grid, UTHREADS, UGEMM_SMEM, s>>>(UmmaSub{}, subs, prefix, nsub, ntiles, active, err);
+    }
 }
 
 }  // namespace ddfmm

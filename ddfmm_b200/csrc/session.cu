@@ -1285,14 +1285,14 @@ void Session::launch_step(const Step& st, cudaStream_t s, double2* spec) {
         case 2:
             if (m)
                 launch_vlist_forward32(static_cast<const VfSub*>(st.msubs), st.mpre, 1, st.mtotal, st.v.L.G, nullptr,
-                                       spec != st.v.spec ? spec : nullptr, s);
+                                       spec != st.v.spec ? spec : nullptr, s, &st.hvf);
             else
                 launch_vlist_forward(st.v.L, st.v.src_boxes, st.v.nsrc, st.v.upeq, spec, s);
             break;
         case 3:
             if (m)
                 launch_vlist_accum32(static_cast<const VaSub*>(st.msubs), st.mpre, 1, st.mtotal, st.v.L.G, nullptr,
-                                     spec != st.v.spec ? spec : nullptr, s);
+                                     spec != st.v.spec ? spec : nullptr, s, &st.hva);
             else
                 launch_vlist_accum(st.v.L, st.v.trg, st.v.ntrg, st.v.vptr, st.v.vsrc, st.v.voff, spec, st.v.dnchk, s);
             break;
@@ -1300,7 +1300,7 @@ void Session::launch_step(const Step& st, cudaStream_t s, double2* spec) {
             CK(cudaMemsetAsync(st.ms.p, 0, st.ms.bytes, s));
             break;
         case 5:
-            launch_umma_cgemm(static_cast<const UmmaSub*>(st.msubs), st.mpre, 1, st.mtotal, nullptr, d_err_, s);
+            launch_umma_cgemm(static_cast<const UmmaSub*>(st.msubs), st.mpre, 1, st.mtotal, nullptr, d_err_, s, &st.hu);
             break;
     }
 }
