@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-json", default=None, help="write the per-pass profile here")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form measurement")
+    ap.add_argument("--no-served", action="store_true", help="skip the continuous-batching server measurement")
     ap.add_argument("--mixed-mma-sync", action="store_true",
                     help="also measure the mixed form with its translations on the mma.sync path")
     return ap.parse_args()
@@ -249,6 +250,121 @@ def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws, profile_json=None, 
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))}}
 
 
+def served_workloads():
+    """The served mix: the bench sphere (K=64) plus smaller spheres and
+    ellipsoids (K = 16, 8, 4; N = 25 pi K^2 points each), all P=6, seeded."""
+    from ddfmm_b200 import geometry, workloads as wl
+    out = [wl.LARGE]
+    seed = 1
+    for K, count in ((16, 2), (8, 6), (4, 7)):
+        for j in range(count):
+            n = geometry.sphere_n_for(K)
+            out.append(wl.sphere(K, n, accu=2, seed=seed) if j % 2 == 0 else wl.ellipsoid(K, n, accu=2, seed=seed))
+            seed += 1
+    return out
+
+
+def measure_served(large_plain_e2e_s, budget_gb=30.0, closed_s=4.0, poisson_s=4.0):
+    """Continuous-batching server (mixed form) on the served mix against the
+    plain FP64 form serving the same requests one at a time."""
+    import threading
+    from ddfmm_b200 import _lib, wave3d
+    ws_list = served_workloads()
+    t0 = time.perf_counter()
+    sv = wave3d.Server(budget_bytes=budget_gb * 1e9)
+    sids = [sv.add_workload(w) for w in ws_list]
+    states = sv.wait_admitted(sids)
+    admit_s = time.perf_counter() - t0
+    live = [(sid, w) for sid, w, st in zip(sids, ws_list, states) if st == sv.ADMITTED]
+    rng = np.random.default_rng(5)
+    dens = {sid: (rng.standard_normal(w.N) + 1j * rng.standard_normal(w.N)).astype(np.complex64) for sid, w in live}
+    # closed loop: one request outstanding per session
+    sv.stats(reset=True)
+    stop = time.perf_counter() + closed_s
+    counts = {}
+
+    def client(sid, w):
+        v = np.zeros(w.N, dtype=np.complex64)
+        n = 0
+        while time.perf_counter() < stop:
+            t = sv.submit(sid, dens[sid], v)
+            sv.wait(t, 120.0)
+            n += 1
+        counts[sid] = n
+
+    th = [threading.Thread(target=client, args=lw) for lw in live]
+    tc = time.perf_counter()
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    closed_wall = time.perf_counter() - tc
+    cst = sv.stats(reset=True)
+    closed_rate = cst["requests"] / closed_wall
+    # open loop: Poisson arrivals at half the saturated rate, sessions drawn uniformly
+    lam = 0.5 * closed_rate
+    arrivals = []
+    tickets = []
+    t_end = time.perf_counter() + poisson_s
+    t_next = time.perf_counter()
+    while True:
+        t_next += rng.exponential(1.0 / lam)
+        if t_next > t_end:
+            break
+        dt = t_next - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        k = int(rng.integers(len(live)))
+        sid, w = live[k]
+        v = np.zeros(w.N, dtype=np.complex64)
+        tickets.append((sv.submit(sid, dens[sid], v), v))
+        arrivals.append((t_next, k))
+    for t, v in tickets:
+        sv.wait(t, 120.0)
+    pst = sv.stats(reset=True)
+    used_gb = sv.stats()["used_bytes"] / 1e9
+    sv.close()
+    # plain FP64 per request: end-to-end service time of each session (host arrays in and out)
+    service = []
+    for sid, w in live:
+        if w.name == ws_list[0].name:
+            service.append(large_plain_e2e_s)
+            continue
+        p = wave3d.from_workload(w, precision=_lib.PLAIN_FP64)
+        d = dens[sid].astype(np.complex128)
+        v = np.zeros(w.N, dtype=np.complex128)
+        p.eval(d, v)
+        ts = []
+        for _ in range(5):
+            a = time.perf_counter()
+            p.eval(d, v)
+            ts.append(time.perf_counter() - a)
+        p.close()
+        service.append(float(np.median(ts)))
+    plain_closed_rate = len(live) / sum(service)
+    # the same Poisson arrivals served one at a time in arrival order
+    free_at, lat = 0.0, []
+    for ta, k in arrivals:
+        start = max(ta, free_at)
+        free_at = start + service[k]
+        lat.append((free_at - ta) * 1e3)
+    lat = np.array(lat) if lat else np.zeros(1)
+    return {"sessions": len(live), "waiting": len(sids) - len(live), "budget_gb": budget_gb,
+            "device_gb_used": used_gb, "admission_s": admit_s,
+            "mix": "K=64 sphere N=321699 + 2 x K=16, 6 x K=8, 7 x K=4 spheres/ellipsoids (N = 25 pi K^2), P=6",
+            "saturated": {"value": closed_rate, "unit": "matvec/s", "mean_batch": cst["mean_batch"],
+                          "p50_ms": cst["p50_ms"], "p99_ms": cst["p99_ms"]},
+            "poisson": {"rate_per_s": lam, "requests": pst["requests"], "mean_batch": pst["mean_batch"],
+                        "p50_ms": pst["p50_ms"], "p99_ms": pst["p99_ms"]},
+            "plain_fp64_per_request": {"value": plain_closed_rate, "unit": "matvec/s",
+                                       "poisson_p50_ms": float(np.percentile(lat, 50)),
+                                       "poisson_p99_ms": float(np.percentile(lat, 99)),
+                                       "how": "measured end-to-end service time per session, requests served one at a "
+                                              "time in arrival order"},
+            "speedup_saturated": closed_rate / plain_closed_rate,
+            "io": "host complex64 arrays in and out of the server (pinned staging, H2D/D2H inside each request)"}
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_env()
@@ -366,6 +482,9 @@ def run_ours(args):
     if not args.no_mixed:
         mixed = measure_mixed(w, wave_args=(local,), steps=args.steps, warmup=args.warmup, dev=dev, chk=chk, ws=ws,
                               profile_json=(args.profile_json + ".mixed") if args.profile_json else None)
+    served = None
+    if not args.no_served and ws == 1 and args.workload == "large":
+        served = measure_served(e2e_s)
     mixed_mma = None
     if args.mixed_mma_sync:
         from ddfmm_b200 import _lib
@@ -390,6 +509,8 @@ def run_ours(args):
                 "clocks": clocks, "cpu_baseline": cpu, "mixed_form": mixed, "passes": passes}
         if mixed_mma:
             line["mixed_form_mma_sync"] = mixed_mma
+        if served:
+            line["served"] = served
         print(json.dumps(line), flush=True)
     wave.close()
     if ws > 1:

@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
+#include <set>
 #include <unordered_map>
 
 namespace ddfmm {
@@ -43,8 +44,18 @@ T* Session::dalloc(size_t count) {
     void* p = nullptr;
     CK(cudaMalloc(&p, count * sizeof(T)));
     allocs_.push_back(p);
+    alloc_bytes_[p] = count * sizeof(T);
     stats_.device_bytes += count * sizeof(T);
     return static_cast<T*>(p);
+}
+
+void Session::dfree(const void* p) {
+    auto it = alloc_bytes_.find(p);
+    if (it == alloc_bytes_.end()) return;  // not an allocation of this session (or an interior pointer)
+    CK(cudaFree(const_cast<void*>(p)));
+    stats_.device_bytes -= it->second;
+    alloc_bytes_.erase(it);
+    allocs_.erase(std::remove(allocs_.begin(), allocs_.end(), p), allocs_.end());
 }
 
 template <class T>
@@ -129,11 +140,11 @@ const float* Session::packed_operator(const GemmProblem& q) {
     const auto key = std::make_pair((const void*)q.A, ((long long)q.m << 32) | (long long)q.k);
     auto it = packed_.find(key);
     if (it != packed_.end()) return it->second;
-    // packed operators are sub-allocated from 256 MiB chunks (16-byte aligned: they are
-    // read with cp.async.bulk)
+    // packed operators are sub-allocated from 16 MiB chunks (256-byte aligned; cp.async.bulk
+    // needs 16); one larger than a chunk gets its own allocation
     const size_t nf = (umma_packed_floats(q.m, q.k) + 63) & ~(size_t)63;
     if (nf > arena_left_) {
-        const size_t chunk = std::max(nf, (size_t)64 << 20);
+        const size_t chunk = std::max(nf, (size_t)4 << 20);
         arena_ = dalloc<float>(chunk);
         arena_left_ = chunk;
     }
@@ -1253,6 +1264,17 @@ void Session::build() {
             }
     }
     flush_packs();
+    if (mixed) {
+        // the mixed eval reads only the FP32 copies (and, on tcgen05, only the packed
+        // GEMM operators): release the FP64 operators and the unpacked GEMM copies
+        CK(cudaStreamSynchronize(stream_));
+        std::set<const void*> vlist32{d_twf, d_twb};
+        for (auto& kv : lfops) vlist32.insert(kv.second.tns);
+        for (auto& kv : op32) {
+            dfree(kv.first);
+            if (umma() && !vlist32.count(kv.second)) dfree(kv.second);
+        }
+    }
     stats_.kernel_launches = (long long)steps_.size() + 2;
 }
 

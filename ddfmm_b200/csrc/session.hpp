@@ -140,6 +140,7 @@ private:
     T* dalloc(size_t count);
     template <class T>
     T* upload(const std::vector<T>& v);
+    void dfree(const void* p);  // release one allocation made by dalloc / upload
     void add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<long long> >& xo,
                   std::vector<std::vector<long long> >& yo, const double2* X, double2* Y, int mode,
                   const char* label);
@@ -163,6 +164,7 @@ private:
     Tree tree_;
     OperatorLib ops_;
     std::vector<void*> allocs_;
+    std::map<const void*, size_t> alloc_bytes_;
     std::vector<Step> steps_;
     cudaStream_t stream_ = nullptr;
     SessionStats stats_;
