@@ -15,6 +15,7 @@ struct GemmProblem {
     int m, k, lda;
     int col0;  // first entry in the column arrays
     int ncol;
+    const float* packed;  // tcgen05 form: an already packed copy of A (A may then be null)
 };
 // A launch is a list of output tiles of up to GEMM_TILE_M rows x GEMM_TILE_N columns.
 constexpr int GEMM_TILE_M = 64, GEMM_TILE_N = 64;

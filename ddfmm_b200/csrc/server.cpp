@@ -140,7 +140,7 @@ ServerStats Server::stats(bool reset) {
         s.p99_ms = pct(0.99);
         s.max_ms = v.back();
     }
-    s.used_bytes = used_;
+    s.used_bytes = used_ + DevChunk::live_bytes(device_);
     for (auto& kv : entries_) {
         if (kv.second->state == ADMITTED) s.admitted++;
         if (kv.second->state == WAITING) s.waiting++;
@@ -177,7 +177,10 @@ void Server::admission_loop() {
             err = "pinned host staging allocation failed";
             s.reset();
         }
-        const size_t bytes = s ? s->stats().device_bytes : 0;
+        // device memory: the session's own buffers plus the packed-operator chunks alive
+        // on the device, which sessions share and which are counted once
+        const size_t total = s ? s->stats().device_bytes : 0;
+        const size_t bytes = s ? total - s->chunk_bytes() : 0;
         lk.lock();
         if (waiting_.empty() || waiting_.front() != sid || e->state != WAITING) {  // removed meanwhile
             lk.unlock();
@@ -191,17 +194,17 @@ void Server::admission_loop() {
             waiting_.pop_front();
             e->state = FAILED;
             e->why = err;
-        } else if (bytes > budget_) {
+        } else if (total > budget_) {
             waiting_.pop_front();
             e->state = REJECTED;
-            e->why = "needs " + std::to_string(bytes) + " device bytes, more than the budget of " +
+            e->why = "needs " + std::to_string(total) + " device bytes, more than the budget of " +
                      std::to_string(budget_);
             lk.unlock();
             s.reset();
             cudaFreeHost(hd);
             cudaFreeHost(hv);
             lk.lock();
-        } else if (used_ + bytes > budget_) {
+        } else if (used_ + bytes + DevChunk::live_bytes(device_) > budget_) {
             // does not fit now: release it and wait for a removal
             blocked_ = true;
             lk.unlock();

@@ -13,7 +13,8 @@
 // Admission: add_session queues a session; an admission thread creates it
 // (tree, operators, device buffers: seconds for large ones, off the serving
 // thread) and admits it if the device bytes of the admitted sessions plus
-// its own stay within the budget.  A session that does not fit is released
+// its own stay within the budget (packed operators shared through the
+// process-wide cache are counted once).  A session that does not fit is released
 // and waits, in order, until a removal frees memory; one larger than the
 // whole budget is rejected.
 #pragma once
@@ -102,7 +103,7 @@ private:
     long long next_ticket_ = 1;
     std::map<long long, int> done_;  // ticket -> 0 done / -1 failed (until read by wait/poll)
     std::map<long long, std::string> failures_;
-    size_t used_ = 0;
+    size_t used_ = 0;  // own device bytes of the admitted sessions (shared operator chunks apart)
     bool changed_ = false;        // admitted set changed since the batch was built
     bool blocked_ = false;        // the head of the waiting queue did not fit
     std::vector<int> slots_;      // batch instance -> sid

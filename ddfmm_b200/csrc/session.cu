@@ -75,6 +75,8 @@ Session::Session(const double* pos3n, int n, const SessionParams& p, const std::
     CK(cudaSetDevice(p.device));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     pos_.assign(pos3n, pos3n + 3 * (size_t)n);
+    ld_path_ = ld_path;
+    hd_path_ = hd_path;
     ops_.load(ld_path, hd_path);
     tree_.build(pos_.data(), n, p.tree);
     build();
@@ -136,21 +138,37 @@ void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<
     stats_.gemm_launches++;
 }
 
+const float* Session::cached_op(const std::string& key) {
+    if (opctx_.empty()) return nullptr;
+    std::shared_ptr<PackedOp> e = OpCache::find(opctx_ + "|" + key);
+    if (!e) return nullptr;
+    held_.push_back(e);
+    return e->p;
+}
+
 const float* Session::packed_operator(const GemmProblem& q) {
+    if (q.packed) return q.packed;  // shared copy from the cache
     const auto key = std::make_pair((const void*)q.A, ((long long)q.m << 32) | (long long)q.k);
     auto it = packed_.find(key);
     if (it != packed_.end()) return it->second;
     // packed operators are sub-allocated from 16 MiB chunks (256-byte aligned; cp.async.bulk
-    // needs 16); one larger than a chunk gets its own allocation
+    // needs 16); one larger than a chunk gets its own
     const size_t nf = (umma_packed_floats(q.m, q.k) + 63) & ~(size_t)63;
-    if (nf > arena_left_) {
-        const size_t chunk = std::max(nf, (size_t)4 << 20);
-        arena_ = dalloc<float>(chunk);
-        arena_left_ = chunk;
+    if (nf > chunk_left_) {
+        const size_t floats = std::max(nf, (size_t)4 << 20);
+        chunk_ = std::make_shared<DevChunk>(prm_.device, floats * sizeof(float));
+        chunk_pos_ = chunk_->data();
+        chunk_left_ = floats;
+        chunk_bytes_ += floats * sizeof(float);
+        stats_.device_bytes += floats * sizeof(float);
     }
-    float* d = arena_;
-    arena_ += nf;
-    arena_left_ -= nf;
+    float* d = chunk_pos_;
+    chunk_pos_ += nf;
+    chunk_left_ -= nf;
+    std::shared_ptr<PackedOp> op = std::make_shared<PackedOp>(PackedOp{chunk_, d});
+    held_.push_back(op);
+    auto k = opkey_.find((const void*)q.A);
+    if (k != opkey_.end()) to_publish_.push_back(std::make_pair(opctx_ + "|" + k->second, op));
     pack_jobs_.push_back(UmmaPackJob{(const float2*)q.A, d, umma_tile_stride(q.k), q.m, q.k, q.lda, umma_nkb(q.k)});
     return packed_[key] = d;
 }
@@ -221,6 +239,9 @@ void Session::flush_packs() {
     CK(cudaStreamSynchronize(stream_));
     CK(cudaFree(d));
     pack_jobs_.clear();
+    // packed and complete: other sessions may use them from now on
+    for (auto& kp : to_publish_) OpCache::publish(kp.first, kp.second);
+    to_publish_.clear();
 }
 
 void Session::check_device_error() {
@@ -353,6 +374,7 @@ void Session::build() {
     // complex state: double2 (plain FP64 form) or float2 (mixed form); plan
     // offsets are in elements, so both forms share one plan
     const bool mixed = this->mixed();
+    if (umma()) opctx_ = OpCache::context(prm_.device, kern, prm_.accu, prm_.tree.npq, ld_path_, hd_path_);
     const size_t es = mixed ? sizeof(float2) : sizeof(double2);
     auto E = [&](double2* base, size_t elems) { return (double2*)((char*)base + elems * es); };
     auto salloc = [&](size_t elems) { return (double2*)dalloc<char>(elems * es); };
@@ -666,9 +688,17 @@ void Session::build() {
         return o;
     };
     size_t scr = 0, keep = 0;
+    // cache keys of the shared operators: (kind, width, wedge, child or offset)
+    auto opk = [](const char* kind, double W, const Idx3& d, int a, int b = 0, int c = 0) {
+        char buf[128];
+        snprintf(buf, sizeof buf, "%s|%.17g|%d,%d,%d|%d,%d,%d", kind, W, d[0], d[1], d[2], a, b, c);
+        return std::string(buf);
+    };
     struct DirMats {
         size_t raw[8], tmp[8], fin[8];
         int mrows, mcols, canon, ccanon;
+        bool cached;            // all eight come from the shared cache
+        const float* pk[8];     // their packed copies
     };
     std::map<std::pair<double, Idx3>, DirMats> m2m_mats, l2l_mats;
     const double* lf_half_uep = nullptr;
@@ -699,7 +729,10 @@ void Session::build() {
             child_pts(W, up[i].dir, true, M.mcols, M.ccanon);
             M.mrows = dp.r2;
             M.canon = dp.canon;
-            for (int ind = 0; ind < 8; ++ind) {
+            M.cached = !opctx_.empty();
+            for (int ind = 0; ind < 8 && M.cached; ++ind)
+                M.cached = (M.pk[ind] = cached_op(opk("m2m", W, up[i].dir, ind))) != nullptr;
+            for (int ind = 0; ind < 8 && !M.cached; ++ind) {
                 size_t n = (size_t)M.mrows * M.mcols;
                 M.raw[ind] = take(scr, n);
                 if (M.ccanon >= 0) M.tmp[ind] = take(scr, n);
@@ -715,7 +748,10 @@ void Session::build() {
             child_pts(W, dn[i].dir, false, M.mrows, M.ccanon);
             M.mcols = dp.r2;
             M.canon = dp.canon;
-            for (int ind = 0; ind < 8; ++ind) {
+            M.cached = !opctx_.empty();
+            for (int ind = 0; ind < 8 && M.cached; ++ind)
+                M.cached = (M.pk[ind] = cached_op(opk("l2l", W, dn[i].dir, ind))) != nullptr;
+            for (int ind = 0; ind < 8 && !M.cached; ++ind) {
                 size_t n = (size_t)M.mrows * M.mcols;
                 M.raw[ind] = take(scr, n);
                 M.fin[ind] = take(keep, n);
@@ -730,6 +766,8 @@ void Session::build() {
         size_t raw, tmp, fin;
         int canon, r1;
         Pt3 shift;
+        const float* pk;  // packed copy from the shared cache, or null
+        std::string key;
     };
     std::vector<M2LMat> m2l_mats;
     std::map<int, std::vector<std::vector<long long> > > m2l_x, m2l_y;  // level -> per problem columns
@@ -763,8 +801,14 @@ void Session::build() {
                     const Canon& c = hfcanon[t.canon];
                     gid = (int)m2l_mats.size();
                     size_t n = (size_t)c.r1 * c.r1;
-                    M2LMat M{take(scr, n), take(scr, n), take(keep, n), t.canon, c.r1,
-                             Pt3{{oc[0] * W, oc[1] * W, oc[2] * W}}};
+                    const std::string k = opk("m2l", W, c.srt, oc[0], oc[1], oc[2]);
+                    const float* pk = cached_op(k);
+                    M2LMat M{0, 0, 0, t.canon, c.r1, Pt3{{oc[0] * W, oc[1] * W, oc[2] * W}}, pk, k};
+                    if (!pk) {
+                        M.raw = take(scr, n);
+                        M.tmp = take(scr, n);
+                        M.fin = take(keep, n);
+                    }
                     m2l_mats.push_back(M);
                     m2l_id[key] = gid;
                 } else {
@@ -804,6 +848,7 @@ void Session::build() {
                            cudaMemcpyDeviceToDevice, stream_));
     }
     for (auto& kv : m2m_mats) {
+        if (kv.second.cached) continue;
         double W = kv.first.first;
         const DirPts& dp = get_dir(W, kv.first.second);
         int rc, cc;
@@ -812,6 +857,7 @@ void Session::build() {
             add_job(dp.ucp, zero3, cp, shifted_point(ind, W), dp.r2, rc, dscr + kv.second.raw[ind]);
     }
     for (auto& kv : l2l_mats) {
+        if (kv.second.cached) continue;
         double W = kv.first.first;
         const DirPts& dp = get_dir(W, kv.first.second);
         int rc, cc;
@@ -820,7 +866,7 @@ void Session::build() {
             add_job(cp, shifted_point(ind, W), dp.dep, zero3, rc, dp.r2, dscr + kv.second.raw[ind]);
     }
     for (const M2LMat& M : m2l_mats)
-        add_job(hfcanon[M.canon].neg_uep, M.shift, hfcanon[M.canon].uep, zero3, M.r1, M.r1, dscr + M.raw);
+        if (!M.pk) add_job(hfcanon[M.canon].neg_uep, M.shift, hfcanon[M.canon].uep, zero3, M.r1, M.r1, dscr + M.raw);
 
     // generate every kernel matrix now
     if (!jobs.empty()) {
@@ -835,7 +881,7 @@ void Session::build() {
         GemmBatch right_s, right_k, left;
         for (auto& kv : m2m_mats) {
             const DirMats& M = kv.second;
-            for (int ind = 0; ind < 8; ++ind) {
+            for (int ind = 0; ind < 8 && !M.cached; ++ind) {
                 if (M.ccanon >= 0) {  // tmp = ue2uc * E1(child)
                     right_s.product(dscr + M.raw[ind], M.mrows, M.mcols, scr_E1[M.ccanon], M.mcols, M.tmp[ind]);
                     left.product(hfcanon[M.canon].E3, M.mrows, M.mrows, M.tmp[ind], M.mcols, M.fin[ind]);
@@ -846,7 +892,7 @@ void Session::build() {
         }
         for (auto& kv : l2l_mats) {
             const DirMats& M = kv.second;
-            for (int ind = 0; ind < 8; ++ind) {
+            for (int ind = 0; ind < 8 && !M.cached; ++ind) {
                 if (M.ccanon >= 0) {  // tmp = de2dc * E3^T ; fin = E1(child)^T * tmp
                     right_s.product(dscr + M.raw[ind], M.mrows, M.mcols, scr_E3t[M.canon], M.mcols, M.tmp[ind]);
                     left.product(hfcanon[M.ccanon].E1t, M.mrows, M.mrows, M.tmp[ind], M.mcols, M.fin[ind]);
@@ -856,6 +902,7 @@ void Session::build() {
             }
         }
         for (const M2LMat& M : m2l_mats) {
+            if (M.pk) continue;
             right_s.product(dscr + M.raw, M.r1, M.r1, scr_E1[M.canon], M.r1, M.tmp);
             left.product(hfcanon[M.canon].E1t, M.r1, M.r1, M.tmp, M.r1, M.fin);
         }
@@ -966,7 +1013,12 @@ void Session::build() {
                     const DirMats& M = m2m_mats.at(std::make_pair(W, u.dir));
                     p = (int)probs.size();
                     pid[u.dir] = p;
-                    probs.push_back(GemmProblem{KP(M.fin[ind]), M.mrows, M.mcols, M.mrows, 0, 0});
+                    if (M.cached) {
+                        probs.push_back(GemmProblem{nullptr, M.mrows, M.mcols, M.mrows, 0, 0, M.pk[ind]});
+                    } else {
+                        probs.push_back(GemmProblem{KP(M.fin[ind]), M.mrows, M.mcols, M.mrows, 0, 0});
+                        if (!opctx_.empty()) opkey_[KP(M.fin[ind])] = opk("m2m", W, u.dir, ind);
+                    }
                     xo.emplace_back();
                     yo.emplace_back();
                 } else {
@@ -989,7 +1041,14 @@ void Session::build() {
                 const Canon& c = hfcanon[u.canon];
                 p = (int)p2.size();
                 cp[u.canon] = p;
-                p2.push_back(GemmProblem{opm(c.E2, (size_t)c.r1 * c.r2), c.r1, c.r2, c.r1, 0, 0});
+                const std::string k = opk("e2", c.W, c.srt, 0);
+                if (const float* pk = cached_op(k)) {
+                    p2.push_back(GemmProblem{nullptr, c.r1, c.r2, c.r1, 0, 0, pk});
+                } else {
+                    const double2* a = opm(c.E2, (size_t)c.r1 * c.r2);
+                    p2.push_back(GemmProblem{a, c.r1, c.r2, c.r1, 0, 0});
+                    if (!opctx_.empty()) opkey_[a] = k;
+                }
                 xa.emplace_back();
                 ya.emplace_back();
             } else {
@@ -1014,7 +1073,12 @@ void Session::build() {
             std::vector<GemmProblem> probs;
             for (int gid : m2l_probs[level]) {
                 const M2LMat& M = m2l_mats[gid];
-                probs.push_back(GemmProblem{KP(M.fin), M.r1, M.r1, M.r1, 0, 0});
+                if (M.pk) {
+                    probs.push_back(GemmProblem{nullptr, M.r1, M.r1, M.r1, 0, 0, M.pk});
+                } else {
+                    probs.push_back(GemmProblem{KP(M.fin), M.r1, M.r1, M.r1, 0, 0});
+                    if (!opctx_.empty()) opkey_[KP(M.fin)] = M.key;
+                }
             }
             add_gemm(probs, m2l_x[level], m2l_y[level], hf_upeq, hf_dnchk, GEMM_ATOMIC, width_label("hf_m2l", W));
         }
@@ -1030,7 +1094,14 @@ void Session::build() {
                 const Canon& c = hfcanon[d.canon];
                 p = (int)p2.size();
                 cp[d.canon] = p;
-                p2.push_back(GemmProblem{opm(c.E2t, (size_t)c.r1 * c.r2), c.r2, c.r1, c.r2, 0, 0});
+                const std::string k = opk("e2t", c.W, c.srt, 0);
+                if (const float* pk = cached_op(k)) {
+                    p2.push_back(GemmProblem{nullptr, c.r2, c.r1, c.r2, 0, 0, pk});
+                } else {
+                    const double2* a = opm(c.E2t, (size_t)c.r1 * c.r2);
+                    p2.push_back(GemmProblem{a, c.r2, c.r1, c.r2, 0, 0});
+                    if (!opctx_.empty()) opkey_[a] = k;
+                }
                 xa.emplace_back();
                 xt.emplace_back();
             } else {
@@ -1063,7 +1134,12 @@ void Session::build() {
                     const DirMats& M = l2l_mats.at(std::make_pair(W, d.dir));
                     p = (int)probs.size();
                     pid[d.dir] = p;
-                    probs.push_back(GemmProblem{KP(M.fin[ind]), M.mrows, M.mcols, M.mrows, 0, 0});
+                    if (M.cached) {
+                        probs.push_back(GemmProblem{nullptr, M.mrows, M.mcols, M.mrows, 0, 0, M.pk[ind]});
+                    } else {
+                        probs.push_back(GemmProblem{KP(M.fin[ind]), M.mrows, M.mcols, M.mrows, 0, 0});
+                        if (!opctx_.empty()) opkey_[KP(M.fin[ind])] = opk("l2l", W, d.dir, ind);
+                    }
                     xo.emplace_back();
                     yo.emplace_back();
                 } else {

@@ -9,7 +9,10 @@
 #include <string>
 #include <vector>
 
+#include <memory>
+
 #include "kernels.cuh"
+#include "opcache.hpp"
 #include "ops.hpp"
 #include "tree.hpp"
 
@@ -75,6 +78,9 @@ public:
     void profile_reset() { prof_.clear(); }
     int npts() const { return npts_; }
     int device() const { return prm_.device; }
+    // device bytes of the packed-operator chunks this session created (part of
+    // stats().device_bytes; other sessions may share them)
+    size_t chunk_bytes() const { return chunk_bytes_; }
     cudaStream_t stream() const { return stream_; }
 
 private:
@@ -181,8 +187,18 @@ private:
     int* d_err_ = nullptr;  // set by a tensor-core GEMM that timed out
     std::map<std::pair<const void*, long long>, const float*> packed_;  // (operator, m k) -> packed copy
     std::vector<UmmaPackJob> pack_jobs_;                                 // packing still to launch
-    float* arena_ = nullptr;  // current chunk for packed operators
-    size_t arena_left_ = 0;   // floats left in it
+    // packed operators (tcgen05 form): the chunk being filled, the operators this
+    // session uses (its own and shared ones), and those it created but has not yet
+    // published to the process-wide cache (they are, once their packing completed)
+    std::string ld_path_, hd_path_, opctx_;
+    std::shared_ptr<DevChunk> chunk_;
+    float* chunk_pos_ = nullptr;
+    size_t chunk_left_ = 0;   // floats
+    size_t chunk_bytes_ = 0;  // bytes of the chunks this session created
+    std::vector<std::shared_ptr<PackedOp> > held_;
+    std::map<const void*, std::string> opkey_;  // operator (FP32 copy) -> cache key
+    std::vector<std::pair<std::string, std::shared_ptr<PackedOp> > > to_publish_;
+    const float* cached_op(const std::string& key);
     size_t spectra_elems_ = 0;
     bool profiling_ = false;
     std::vector<cudaEvent_t> ev_;
