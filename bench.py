@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--profile-json", default=None, help="write the per-pass profile here")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form measurement")
     ap.add_argument("--no-served", action="store_true", help="skip the continuous-batching server measurement")
+    ap.add_argument("--batched", action="store_true",
+                    help="also measure 64 uneven instances evaluated as one batch (about two minutes of setup)")
     ap.add_argument("--mixed-mma-sync", action="store_true",
                     help="also measure the mixed form with its translations on the mma.sync path")
     return ap.parse_args()
@@ -250,18 +252,23 @@ def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws, profile_json=None, 
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))}}
 
 
-def served_workloads():
-    """The served mix: the bench sphere (K=64) plus smaller spheres and
-    ellipsoids (K = 16, 8, 4; N = 25 pi K^2 points each), all P=6, seeded."""
+def instance_mix(Ks, seed0):
+    """Spheres and ellipsoids (alternating) of the given K, N = 25 pi K^2 points,
+    P=6, seeded: the instances of the batched and served configurations."""
     from ddfmm_b200 import geometry, workloads as wl
-    out = [wl.LARGE]
-    seed = 1
-    for K, count in ((16, 2), (8, 6), (4, 7)):
-        for j in range(count):
-            n = geometry.sphere_n_for(K)
-            out.append(wl.sphere(K, n, accu=2, seed=seed) if j % 2 == 0 else wl.ellipsoid(K, n, accu=2, seed=seed))
-            seed += 1
+    out = []
+    for j, K in enumerate(Ks):
+        n = geometry.sphere_n_for(K)
+        seed = seed0 + j
+        out.append(wl.sphere(K, n, accu=2, seed=seed) if j % 2 == 0 else wl.ellipsoid(K, n, accu=2, seed=seed))
     return out
+
+
+def served_workloads():
+    """16 sessions: the bench sphere (K=64, N=321,699) and 15 spheres /
+    ellipsoids with K cycling over 8, 16, 32, 64."""
+    from ddfmm_b200 import workloads as wl
+    return [wl.LARGE] + instance_mix([(8, 16, 32, 64)[j % 4] for j in range(15)], 1)
 
 
 def measure_served(large_plain_e2e_s, budget_gb=30.0, closed_s=4.0, poisson_s=4.0):
@@ -351,7 +358,8 @@ def measure_served(large_plain_e2e_s, budget_gb=30.0, closed_s=4.0, poisson_s=4.
     lat = np.array(lat) if lat else np.zeros(1)
     return {"sessions": len(live), "waiting": len(sids) - len(live), "budget_gb": budget_gb,
             "device_gb_used": used_gb, "admission_s": admit_s,
-            "mix": "K=64 sphere N=321699 + 2 x K=16, 6 x K=8, 7 x K=4 spheres/ellipsoids (N = 25 pi K^2), P=6",
+            "mix": "K=64 sphere N=321699 + 15 spheres/ellipsoids, K cycling 8, 16, 32, 64 (N = 25 pi K^2), P=6",
+            "admitted_K": sorted(int(w.K) for _, w in live),
             "saturated": {"value": closed_rate, "unit": "matvec/s", "mean_batch": cst["mean_batch"],
                           "p50_ms": cst["p50_ms"], "p99_ms": cst["p99_ms"]},
             "poisson": {"rate_per_s": lam, "requests": pst["requests"], "mean_batch": pst["mean_batch"],
@@ -363,6 +371,82 @@ def measure_served(large_plain_e2e_s, budget_gb=30.0, closed_s=4.0, poisson_s=4.
                                               "time in arrival order"},
             "speedup_saturated": closed_rate / plain_closed_rate,
             "io": "host complex64 arrays in and out of the server (pinned staging, H2D/D2H inside each request)"}
+
+
+def measure_batched(steps=5):
+    """64 independent instances (K drawn from 4, 8, 16, 32; spheres and
+    ellipsoids; N = 25 pi K^2; P=6) evaluated as one batch (merged
+    multi-instance launches, one CUDA graph) against the same instances one
+    after another, mixed and plain FP64; device-resident densities."""
+    import torch
+    from ddfmm_b200 import _lib, wave3d
+    rng = np.random.default_rng(64)
+    Ks = [int(k) for k in rng.choice([4, 8, 16, 32], 64)]
+    ws_list = instance_mix(Ks, 100)
+    t0 = time.perf_counter()
+    waves = [wave3d.from_workload(w, precision=_lib.MIXED) for w in ws_list]
+    setup_s = time.perf_counter() - t0
+    dev_gb = sum(wv.stats()["device_bytes"] for wv in waves) / 1e9
+    b = wave3d.Batch(waves)
+    dens = [torch.from_numpy(w.densities(np.complex64).view(np.float32)).cuda() for w in ws_list]
+    vals = [torch.empty_like(d) for d in dens]
+    dp = [d.data_ptr() for d in dens]
+    vp = [v.data_ptr() for v in vals]
+    st = torch.cuda.Stream()
+    for _ in range(3):
+        b.eval_device(dp, vp, st.cuda_stream)
+    st.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(st):
+        e0.record(st)
+    for _ in range(steps):
+        b.eval_device(dp, vp, st.cuda_stream)
+    with torch.cuda.stream(st):
+        e1.record(st)
+    st.synchronize()
+    batch_ms = e0.elapsed_time(e1) / steps
+    # one after another, mixed
+    for wv, d, v in zip(waves, dens, vals):
+        wv.eval_device(d.data_ptr(), v.data_ptr(), st.cuda_stream, c64=True)
+    st.synchronize()
+    with torch.cuda.stream(st):
+        e0.record(st)
+    for _ in range(steps):
+        for wv, d, v in zip(waves, dens, vals):
+            wv.eval_device(d.data_ptr(), v.data_ptr(), st.cuda_stream, c64=True)
+    with torch.cuda.stream(st):
+        e1.record(st)
+    st.synchronize()
+    seq_ms = e0.elapsed_time(e1) / steps
+    launches = b.launches()
+    b.close()
+    for wv in waves:
+        wv.close()
+    # one after another, plain FP64 (sessions created one at a time)
+    plain_ms = 0.0
+    for w in ws_list:
+        p = wave3d.from_workload(w, precision=_lib.PLAIN_FP64)
+        d = torch.from_numpy(w.densities().view(np.float64)).cuda()
+        v = torch.empty_like(d)
+        p.eval_device(d.data_ptr(), v.data_ptr(), st.cuda_stream)
+        st.synchronize()
+        with torch.cuda.stream(st):
+            e0.record(st)
+        for _ in range(steps):
+            p.eval_device(d.data_ptr(), v.data_ptr(), st.cuda_stream)
+        with torch.cuda.stream(st):
+            e1.record(st)
+        st.synchronize()
+        plain_ms += e0.elapsed_time(e1) / steps
+        p.close()
+    n = len(ws_list)
+    return {"instances": n, "K_counts": {str(k): Ks.count(k) for k in (4, 8, 16, 32)},
+            "points": int(sum(w.N for w in ws_list)), "setup_s": setup_s, "device_gb": dev_gb,
+            "launches_per_batch_matvec": launches,
+            "batched": {"value": n * 1e3 / batch_ms, "unit": "matvec/s", "ms_per_batch": batch_ms},
+            "mixed_one_by_one": {"value": n * 1e3 / seq_ms, "unit": "matvec/s", "ms_per_round": seq_ms},
+            "plain_fp64_one_by_one": {"value": n * 1e3 / plain_ms, "unit": "matvec/s", "ms_per_round": plain_ms},
+            "speedup_vs_plain": plain_ms / batch_ms, "speedup_vs_mixed_one_by_one": seq_ms / batch_ms}
 
 
 def run_ours(args):
@@ -485,6 +569,7 @@ def run_ours(args):
     served = None
     if not args.no_served and ws == 1 and args.workload == "large":
         served = measure_served(e2e_s)
+    batched = measure_batched() if args.batched and ws == 1 else None
     mixed_mma = None
     if args.mixed_mma_sync:
         from ddfmm_b200 import _lib
@@ -511,6 +596,8 @@ def run_ours(args):
             line["mixed_form_mma_sync"] = mixed_mma
         if served:
             line["served"] = served
+        if batched:
+            line["batched"] = batched
         print(json.dumps(line), flush=True)
     wave.close()
     if ws > 1:
