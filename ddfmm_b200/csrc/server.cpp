@@ -310,6 +310,22 @@ void Server::serving_loop() {
             changed_ = false;
         }
         if (!batch_) continue;
+        // gather window: sessions of the previous tick usually submit their next
+        // request right after its completion; wait briefly for the stragglers
+        {
+            const auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(300);
+            auto stragglers = [&] {
+                for (int sid : prev_tick_) {
+                    auto it = entries_.find(sid);
+                    if (it != entries_.end() && it->second->state == ADMITTED && !it->second->removing &&
+                        it->second->queue.empty())
+                        return true;
+                }
+                return false;
+            };
+            while (!stop_ && stragglers() && cv_work_.wait_until(lk, until) != std::cv_status::timeout) {
+            }
+        }
         // the tick: the oldest request of every session that has one
         std::vector<std::pair<int, Request> > tick;  // (slot, request)
         for (size_t i = 0; i < slots_.size(); ++i) {
@@ -320,6 +336,8 @@ void Server::serving_loop() {
             }
         }
         if (tick.empty()) continue;
+        prev_tick_.clear();
+        for (auto& tr : tick) prev_tick_.push_back(slots_[tr.first]);
         std::vector<Entry*> ent(slots_.size(), nullptr);
         for (size_t i = 0; i < slots_.size(); ++i) ent[i] = entries_[slots_[i]].get();
         lk.unlock();

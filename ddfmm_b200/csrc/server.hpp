@@ -8,7 +8,10 @@
 // the tick's sessions in the same merged launches), copies the values out and
 // completes the requests.  Requests that arrive during a tick are taken by
 // the next one, so work of sessions that become busy at different times
-// shares the device as soon as the current tick ends.
+// shares the device as soon as the current tick ends.  Before a tick the
+// serving thread waits up to 0.3 ms for sessions of the previous tick that
+// have not yet sent their next request (a client typically answers a
+// completion with a new request within microseconds).
 //
 // Admission: add_session queues a session; an admission thread creates it
 // (tree, operators, device buffers: seconds for large ones, off the serving
@@ -107,6 +110,7 @@ private:
     bool changed_ = false;        // admitted set changed since the batch was built
     bool blocked_ = false;        // the head of the waiting queue did not fit
     std::vector<int> slots_;      // batch instance -> sid
+    std::vector<int> prev_tick_;  // sessions of the last tick
     std::unique_ptr<Batch> batch_;
     cudaStream_t stream_ = nullptr;
     int* d_active_ = nullptr;
