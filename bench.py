@@ -56,6 +56,22 @@ def workload(name):
     return {"large": wl.LARGE, "medium": wl.MEDIUM, "small": wl.SMALL}[name]
 
 
+def max_over_ranks(x, ws, dev=None):
+    """The largest value of x over all ranks; every rank calls it (a collective)."""
+    if ws == 1:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(ms_per_step, ws):
+    """matvec/s of the whole job: every rank evaluates its own instance (a
+    replica) in each step, and a step lasts as long as the slowest rank's."""
+    return ws * 1e3 / ms_per_step
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -239,14 +255,10 @@ def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws, profile_json=None, 
         json.dump({k: dict(v, ms_per_step=v["ms"] / steps) for k, v in prof.items()}, open(profile_json, "w"),
                   indent=1)
     lat = np.array([a.elapsed_time(b) for a, b in ev])
-    ms = ev[0][0].elapsed_time(ev[-1][1]) / steps
-    if ws > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev[0][0].elapsed_time(ev[-1][1]) / steps, ws, dev)
     m.close()
     gemm = "tcgen05" if precision == _lib.MIXED else "mma.sync"
-    return {"value": ws * 1e3 / ms, "unit": "matvec/s", "ms_per_step": ms,
+    return {"value": whole_job_rate(ms, ws), "unit": "matvec/s", "ms_per_step": ms,
             "dtype": "c64 (3xTF32 translations on %s)" % gemm,
             "relerr_vs_fp64_direct": relerr, "setup_s": setup_s,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))}}
@@ -502,12 +514,8 @@ def run_ours(args):
         torch.distributed.barrier()
     lat = np.array([a.elapsed_time(b) for a, b in ev])
     total_ms = ev[0][0].elapsed_time(ev[-1][1])
-    ms_per_step = total_ms / args.steps
-    if ws > 1:
-        t = torch.tensor([ms_per_step], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_per_step = float(t.item())
-    value = ws * 1e3 / ms_per_step  # whole-job matvecs / s (every rank runs its own instance)
+    ms_per_step = max_over_ranks(total_ms / args.steps, ws, dev)
+    value = whole_job_rate(ms_per_step, ws)
     # end to end through the public API with pinned host buffers ---------------
     den_h = torch.from_numpy(np.ascontiguousarray(den).view(np.float64)).pin_memory()
     val_h = torch.empty(2 * w.N, dtype=torch.float64).pin_memory()
@@ -520,11 +528,7 @@ def run_ours(args):
     t1 = time.perf_counter()
     for _ in range(e2e_steps):
         wave.eval(dh, vh)
-    e2e_s = (time.perf_counter() - t1) / e2e_steps
-    if ws > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t1) / e2e_steps, ws, dev)
     e2e_relerr = float(np.linalg.norm(vh - val0) / np.linalg.norm(val0))
     # roofline of the dominant kernel -------------------------------------------
     by_kernel = {}
@@ -588,7 +592,7 @@ def run_ours(args):
                            "kernel": "exp(ir)/r", "npq": w.npq, "ptsmax": w.ptsmax, "form": "plain FP64",
                            "l2": "inputs larger than L2 (device working set %.1f GB)" % (st["device_bytes"] / 1e9),
                            "parallelism": "replicas" if ws > 1 else "single GPU", "setup_s": setup_s},
-                "e2e": {"value": 1.0 / e2e_s, "unit": "matvec/s", "h2d_bytes_per_step": 16 * w.N,
+                "e2e": {"value": whole_job_rate(1e3 * e2e_s, ws), "unit": "matvec/s", "h2d_bytes_per_step": 16 * w.N,
                         "d2h_bytes_per_step": 16 * w.N, "rel_diff_vs_device_path": e2e_relerr},
                 "roofline": roof, "gpu_launches": int(round(launches / args.steps)) * args.steps,
                 "clocks": clocks, "cpu_baseline": cpu, "mixed_form": mixed, "passes": passes}
