@@ -106,6 +106,11 @@ Batch::Batch(const std::vector<Session*>& sessions) : sessions_(sessions) {
                     n.push_back(u.nitems);
                 }
                 add(PT, subs, n);
+                if (!launches_.empty() && launches_.back().kind == PT) {
+                    int tpi = 4;  // the widest shape any of the merged steps was tuned to
+                    for (auto& e : kk.second) tpi = std::max(tpi, e.second->tpi ? e.second->tpi : 32);
+                    launches_.back().tpi = tpi;
+                }
             } else if (kind == 2 || kind == 3) {
                 // V-list launches are templated on the grid size: one launch per G
                 std::map<int, std::vector<std::pair<int, const Session::Step*> > > by_g;
@@ -190,7 +195,7 @@ void Batch::run(const int* active, cudaStream_t s) {
                 break;
             case PT:
                 launch_pt32(static_cast<const PtSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub, (int)L.total,
-                            active, s);
+                            active, s, L.tpi);
                 break;
             case VFWD:
                 launch_vlist_forward32(static_cast<const VfSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub,

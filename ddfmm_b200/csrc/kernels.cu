@@ -216,12 +216,15 @@ void launch_gemm(const GemmProblem* probs, const GemmTile* tiles, int ntiles, co
 
 // ---------------------------------------------------------------- points
 // One warp per item; lanes over the item's target points.
+// TPI consecutive threads per item, striding over its targets (TPI = 32: a
+// warp per item, for items with many targets; 4 or 8 for leaf-sized ones).
+template <int TPI>
 __global__ void pt_kernel(const PtItem* __restrict__ items, int nitems, const PtSrc* __restrict__ srcs,
                           int kernel) {
-    int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) / TPI, lane = threadIdx.x % TPI;
     if (w >= nitems) return;
     const PtItem it = items[w];
-    for (int t = lane; t < it.trg.n; t += 32) {
+    for (int t = lane; t < it.trg.n; t += TPI) {
         const double* tp = it.trg.x + 3 * t;
         double tx = it.trg.scale * tp[0] + it.trg.shift[0];
         double ty = it.trg.scale * tp[1] + it.trg.shift[1];
@@ -244,10 +247,15 @@ __global__ void pt_kernel(const PtItem* __restrict__ items, int nitems, const Pt
     }
 }
 
-void launch_pt(const PtItem* items, int nitems, const PtSrc* srcs, int kernel, cudaStream_t s) {
+void launch_pt(const PtItem* items, int nitems, const PtSrc* srcs, int kernel, cudaStream_t s, int tpi) {
     if (nitems == 0) return;
-    int blocks = (nitems * 32 + 255) / 256;
-    pt_kernel<<<blocks, 256, 0, s>>>(items, nitems, srcs, kernel);
+    const int blocks = (int)(((long long)nitems * tpi + 255) / 256);
+    switch (tpi) {
+        case 4: pt_kernel<4><<<blocks, 256, 0, s>>>(items, nitems, srcs, kernel); break;
+        case 8: pt_kernel<8><<<blocks, 256, 0, s>>>(items, nitems, srcs, kernel); break;
+        case 16: pt_kernel<16><<<blocks, 256, 0, s>>>(items, nitems, srcs, kernel); break;
+        default: pt_kernel<32><<<blocks, 256, 0, s>>>(items, nitems, srcs, kernel); break;
+    }
 }
 
 // ---------------------------------------------------------------- V list

@@ -62,7 +62,8 @@ void launch_kmat(const KmatJob* jobs_dev, int njobs, long long total, int kernel
 void launch_gemm(const GemmProblem* probs_dev, const GemmTile* tiles_dev, int ntiles,
                  const long long* xoff, const long long* yoff, const double2* X, double2* Y, int mode,
                  cudaStream_t s);
-void launch_pt(const PtItem* items_dev, int nitems, const PtSrc* srcs_dev, int kernel, cudaStream_t s);
+// tpi: threads per item (4, 8, 16 or 32), chosen per launch by the session's autotuner
+void launch_pt(const PtItem* items_dev, int nitems, const PtSrc* srcs_dev, int kernel, cudaStream_t s, int tpi = 32);
 
 // FFT-based low-frequency M2L on a G^3 grid (G = 2P), see kernels.cu.
 struct VlistLevel {
@@ -134,7 +135,8 @@ struct ZeroSub {
     int inst;
     int pad;
 };
-void launch_pt32(const PtSub* subs, const int* prefix, int nsub, int nitems, const int* active, cudaStream_t s);
+void launch_pt32(const PtSub* subs, const int* prefix, int nsub, int nitems, const int* active, cudaStream_t s,
+                 int tpi = 32);
 void vlist32_init(int G);
 // A launch with nsub == 1 passes its sub-launch as `one` (host copy, sent as
 // a kernel parameter); `subs` / `prefix` are then not read.

@@ -243,16 +243,17 @@ __device__ __forceinline__ int find_sub(const T* __restrict__ prefix, int nsub, 
 // One warp per item as pt_kernel; densities / outputs are float2 (the
 // descriptors' double2 pointers are reinterpreted).  Differences of the FP64
 // coordinates are taken in FP64, the kernel is evaluated in FP32.
+template <int TPI>
 __global__ void pt32_kernel(const PtSub* __restrict__ subs, const int* __restrict__ prefix, int nsub, int nitems,
                             const int* __restrict__ active) {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) / TPI, lane = threadIdx.x % TPI;
     if (w >= nitems) return;
     const int j = find_sub(prefix, nsub, w);
     const PtSub S = subs[j];
     if (active && !active[S.inst]) return;
     const PtItem it = S.items[w - prefix[j]];
     float2* out = reinterpret_cast<float2*>(it.out);
-    for (int t = lane; t < it.trg.n; t += 32) {
+    for (int t = lane; t < it.trg.n; t += TPI) {
         const double* tp = it.trg.x + 3 * t;
         double tx = it.trg.scale * tp[0] + it.trg.shift[0];
         double ty = it.trg.scale * tp[1] + it.trg.shift[1];
@@ -274,9 +275,16 @@ __global__ void pt32_kernel(const PtSub* __restrict__ subs, const int* __restric
     }
 }
 
-void launch_pt32(const PtSub* subs, const int* prefix, int nsub, int nitems, const int* active, cudaStream_t s) {
+void launch_pt32(const PtSub* subs, const int* prefix, int nsub, int nitems, const int* active, cudaStream_t s,
+                 int tpi) {
     if (nitems == 0) return;
-    pt32_kernel<<<(nitems * 32 + 255) / 256, 256, 0, s>>>(subs, prefix, nsub, nitems, active);
+    const int blocks = (int)(((long long)nitems * tpi + 255) / 256);
+    switch (tpi) {
+        case 4: pt32_kernel<4><<<blocks, 256, 0, s>>>(subs, prefix, nsub, nitems, active); break;
+        case 8: pt32_kernel<8><<<blocks, 256, 0, s>>>(subs, prefix, nsub, nitems, active); break;
+        case 16: pt32_kernel<16><<<blocks, 256, 0, s>>>(subs, prefix, nsub, nitems, active); break;
+        default: pt32_kernel<32><<<blocks, 256, 0, s>>>(subs, prefix, nsub, nitems, active); break;
+    }
 }
 
 // ---------------------------------------------------------------- V list (FP32)

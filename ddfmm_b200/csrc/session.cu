@@ -80,6 +80,7 @@ Session::Session(const double* pos3n, int n, const SessionParams& p, const std::
     ops_.load(ld_path, hd_path);
     tree_.build(pos_.data(), n, p.tree);
     build();
+    autotune();
     CK(cudaStreamSynchronize(stream_));
     stats_.setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -1376,9 +1377,9 @@ void Session::launch_step(const Step& st, cudaStream_t s, double2* spec) {
             break;
         case 1:
             if (m)
-                launch_pt32(static_cast<const PtSub*>(st.msubs), st.mpre, 1, st.mtotal, nullptr, s);
+                launch_pt32(static_cast<const PtSub*>(st.msubs), st.mpre, 1, st.mtotal, nullptr, s, st.tpi ? st.tpi : 32);
             else
-                launch_pt(st.pt.items, st.pt.nitems, st.pt.srcs, prm_.kernel, s);
+                launch_pt(st.pt.items, st.pt.nitems, st.pt.srcs, prm_.kernel, s, st.tpi ? st.tpi : 32);
             break;
         case 2:
             if (m)
@@ -1401,6 +1402,38 @@ void Session::launch_step(const Step& st, cudaStream_t s, double2* spec) {
             launch_umma_cgemm(static_cast<const UmmaSub*>(st.msubs), st.mpre, 1, st.mtotal, nullptr, d_err_, s, &st.hu);
             break;
     }
+}
+
+// The accumulators a point-interaction step writes are zeroed at the start of
+// every eval, so running it here on setup-time contents is harmless.
+void Session::autotune() {
+    cudaEvent_t a = nullptr, b = nullptr;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    for (Step& st : steps_) {
+        if (st.kind != 1) continue;
+        float best = 0.f;
+        int best_tpi = 32;
+        for (int tpi : {32, 16, 8, 4}) {
+            st.tpi = tpi;
+            launch_step(st, stream_, st.v.spec);  // warm-up
+            CK(cudaEventRecord(a, stream_));
+            for (int r = 0; r < 3; ++r) launch_step(st, stream_, st.v.spec);
+            CK(cudaEventRecord(b, stream_));
+            CK(cudaEventSynchronize(b));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, a, b));
+            if (tpi == 32 || ms < best) {
+                best = ms;
+                best_tpi = tpi;
+            }
+        }
+        st.tpi = best_tpi;
+        stats_.tuned_steps++;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CK(cudaGetLastError());
 }
 
 void Session::run_steps(cudaStream_t s) {

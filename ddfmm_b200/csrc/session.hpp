@@ -35,6 +35,7 @@ struct SessionStats {
     long long fft_spectra_bytes = 0;
     double setup_seconds = 0;
     size_t device_bytes = 0;
+    int tuned_steps = 0;  // steps whose launch shape the autotuner chose
 };
 
 class Session {
@@ -130,6 +131,7 @@ private:
         // that play the same part (phase, width, step type, occurrence): a Batch
         // merges the steps of its sessions that share a key into one launch.
         long long key;
+        int tpi;  // point interactions: threads per item (0 = 32), set by autotune()
         // mixed form: the step as a one-instance launch (device sub-launch array and
         // prefix sums) and the host copy of its sub-launch
         void* msubs;
@@ -160,6 +162,9 @@ private:
     void begin_block(int phase, double W);
     void push_step(Step st);
     void build();
+    // Times the launch-shape variants of each step on this session's own data
+    // and keeps the fastest (point interactions: threads per item).
+    void autotune();
     void run_steps(cudaStream_t s);
     void run_steps_spec(cudaStream_t s, double2* spec);
     void launch_step(const Step& st, cudaStream_t s, double2* spec);
