@@ -47,8 +47,8 @@ def parse():
     ap.add_argument("--batched", action="store_true",
                     help="also measure 64 uneven instances evaluated as one batch (about two minutes of setup)")
     ap.add_argument("--ellipsoid-table", default=None,
-                    help="only tabulate the mixed form on the K=128 ellipsoid (N=900k) for the given ACCU "
-                         "levels and kernels, e.g. '1,2:0,1'")
+                    help="only tabulate the mixed form on the ellipsoid (K=128, N=900k by default) for the given "
+                         "ACCU levels and kernels, optionally K, e.g. '1,2:0,1' or '1,2,3:0:64'")
     ap.add_argument("--mixed-mma-sync", action="store_true",
                     help="also measure the mixed form with its translations on the mma.sync path")
     return ap.parse_args()
@@ -492,17 +492,18 @@ def measure_batched(steps=5):
             "speedup_vs_plain": plain_ms / batch_ms, "speedup_vs_mixed_one_by_one": seq_ms / batch_ms}
 
 
-def ellipsoid_table(accus, kernels, steps=3):
-    """The mixed form on the ellipsoid (semi-axes 0.5, 0.25, 0.125 of a root box
-    of K=128 wavelengths, N = 900,000 uniform by area, complex64 N(0,1)
-    densities) for each kernel and accuracy level: matvec/s and the relative
+def ellipsoid_table(accus, kernels, K=128, steps=3):
+    """The mixed form on the ellipsoid with semi-axes 0.5, 0.25, 0.125 of a root
+    box of K wavelengths (K=128: N = 900,000 uniform by area, 55 points per
+    square wavelength; other K at the same density), complex64 N(0,1)
+    densities, for each kernel and accuracy level: matvec/s and the relative
     error against the FP64 direct sum at 200 seeded targets."""
     import torch
     from ddfmm_b200 import _lib, wave3d, workloads as wl
     rows = []
     for kernel in kernels:
         for accu in accus:
-            w = wl.ellipsoid(128, 900000, accu=accu, kernel=kernel)
+            w = wl.ellipsoid(K, int(round(900000 * (K / 128.0) ** 2)), accu=accu, kernel=kernel)
             t0 = time.perf_counter()
             w.operators()
             ops_s = time.perf_counter() - t0
@@ -527,7 +528,7 @@ def ellipsoid_table(accus, kernels, steps=3):
             st.synchronize()
             ms = e0.elapsed_time(e1) / steps
             stt = m.stats()
-            rows.append({"kernel": "exp(ir)/r" if kernel == 0 else "exp(ir)", "ACCU": accu, "P": w.P, "N": w.N,
+            rows.append({"kernel": "exp(ir)/r" if kernel == 0 else "exp(ir)", "ACCU": accu, "P": w.P, "K": K, "N": w.N,
                          "relerr_vs_fp64_direct": relerr, "ms_per_matvec": ms, "matvec_per_s": 1e3 / ms,
                          "setup_s": setup_s, "operator_files_s": ops_s, "device_gb": stt["device_bytes"] / 1e9})
             m.close()
@@ -685,10 +686,12 @@ def run_ours(args):
 def main():
     args = parse()
     if args.ellipsoid_table:
-        a, k = args.ellipsoid_table.split(":")
-        rows = ellipsoid_table([int(x) for x in a.split(",")], [int(x) for x in k.split(",")])
-        print(json.dumps({"ellipsoid_table": rows, "config": "ellipsoid semi-axes 0.5/0.25/0.125 K, K=128, "
-                          "N=900000, NPQ 4, ptsmax 100, mixed form, complex64 N(0,1) densities, 200 check targets"}))
+        parts = args.ellipsoid_table.split(":")
+        K = int(parts[2]) if len(parts) > 2 else 128
+        rows = ellipsoid_table([int(x) for x in parts[0].split(",")], [int(x) for x in parts[1].split(",")], K)
+        print(json.dumps({"ellipsoid_table": rows, "config": "ellipsoid semi-axes 0.5/0.25/0.125 K, K=%d, "
+                          "55 points per square wavelength, NPQ 4, ptsmax 100, mixed form, complex64 N(0,1) "
+                          "densities, 200 check targets" % K}))
         return
     if args.impl == "reference":
         run_reference(args)

@@ -33,7 +33,8 @@
 //   W_MMA      one thread: per tile waits until its accumulator is drained
 //              (tmem_empty), then per block waits full[s], issues the three
 //              MMAs, commits to empty[s]; after the tile commits tmem_full.
-//   W_EPI..+3  epilogue, warp w on TMEM lanes 32 (w % 4) ..: TMEM -> a parking
+//   W_EPI..    epilogue, UEPI groups of 4 warps: warp w on TMEM lanes 32 (w % 4) ..,
+//              its group on every UEPI-th 64-column chunk: TMEM -> a parking
 //              area -> global, one column at a time in 256-byte coalesced
 //              rows; then arrive on tmem_empty.
 // Every mbarrier wait is bounded (1 s, or sooner once another role failed):
@@ -74,16 +75,20 @@ constexpr int UPREF = DDFMM_UMMA_PREF;      // gathered-column blocks prefetched
 #endif
 constexpr int UPSETS = DDFMM_UMMA_PSETS;     // producer sets (4 warps each), alternating K blocks
 constexpr bool UELECT = DDFMM_UMMA_ELECT;    // one mbarrier arrival per warp instead of per thread
+#ifndef DDFMM_UMMA_EPI
+#define DDFMM_UMMA_EPI 1
+#endif
+constexpr int UEPI = DDFMM_UMMA_EPI;  // epilogue groups of 4 warps (split an accumulator's columns)
 constexpr int W_LOAD_B = 4 * UPSETS, W_MMA = W_LOAD_B + 1, W_EPI = W_LOAD_B + 2;  // warp roles
-constexpr int UTHREADS = 32 * (W_EPI + 4);
+constexpr int UTHREADS = 32 * (W_EPI + 4 * UEPI);
 constexpr int U_FULL_COUNT = (UELECT ? 4 : UM) + 1;  // producer arrivals + the operator loader's
-constexpr int U_EMPTY_ACC_COUNT = UELECT ? 4 : UM;   // epilogue arrivals
+constexpr int U_EMPTY_ACC_COUNT = (UELECT ? 4 : UM) * UEPI;  // epilogue arrivals
 constexpr int U_A_BYTES = UM * UBK * 4;
 constexpr int U_B_BYTES = UNMAX * UBK * 4;
 constexpr int U_STAGE_BYTES = 2 * U_A_BYTES + 2 * U_B_BYTES;
 constexpr int PCH = DDFMM_UMMA_PCH;  // epilogue chunk: complex rows parked per column
 static_assert(PCH == 16 || PCH == 32, "epilogue chunk of 16 or 32 rows");
-constexpr int U_PARK_BYTES = 4 * 32 * (PCH + 1) * 8;  // 32 columns x PCH complex (+1 pad) per warp
+constexpr int U_PARK_BYTES = 4 * UEPI * 32 * (PCH + 1) * 8;  // 32 columns x PCH complex (+1 pad) per warp
 // ring + parking area + alignment slack: one block per SM (also what the 512
 // TMEM columns need)
 constexpr int UGEMM_SMEM = USTAGES * U_STAGE_BYTES + U_PARK_BYTES + 1024;
@@ -532,8 +537,19 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
         }
     } else {
         // ------------------------------------------------ epilogue
-        const int qw = warp & 3;  // TMEM lanes 32 qw .. 32 qw + 31 = tile columns
-        float2* park = park_all + qw * (32 * (PCH + 1));
+        const int ew = warp - W_EPI;  // group ew / 4 takes every UEPI-th chunk of accumulator columns
+        const int qw = warp & 3;      // TMEM lanes 32 qw .. 32 qw + 31 = tile columns
+        const int first = (ew >> 2) * 2 * PCH;
+        float2* park = park_all + ew * (32 * (PCH + 1));
+        auto release = [&](int acc) {  // this warp is done reading the accumulator
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+            if (UELECT) {
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tmem_empty[acc]);
+            } else {
+                mbar_arrive(&tmem_empty[acc]);
+            }
+        };
         int it = 0;
         for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
             const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, active, ti);
@@ -553,7 +569,8 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             const uint32_t src = tmem + ((uint32_t)(qw * 32) << 16) + (uint32_t)(acc * 256);
-            for (int c0 = 0; c0 < N; c0 += 2 * PCH) {
+            if (first >= N) release(acc);
+            for (int c0 = first; c0 < N; c0 += UEPI * 2 * PCH) {
 #pragma unroll
                 for (int h = 0; h < 2 * PCH; h += 16) {
                     if (c0 + h < N) {  // N is a multiple of 16
@@ -573,15 +590,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
                                 make_float2(__uint_as_float(v[2 * e]), __uint_as_float(v[2 * e + 1]));
                     }
                 }
-                if (c0 + 2 * PCH >= N) {  // accumulator fully read: hand it back to the MMA issuer
-                    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-                    if (UELECT) {
-                        __syncwarp();
-                        if (lane == 0) mbar_arrive(&tmem_empty[acc]);
-                    } else {
-                        mbar_arrive(&tmem_empty[acc]);
-                    }
-                }
+                if (c0 + UEPI * 2 * PCH >= N) release(acc);  // last chunk read: accumulator back to the MMA issuer
                 __syncwarp();
                 const int i = (c0 >> 1) + lane % PCH;  // complex row of this lane
                 if (mode == GEMM_SET)

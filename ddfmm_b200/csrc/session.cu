@@ -505,11 +505,18 @@ void Session::build() {
         L.r = op.up.m;
         L.uep = upload(op.uep.x);
         L.ucp = upload(op.ucp.x);
-        // fold the 1/sigma scaling into the rows of U^H (up) and of v^T
+        // fold the 1/sigma scaling into the rows of U^H (up) and of v^T.  The mixed
+        // form truncates the pseudo-inverse further, at sigma < 1e-7 sigma_max: FP32
+        // check values carry ~1e-7 relative noise, which the directions below that
+        // would amplify into equivalent densities whose norm swamps every later FP32
+        // translation (at P = 8 sigma spans 12 decades)
+        double smax = 0;
+        for (int i = 0; i < L.r; ++i) smax = std::max(smax, 1.0 / std::abs(op.is(i, 0)));
         std::vector<double2> up_s((size_t)L.r * nE), vT_s((size_t)L.r * nE);
         for (int i = 0; i < L.r; ++i)
             for (int j = 0; j < nE; ++j) {
                 cpx s = op.is(i, 0);
+                if (mixed && 1.0 / std::abs(s) < 1e-7 * smax) s = 0;
                 cpx a = s * op.up(i, j), b = s * op.v(j, i);
                 up_s[(size_t)j * L.r + i] = make_double2(a.real(), a.imag());
                 vT_s[(size_t)j * L.r + i] = make_double2(b.real(), b.imag());

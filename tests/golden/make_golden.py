@@ -34,6 +34,7 @@ CASES = {
     "cluster_k4_n1500_p4_helm_m8": wl.cluster(4, 1500, accu=1, ptsmax=8),
     "ellipsoid_k8_n3000_p4_helm": wl.ellipsoid(8, 3000, accu=1),
     "sphere_k16_n4000_p4_helm": wl.sphere(16, 4000, accu=1),
+    "sphere_k4_n1500_p8_helm": wl.sphere(4, 1500, accu=3),
 }
 
 
@@ -79,7 +80,8 @@ def make(name, w):
     r = run_ref.run_workload(w, chk=True)
     pos, den = w.points(), w.densities()
     ld = formats.read_ld(ld_path)
-    hd = formats.read_hd(hd_path)
+    # only the high-frequency widths this tree uses (the file may hold wider ones)
+    hd = {W: e for W, e in formats.read_hd(hd_path).items() if W <= w.wmax}
     widths = lf_widths(pos, w.K, w.ptsmax, w.maxlevel, w.nc)
     params = dict(K=w.K, accu=w.accu, kernel=w.kernel, ptsmax=w.ptsmax, maxlevel=w.maxlevel, nc=w.nc,
                   npq=w.npq, workload=w.name, ref_eval_s=r["eval_s"])
