@@ -48,7 +48,8 @@ def parse():
                     help="also measure 64 uneven instances evaluated as one batch (about two minutes of setup)")
     ap.add_argument("--ellipsoid-table", default=None,
                     help="only tabulate the mixed form on the ellipsoid (K=128, N=900k by default) for the given "
-                         "ACCU levels and kernels, optionally K, e.g. '1,2:0,1' or '1,2,3:0:64'")
+                         "ACCU levels and kernels, optionally K and the form (mixed or plain), e.g. '1,2:0,1' or "
+                         "'1,2,3:0:64:plain'")
     ap.add_argument("--mixed-mma-sync", action="store_true",
                     help="also measure the mixed form with its translations on the mma.sync path")
     return ap.parse_args()
@@ -492,7 +493,7 @@ def measure_batched(steps=5):
             "speedup_vs_plain": plain_ms / batch_ms, "speedup_vs_mixed_one_by_one": seq_ms / batch_ms}
 
 
-def ellipsoid_table(accus, kernels, K=128, steps=3):
+def ellipsoid_table(accus, kernels, K=128, steps=3, form="mixed"):
     """The mixed form on the ellipsoid with semi-axes 0.5, 0.25, 0.125 of a root
     box of K wavelengths (K=128: N = 900,000 uniform by area, 55 points per
     square wavelength; other K at the same density), complex64 N(0,1)
@@ -508,27 +509,29 @@ def ellipsoid_table(accus, kernels, K=128, steps=3):
             w.operators()
             ops_s = time.perf_counter() - t0
             t0 = time.perf_counter()
-            m = wave3d.from_workload(w, precision=_lib.MIXED)
+            mixed = form == "mixed"
+            m = wave3d.from_workload(w, precision=_lib.MIXED if mixed else _lib.PLAIN_FP64)
             setup_s = time.perf_counter() - t0
-            den = w.densities(np.complex64)
-            d = torch.from_numpy(den.view(np.float32)).cuda()
+            den = w.densities(np.complex64 if mixed else np.complex128)
+            d = torch.from_numpy(den.view(np.float32 if mixed else np.float64)).cuda()
             v = torch.empty_like(d)
             st = torch.cuda.Stream()
-            m.eval_device(d.data_ptr(), v.data_ptr(), st.cuda_stream, c64=True)
+            m.eval_device(d.data_ptr(), v.data_ptr(), st.cuda_stream, c64=mixed)
             st.synchronize()
-            val = v.cpu().numpy().view(np.complex64).astype(np.complex128)
+            val = v.cpu().numpy().view(np.complex64 if mixed else np.complex128).astype(np.complex128)
             relerr = m.check(den.astype(np.complex128), val, w.check_ids())
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             with torch.cuda.stream(st):
                 e0.record(st)
             for _ in range(steps):
-                m.eval_device(d.data_ptr(), v.data_ptr(), st.cuda_stream, c64=True)
+                m.eval_device(d.data_ptr(), v.data_ptr(), st.cuda_stream, c64=mixed)
             with torch.cuda.stream(st):
                 e1.record(st)
             st.synchronize()
             ms = e0.elapsed_time(e1) / steps
             stt = m.stats()
-            rows.append({"kernel": "exp(ir)/r" if kernel == 0 else "exp(ir)", "ACCU": accu, "P": w.P, "K": K, "N": w.N,
+            rows.append({"form": form, "kernel": "exp(ir)/r" if kernel == 0 else "exp(ir)", "ACCU": accu, "P": w.P,
+                         "K": K, "N": w.N,
                          "relerr_vs_fp64_direct": relerr, "ms_per_matvec": ms, "matvec_per_s": 1e3 / ms,
                          "setup_s": setup_s, "operator_files_s": ops_s, "device_gb": stt["device_bytes"] / 1e9})
             m.close()
@@ -688,7 +691,9 @@ def main():
     if args.ellipsoid_table:
         parts = args.ellipsoid_table.split(":")
         K = int(parts[2]) if len(parts) > 2 else 128
-        rows = ellipsoid_table([int(x) for x in parts[0].split(",")], [int(x) for x in parts[1].split(",")], K)
+        form = parts[3] if len(parts) > 3 else "mixed"
+        rows = ellipsoid_table([int(x) for x in parts[0].split(",")], [int(x) for x in parts[1].split(",")], K,
+                               form=form)
         print(json.dumps({"ellipsoid_table": rows, "config": "ellipsoid semi-axes 0.5/0.25/0.125 K, K=%d, "
                           "55 points per square wavelength, NPQ 4, ptsmax 100, mixed form, complex64 N(0,1) "
                           "densities, 200 check targets" % K}))
