@@ -311,9 +311,13 @@ void Server::serving_loop() {
         }
         if (!batch_) continue;
         // gather window: sessions of the previous tick usually submit their next
-        // request right after its completion; wait briefly for the stragglers
+        // request soon after its completion; wait for the stragglers up to 5% of
+        // the last tick's duration (0.3 to 5 ms)
         {
-            const auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(300);
+            const double win = std::min(5e-3, std::max(3e-4, 0.05 * last_tick_s_));
+            const auto until = std::chrono::steady_clock::now() +
+                               std::chrono::duration_cast<std::chrono::steady_clock::duration>(
+                                   std::chrono::duration<double>(win));
             auto stragglers = [&] {
                 for (int sid : prev_tick_) {
                     auto it = entries_.find(sid);
@@ -370,6 +374,7 @@ void Server::serving_loop() {
         }
         const double t1 = now();
         lk.lock();
+        last_tick_s_ = t1 - t0;
         ticks_++;
         reqs_in_ticks_ += (long long)tick.size();
         busy_s_ += t1 - t0;

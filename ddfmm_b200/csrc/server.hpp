@@ -9,9 +9,10 @@
 // completes the requests.  Requests that arrive during a tick are taken by
 // the next one, so work of sessions that become busy at different times
 // shares the device as soon as the current tick ends.  Before a tick the
-// serving thread waits up to 0.3 ms for sessions of the previous tick that
-// have not yet sent their next request (a client typically answers a
-// completion with a new request within microseconds).
+// serving thread waits briefly for sessions of the previous tick that have
+// not yet sent their next request (a client answers a completion with a new
+// request soon after, but client threads that share an interpreter lock take
+// turns): at most 5% of the last tick's duration, between 0.3 and 5 ms.
 //
 // Admission: add_session queues a session; an admission thread creates it
 // (tree, operators, device buffers: seconds for large ones, off the serving
@@ -118,6 +119,7 @@ private:
     std::vector<double> lat_ms_;
     long long ticks_ = 0, reqs_in_ticks_ = 0;
     double busy_s_ = 0;
+    double last_tick_s_ = 0;  // duration of the last tick (sizes the gather window)
     std::thread admit_thread_, serve_thread_;
 };
 
