@@ -383,17 +383,22 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
         // ------------------------------------------------ gathered columns
         // producer set `set` takes the blocks g = set, set + UPSETS, ... of the block
         // sequence of this block's tiles; within a set, warp cw covers columns 32cw ..
-        // 32cw + 31, load i columns 32cw + 8i .. +7, lane = (column, complex q); blocks
-        // are prefetched UPREF deep into registers and split into a ring slot once free
+        // 32cw + 31.  Lane bits: b0 = complex q & 1, b1..b3 = column & 7, b4 = bit 1
+        // of q, so each half-warp store fills one core matrix (8 columns x 16 B, all
+        // 32 banks once) and each column's load is 4 consecutive complex.  Load
+        // i = (column group cg = i / (CPB/4), q group jj = i % (CPB/4)) reads column
+        // 32cw + 8cg + (lane>>1 & 7), complex q = 4jj + 2 b4 + b0.  Blocks are
+        // prefetched UPREF deep into registers and split into a ring slot once free.
+        static_assert(CPB % 4 == 0, "the producer mapping needs 4 complex per column and load");
+        constexpr int QG = CPB / 4;  // q groups per block
         const int set = warp >> 2, cw = warp & 3;
-        // load i covers columns 32cw + i (32 / CPB) .., CPB lanes per column
-        const int q = lane % CPB;
-        int coff[CPB];  // core_off(column, 2q)
+        const int colw = cw * 32 + ((lane >> 1) & 7), qb = 2 * (lane >> 4) + (lane & 1);
+        int coff[CPB];  // core_off(column, 2q) of load i
 #pragma unroll
-        for (int i = 0; i < CPB; ++i) coff[i] = core_off(cw * 32 + i * (32 / CPB) + lane / CPB, 2 * q);
+        for (int i = 0; i < CPB; ++i) coff[i] = core_off(colw + 8 * (i / QG), 2 * (4 * (i % QG) + qb));
         // load cursor: tile ti_i, block kb_i of nkb_i, its columns' offsets xr[]
         int ti_i = blockIdx.x, kb_i = 0, nkb_i = 0, k_i = 0;
-        long long xr[CPB];
+        long long xr[4];
         const float2* X = nullptr;
         auto load_tile = [&]() {  // the first active tile from ti_i on
             for (; ti_i < ntiles; ti_i += gridDim.x) {
@@ -404,9 +409,9 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
                 X = T.X;
                 const int ncol = min(UM, T.p.ncol - T.t.col0);
 #pragma unroll
-                for (int i = 0; i < CPB; ++i) {
-                    const int c = cw * 32 + i * (32 / CPB) + lane / CPB;
-                    xr[i] = c < ncol ? __ldg(T.xoff + T.p.col0 + T.t.col0 + c) : -1;
+                for (int cg = 0; cg < 4; ++cg) {
+                    const int c = colw + 8 * cg;
+                    xr[cg] = c < ncol ? __ldg(T.xoff + T.p.col0 + T.t.col0 + c) : -1;
                 }
                 return;
             }
@@ -419,10 +424,12 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
             }
         };
         auto fetch = [&](float2(&dst)[CPB]) {  // the block at the cursor, then advance it
-            const int kc = kb_i * CPB + q;
 #pragma unroll
-            for (int i = 0; i < CPB; ++i)
-                dst[i] = (xr[i] >= 0 && kc < k_i) ? __ldg(X + xr[i] + kc) : make_float2(0.f, 0.f);
+            for (int i = 0; i < CPB; ++i) {
+                const int kc = kb_i * CPB + 4 * (i % QG) + qb;
+                const long long x = xr[i / QG];
+                dst[i] = (x >= 0 && kc < k_i) ? __ldg(X + x + kc) : make_float2(0.f, 0.f);
+            }
             for (int a = 0; a < UPSETS && ti_i < ntiles; ++a) advance();
         };
         load_tile();
