@@ -11,11 +11,14 @@
 // Xhi Blo accumulated in FP32 in tensor memory (TMEM lane = gathered column,
 // TMEM column = real output row).
 //
-// Operands sit in shared memory in the no-swizzle K-major core-matrix layout:
-// a core matrix is 8 rows x 16 bytes (4 TF32 along K); the two core matrices
-// of an 8-wide K block are 128 B apart (descriptor LBO) and 8-row groups 256 B
-// apart (SBO).  The operator is packed into exactly this layout, already
-// split, at session setup (umma_pack_kernel).
+// Operands sit in shared memory K-major.  The operator uses the no-swizzle
+// core-matrix layout: a core matrix is 8 rows x 16 bytes (4 TF32 along K); the
+// two core matrices of an 8-wide K block are 128 B apart (descriptor LBO) and
+// 8-row groups UBK * 32 B apart (SBO); it is packed into exactly this layout,
+// already split, at session setup (umma_pack_kernel), and copied in linearly.
+// The gathered columns use the 64-byte swizzled layout (core_off_a): a
+// column's K block is one 64-byte row, so the producers' stores of whole
+// column blocks hit every shared-memory bank once per half-warp.
 //
 // Persistent: one block per SM walks the tile list (tiles of one
 // problem adjacent, so the blocks in flight share its packed operator in L2)
@@ -23,12 +26,12 @@
 // overlaps the main loop of the next.  Warp roles, over a USTAGES-deep ring of
 // K blocks that runs on across tiles:
 //   producers  UPSETS sets of 4 warps, set j taking every UPSETS-th K block from
-//              j on; 32 gathered columns per warp: load the 4 complex of a K block
-//              of each column (8-lane groups, 32 contiguous bytes; zero past k
+//              j on; 32 gathered columns per warp: load the 8 complex of a K block
+//              of each column (8-lane groups, 64 contiguous bytes; zero past k
 //              or ncol), UPREF blocks ahead in registers; when a ring slot is
 //              free, split (hi = the top 19 bits, lo = TF32(x - hi)) into it,
-//              fence to the async proxy, arrive on full[s] (one elected lane
-//              per warp after __syncwarp).
+//              fence to the async proxy, arrive on full[s] (every lane, or one
+//              elected lane per warp after __syncwarp).
 //   W_LOAD_B   one thread: operator hi/lo blocks by cp.async.bulk onto full[s].
 //   W_MMA      one thread: per tile waits until its accumulator is drained
 //              (tmem_empty), then per block waits full[s], issues the three
@@ -101,7 +104,32 @@ __host__ __device__ __forceinline__ int core_off(int r, int kk) {
     return (r >> 3) * (UBK * 32) + (kk >> 2) * 128 + (r & 7) * 16 + (kk & 3) * 4;
 }
 
+constexpr int U_ARB = UBK * 4;         // bytes of one gathered column per K block
+// byte offset of element (r, kk) of a gathered-column K block in the K-major
+// swizzled layout (64-byte swizzle for UBK = 16, 32-byte for UBK = 8): row r
+// is U_ARB contiguous bytes at (r>>3) 8 U_ARB + (r&7) U_ARB, its 16-byte chunk
+// j stored at chunk j ^ (address bits 7.. of the row), so rows r and r+1 of a
+// half-warp store cover the 32 banks once
+__host__ __device__ __forceinline__ int core_off_a(int r, int kk) {
+    const int row = (r >> 3) * (8 * U_ARB) + (r & 7) * U_ARB;
+    return row + ((((kk >> 2) ^ ((((r & 7) * U_ARB) >> 7) & (U_ARB / 16 - 1)))) << 4) + (kk & 3) * 4;
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// descriptor of a gathered-column block in the swizzled layout: 8-row groups
+// 8 U_ARB bytes apart (SBO), leading offset unused (one swizzle row spans the
+// block's K), layout type 64-byte (4) or 32-byte (6) swizzle in bits 61-63;
+// the K step of 8 TF32 moves the start address by 32 bytes
+__device__ __forceinline__ uint64_t sdesc_a(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(((8 * U_ARB) >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)(U_ARB == 64 ? 4 : 6) << 61;
+    return d;
+}
 
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
     uint64_t d = 0;
@@ -200,10 +228,13 @@ __device__ __forceinline__ void split2(float x, uint32_t& hi, uint32_t& lo) {
 }
 
 // gathered-column split in place: hi = x with the 13 low mantissa bits cleared
-// (exact), lo = TF32 rounding of x - hi
+// (exact), lo = x - hi rounded to TF32 (nearest, ties away from zero) on its
+// bit pattern: add half of the dropped range, clear it (a carry moves into the
+// exponent as it should).  Two integer operations instead of a conversion,
+// which runs on the SM's narrow conversion pipe.
 __device__ __forceinline__ void split_mask(uint32_t& w, uint32_t& lo) {
     const uint32_t hi = w & 0xFFFFE000u;
-    lo = tf32_bits(__uint_as_float(w) - __uint_as_float(hi));
+    lo = (__float_as_uint(__uint_as_float(w) - __uint_as_float(hi)) + 0x1000u) & 0xFFFFE000u;
     w = hi;
 }
 
@@ -383,22 +414,19 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
         // ------------------------------------------------ gathered columns
         // producer set `set` takes the blocks g = set, set + UPSETS, ... of the block
         // sequence of this block's tiles; within a set, warp cw covers columns 32cw ..
-        // 32cw + 31.  Lane bits: b0 = complex q & 1, b1..b3 = column & 7, b4 = bit 1
-        // of q, so each half-warp store fills one core matrix (8 columns x 16 B, all
-        // 32 banks once) and each column's load is 4 consecutive complex.  Load
-        // i = (column group cg = i / (CPB/4), q group jj = i % (CPB/4)) reads column
-        // 32cw + 8cg + (lane>>1 & 7), complex q = 4jj + 2 b4 + b0.  Blocks are
-        // prefetched UPREF deep into registers and split into a ring slot once free.
-        static_assert(CPB % 4 == 0, "the producer mapping needs 4 complex per column and load");
-        constexpr int QG = CPB / 4;  // q groups per block
+        // 32cw + 31: load i reads columns 32cw + i (32/CPB) .., CPB lanes per column
+        // (lane = column, complex q), so each column's block is one contiguous load
+        // and a half-warp store fills two swizzled rows (all 32 banks once).  Blocks
+        // are prefetched UPREF deep into registers and split into a ring slot once
+        // free.
         const int set = warp >> 2, cw = warp & 3;
-        const int colw = cw * 32 + ((lane >> 1) & 7), qb = 2 * (lane >> 4) + (lane & 1);
-        int coff[CPB];  // core_off(column, 2q) of load i
+        const int colw = cw * 32 + lane / CPB, q = lane % CPB;
+        int coff[CPB];  // core_off_a(column, 2q) of load i
 #pragma unroll
-        for (int i = 0; i < CPB; ++i) coff[i] = core_off(colw + 8 * (i / QG), 2 * (4 * (i % QG) + qb));
+        for (int i = 0; i < CPB; ++i) coff[i] = core_off_a(colw + i * (32 / CPB), 2 * q);
         // load cursor: tile ti_i, block kb_i of nkb_i, its columns' offsets xr[]
         int ti_i = blockIdx.x, kb_i = 0, nkb_i = 0, k_i = 0;
-        long long xr[4];
+        long long xr[CPB];
         const float2* X = nullptr;
         auto load_tile = [&]() {  // the first active tile from ti_i on
             for (; ti_i < ntiles; ti_i += gridDim.x) {
@@ -409,9 +437,9 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
                 X = T.X;
                 const int ncol = min(UM, T.p.ncol - T.t.col0);
 #pragma unroll
-                for (int cg = 0; cg < 4; ++cg) {
-                    const int c = colw + 8 * cg;
-                    xr[cg] = c < ncol ? __ldg(T.xoff + T.p.col0 + T.t.col0 + c) : -1;
+                for (int i = 0; i < CPB; ++i) {
+                    const int c = colw + i * (32 / CPB);
+                    xr[i] = c < ncol ? __ldg(T.xoff + T.p.col0 + T.t.col0 + c) : -1;
                 }
                 return;
             }
@@ -426,8 +454,8 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
         auto fetch = [&](float2(&dst)[CPB]) {  // the block at the cursor, then advance it
 #pragma unroll
             for (int i = 0; i < CPB; ++i) {
-                const int kc = kb_i * CPB + 4 * (i % QG) + qb;
-                const long long x = xr[i / QG];
+                const int kc = kb_i * CPB + q;
+                const long long x = xr[i];
                 dst[i] = (x >= 0 && kc < k_i) ? __ldg(X + x + kc) : make_float2(0.f, 0.f);
             }
             for (int a = 0; a < UPSETS && ti_i < ntiles; ++a) advance();
@@ -526,11 +554,12 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
                     const uint32_t ahi = smem_u32(usm + s * U_STAGE_BYTES), alo = ahi + U_A_BYTES;
                     const uint32_t bhi = ahi + 2 * U_A_BYTES, blo = bhi + U_B_BYTES;
 #pragma unroll
-                    for (int ks = 0; ks < UBK / 8; ++ks) {  // K = 8 per MMA: two core matrices, 256 B
-                        const uint32_t o = ks * 256;
-                        umma_tf32(d, sdesc(ahi + o), sdesc(bhi + o), idesc, (kb > 0 || ks > 0) ? 1u : 0u);
-                        umma_tf32(d, sdesc(alo + o), sdesc(bhi + o), idesc, 1u);
-                        umma_tf32(d, sdesc(ahi + o), sdesc(blo + o), idesc, 1u);
+                    for (int ks = 0; ks < UBK / 8; ++ks) {  // K = 8 per MMA
+                        const uint32_t o = ks * 256, oa = ks * 32;  // operator: two core matrices; columns: 32 B
+                        const uint64_t dah = sdesc_a(ahi + oa), dal = sdesc_a(alo + oa);
+                        umma_tf32(d, dah, sdesc(bhi + o), idesc, (kb > 0 || ks > 0) ? 1u : 0u);
+                        umma_tf32(d, dal, sdesc(bhi + o), idesc, 1u);
+                        umma_tf32(d, dah, sdesc(blo + o), idesc, 1u);
                     }
                     umma_commit(&empty[s]);
                     last = g;
