@@ -38,8 +38,9 @@
 //              MMAs, commits to empty[s]; after the tile commits tmem_full.
 //   W_EPI..    epilogue, UEPI groups of 4 warps: warp w on TMEM lanes 32 (w % 4) ..,
 //              its group on every UEPI-th 64-column chunk: TMEM -> a parking
-//              area -> global, one column at a time in 256-byte coalesced
-//              rows; then arrive on tmem_empty.
+//              area -> global, two columns at a time in 256-byte coalesced
+//              rows of 16-byte stores (vector atomics where outputs collide);
+//              then arrive on tmem_empty.
 // Every mbarrier wait is bounded (1 s, or sooner once another role failed):
 // a block that gives up stops issuing work, lets its MMAs and copies drain
 // (bounded), frees its TMEM and sets *err.
@@ -90,8 +91,9 @@ constexpr int U_A_BYTES = UM * UBK * 4;
 constexpr int U_B_BYTES = UNMAX * UBK * 4;
 constexpr int U_STAGE_BYTES = 2 * U_A_BYTES + 2 * U_B_BYTES;
 constexpr int PCH = DDFMM_UMMA_PCH;  // epilogue chunk: complex rows parked per column
-static_assert(PCH == 16 || PCH == 32, "epilogue chunk of 16 or 32 rows");
-constexpr int U_PARK_BYTES = 4 * UEPI * 32 * (PCH + 1) * 8;  // 32 columns x PCH complex (+1 pad) per warp
+static_assert(PCH == 32, "epilogue chunk of 32 rows");
+constexpr int UPS = PCH + 2;  // parking-area row stride (complex): 16-byte rows, conflict-free 16-byte accesses
+constexpr int U_PARK_BYTES = 4 * UEPI * 32 * UPS * 8;  // 32 columns x PCH complex (+2 pad) per warp
 // ring + parking area + alignment slack: one block per SM (also what the 512
 // TMEM columns need)
 constexpr int UGEMM_SMEM = USTAGES * U_STAGE_BYTES + U_PARK_BYTES + 1024;
@@ -293,26 +295,47 @@ size_t umma_packed_floats(int m, int k) {
 }
 
 // ---------------------------------------------------------------- GEMM
-// Epilogue stores of one parked chunk: 32 / PCH columns per instruction, PCH
-// consecutive rows each; column c of the warp's 32 writes at Y + (c's yoff) + i.
+// Epilogue stores of one parked chunk (PCH complex rows from row0 on, 32 columns):
+// two columns per instruction, each lane two consecutive rows of one column, as
+// one 16-byte store or vector atomic where the output is 16-byte aligned (two
+// 8-byte ones otherwise, or one at an odd last row).  Column c of the warp's 32
+// writes at Y + (c's yoff) + row.
+template <int MODE>
+__device__ __forceinline__ void store_one(float2* y, float2 v) {
+    if (MODE == GEMM_SET) {
+        *y = v;
+    } else if (MODE == GEMM_ADD) {
+        const float2 o = *y;
+        *y = make_float2(o.x + v.x, o.y + v.y);
+    } else {
+        atomicAdd(y, v);
+    }
+}
 template <int MODE>
 __device__ __forceinline__ void store_chunk(const float2* park, float2* Y, long long my_yo, int col_base, int ncol,
-                                            int i, int rows, int lane) {
-    const int sub = lane / PCH, r = lane % PCH;
-    for (int cc = 0; cc < 32; cc += 32 / PCH) {
+                                            int row0, int rows, int lane) {
+    const int sub = lane >> 4, r2 = 2 * (lane & 15), i = row0 + r2;
+    for (int cc = 0; cc < 32; cc += 2) {
         const int col = cc + sub;
         const long long yb = __shfl_sync(0xffffffffu, my_yo, col);
         if (col_base + cc >= ncol) break;
         if (i >= rows || col_base + col >= ncol) continue;
-        const float2 val = park[col * (PCH + 1) + r];
+        const float4 v = *reinterpret_cast<const float4*>(park + col * UPS + r2);
         float2* y = Y + yb + i;
-        if (MODE == GEMM_SET) {
-            *y = val;
-        } else if (MODE == GEMM_ADD) {
-            const float2 o = *y;
-            *y = make_float2(o.x + val.x, o.y + val.y);
+        const bool two = i + 1 < rows;
+        if (two && (reinterpret_cast<uintptr_t>(y) & 15) == 0) {
+            float4* y4 = reinterpret_cast<float4*>(y);
+            if (MODE == GEMM_SET) {
+                *y4 = v;
+            } else if (MODE == GEMM_ADD) {
+                const float4 o = *y4;
+                *y4 = make_float4(o.x + v.x, o.y + v.y, o.z + v.z, o.w + v.w);
+            } else {
+                atomicAdd(y4, v);
+            }
         } else {
-            atomicAdd(y, val);
+            store_one<MODE>(y, make_float2(v.x, v.y));
+            if (two) store_one<MODE>(y + 1, make_float2(v.z, v.w));
         }
     }
 }
@@ -576,7 +599,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
         const int ew = warp - W_EPI;  // group ew / 4 takes every UEPI-th chunk of accumulator columns
         const int qw = warp & 3;      // TMEM lanes 32 qw .. 32 qw + 31 = tile columns
         const int first = (ew >> 2) * 2 * PCH;
-        float2* park = park_all + ew * (32 * (PCH + 1));
+        float2* park = park_all + ew * (32 * UPS);
         auto release = [&](int acc) {  // this warp is done reading the accumulator
             asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
             if (UELECT) {
@@ -621,20 +644,21 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
                             : "memory");
                         asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-                        for (int e = 0; e < 8; ++e)
-                            park[lane * (PCH + 1) + (h >> 1) + e] =
-                                make_float2(__uint_as_float(v[2 * e]), __uint_as_float(v[2 * e + 1]));
+                        for (int e = 0; e < 8; e += 2)  // 16-byte stores: 8 lanes cover the 32 banks once
+                            *reinterpret_cast<float4*>(park + lane * UPS + (h >> 1) + e) =
+                                make_float4(__uint_as_float(v[2 * e]), __uint_as_float(v[2 * e + 1]),
+                                            __uint_as_float(v[2 * e + 2]), __uint_as_float(v[2 * e + 3]));
                     }
                 }
                 if (c0 + UEPI * 2 * PCH >= N) release(acc);  // last chunk read: accumulator back to the MMA issuer
                 __syncwarp();
-                const int i = (c0 >> 1) + lane % PCH;  // complex row of this lane
+                const int row0 = c0 >> 1;  // first complex row of the chunk
                 if (mode == GEMM_SET)
-                    store_chunk<GEMM_SET>(park, Y, my_yo, qw * 32, ncol, i, rows, lane);
+                    store_chunk<GEMM_SET>(park, Y, my_yo, qw * 32, ncol, row0, rows, lane);
                 else if (mode == GEMM_ADD)
-                    store_chunk<GEMM_ADD>(park, Y, my_yo, qw * 32, ncol, i, rows, lane);
+                    store_chunk<GEMM_ADD>(park, Y, my_yo, qw * 32, ncol, row0, rows, lane);
                 else
-                    store_chunk<GEMM_ATOMIC>(park, Y, my_yo, qw * 32, ncol, i, rows, lane);
+                    store_chunk<GEMM_ATOMIC>(park, Y, my_yo, qw * 32, ncol, row0, rows, lane);
                 __syncwarp();
             }
             ++it;
