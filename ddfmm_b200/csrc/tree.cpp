@@ -4,7 +4,9 @@
 #include <algorithm>
 #include <cmath>
 #include <deque>
+#include <exception>
 #include <stdexcept>
+#include <thread>
 
 namespace ddfmm {
 
@@ -237,6 +239,31 @@ void Tree::highlist(int bi) {
     }
 }
 
+// f(i) for i in [0, n) on the host's cores; each i is independent.  The first
+// exception thrown by any call is rethrown here after every thread has joined.
+template <class F>
+static void parallel_for(size_t n, F f) {
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>(std::min<size_t>(hw, 64), (n + 255) / 256);
+    if (nt <= 1) {
+        for (size_t i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::vector<std::exception_ptr> err(nt);
+    std::vector<std::thread> th;
+    for (size_t t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            try {
+                for (size_t i = t; i < n; i += nt) f(i);  // interleaved: boxes of a level differ in cost
+            } catch (...) {
+                err[t] = std::current_exception();
+            }
+        });
+    for (auto& x : th) x.join();
+    for (auto& e : err)
+        if (e) std::rethrow_exception(e);
+}
+
 // setup_tree, src/wave3d_setup.cpp:100-299
 void Tree::build(const double* p3n, int n, const TreeParams& p) {
     prm = p;
@@ -302,40 +329,50 @@ void Tree::build(const double* p3n, int n, const TreeParams& p) {
     std::sort(order.begin(), order.end(), [&](int x, int y) {
         return pack(boxes[x].level, boxes[x].idx) < pack(boxes[y].level, boxes[y].idx);
     });
-    // lists for every box with points (src/wave3d_setup.cpp:206-220)
+    // lists for every box with points (src/wave3d_setup.cpp:206-220), then the
+    // directional sets (:255-296).  A box's low-frequency lists read only the tree;
+    // its high-frequency lists and directional sets read its parent's, so both run
+    // level by level (levels are contiguous in key order), the boxes of a level in
+    // parallel.  Every box's lists come from the same sequential code, so the result
+    // does not depend on the thread count.
     const double eps = 1e-12;
-    for (int bi : order) {
-        if (!boxes[bi].has_pts()) continue;
-        if (width(boxes[bi].level) < 1 - eps)
-            lowlist(bi);
-        else
-            highlist(bi);
-    }
-    // directional sets (src/wave3d_setup.cpp:255-296); parents come first in key order
-    for (int bi : order) {
-        Box& cur = boxes[bi];
-        double W = width(cur.level);
-        if (!(W > 1 - eps && cur.has_pts())) continue;
-        if (cur.level != lvlC) {
-            int pi = find(cur.level - 1, Idx3{{cur.idx[0] / 2, cur.idx[1] / 2, cur.idx[2] / 2}});
-            check(pi >= 0, "missing parent");
-            for (const Idx3& d : boxes[pi].outdirs) cur.outdirs.insert(parent_dir(d));
-            for (const Idx3& d : boxes[pi].incdirs) cur.incdirs.insert(parent_dir(d));
-        }
-        Pt3 cc = center(cur);
-        for (auto& kv : cur.far)
-            for (int oi : kv.second) {
-                Pt3 oc = center(boxes[oi]);
-                Pt3 t = sub(oc, cc);
-                double nt = l2(t);
-                for (int d = 0; d < 3; ++d) t[d] /= nt;
-                cur.outdirs.insert(nml2dir(t, W));
-                t = sub(cc, oc);
-                nt = l2(t);
-                for (int d = 0; d < 3; ++d) t[d] /= nt;
-                cur.incdirs.insert(nml2dir(t, W));
+    std::vector<size_t> lv(1, 0);
+    for (size_t i = 1; i < order.size(); ++i)
+        if (boxes[order[i]].level != boxes[order[i - 1]].level) lv.push_back(i);
+    lv.push_back(order.size());
+    for (size_t l = 0; l + 1 < lv.size(); ++l)
+        parallel_for(lv[l + 1] - lv[l], [&](size_t i) {
+            const int bi = order[lv[l] + i];
+            if (!boxes[bi].has_pts()) return;
+            if (width(boxes[bi].level) < 1 - eps)
+                lowlist(bi);
+            else
+                highlist(bi);
+        });
+    for (size_t l = 0; l + 1 < lv.size(); ++l)
+        parallel_for(lv[l + 1] - lv[l], [&](size_t i) {
+            Box& cur = boxes[order[lv[l] + i]];
+            double W = width(cur.level);
+            if (!(W > 1 - eps && cur.has_pts())) return;
+            if (cur.level != lvlC) {
+                int pi = find(cur.level - 1, Idx3{{cur.idx[0] / 2, cur.idx[1] / 2, cur.idx[2] / 2}});
+                check(pi >= 0, "missing parent");
+                for (const Idx3& d : boxes[pi].outdirs) cur.outdirs.insert(parent_dir(d));
+                for (const Idx3& d : boxes[pi].incdirs) cur.incdirs.insert(parent_dir(d));
             }
-    }
+            Pt3 cc = center(cur);
+            for (auto& kv : cur.far) {
+                // the incoming direction of every far box is its key: highlist classified
+                // (cc - oc) / |cc - oc| with the same arithmetic
+                cur.incdirs.insert(kv.first);
+                for (int oi : kv.second) {
+                    Pt3 t = sub(center(boxes[oi]), cc);
+                    double nt = l2(t);
+                    for (int d = 0; d < 3; ++d) t[d] /= nt;
+                    cur.outdirs.insert(nml2dir(t, W));
+                }
+            }
+        });
 }
 
 // HighFetchIndex3Sort, src/mlib3d.cpp:328-357
