@@ -214,6 +214,21 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def gemm_traffic(kernel, workload_name):
+    """DRAM bytes (read + write) per launch of the GEMM kernel over one matvec of
+    the bench workload, from the one-pass ncu capture committed under profiles/,
+    or None for other workloads or kernels."""
+    from ddfmm_b200 import workloads as wl
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "gemm_dram_traffic_sphere_K64_P6.txt")
+    if workload_name != wl.LARGE.name or not os.path.exists(path):
+        return None
+    for line in open(path):
+        f = line.split()
+        if f and not line.startswith("#") and f[0] == kernel:
+            return (float(f[2]) + float(f[3])) / float(f[1])
+    return None
+
+
 def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws, profile_json=None, precision=None):
     """The mixed-precision form on the same workload: complex64 densities on
     the device, 3xTF32 translations (tcgen05 by default, or the mma.sync
@@ -268,12 +283,13 @@ def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws, profile_json=None, 
     stream.synchronize()
     prof = m.profile_read(reset=True)
     m.profile(False)
-    gk = {"launches": 0, "ms": 0.0, "flops": 0.0}
+    gk = {"launches": 0, "ms": 0.0, "flops": 0.0, "bytes": 0.0}
     for e in prof.values():
         if e["kernel"] in ("umma_cgemm_kernel", "zgemm_kernel"):
             gk["launches"] += e["launches"]
             gk["ms"] += e["ms"]
             gk["flops"] += e["flops"]
+            gk["bytes"] += e["bytes"]
     roof = None
     if gk["ms"] > 0:
         peaks = measured_peaks()
@@ -283,8 +299,14 @@ def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws, profile_json=None, 
             peak, src = peaks["bf16_tflops_sustained"] / 2, "MEASURED_PEAKS.json bf16_tflops_sustained / 2"
         else:
             peak, src = 1400.0 / 2, "fallback 1.4 PFLOP/s bf16 sustained / 2"
-        roof = {"bound": "tensor", "kernel": "umma_cgemm_kernel" if precision == _lib.MIXED else "cgemm_kernel",
-                "achieved": executed, "peak": peak, "unit": "TFLOP/s", "frac": executed / peak, "traffic": None,
+        kname = "umma_cgemm_kernel" if precision == _lib.MIXED else "cgemm_kernel"
+        roof = {"bound": "tensor", "kernel": kname,
+                "achieved": executed, "peak": peak, "unit": "TFLOP/s", "frac": executed / peak,
+                "traffic": gemm_traffic(kname, w.name),
+                "traffic_note": "DRAM read + write bytes per launch, averaged over one matvec's GEMM launches "
+                                "(one-pass ncu capture); algorithmic bytes per launch with complex64 columns "
+                                "and operators: algorithmic_bytes",
+                "algorithmic_bytes": 0.5 * gk["bytes"] / max(1, gk["launches"]),
                 "algorithmic_complex_tflops": algo, "launches": gk["launches"] // 3,
                 "peak_source": src + " (dense TF32 runs at half the BF16 rate on B200's tensor cores)",
                 "note": "executed = 3 x algorithmic (hi*hi + lo*hi + hi*lo TF32 products)"}
@@ -621,7 +643,11 @@ def run_ours(args):
         peak = fp64_peak_tflops(torch, dev)
         achieved = dk["flops"] / (dk["ms"] * 1e-3) / 1e12
         roof = {"bound": "tensor", "pipe": "FP64 DMMA (mma.sync.m8n8k4.f64)", "kernel": dom, "achieved": achieved,
-                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": gemm_traffic(dom, w.name),
+                "traffic_note": "DRAM read + write bytes per launch, averaged over one matvec's GEMM launches "
+                                "(one-pass ncu capture); algorithmic bytes per launch: algorithmic_bytes",
+                "algorithmic_bytes": dk["bytes"] / max(1, dk["launches"]),
                 "peak_source": "measured cuBLAS DGEMM 4096^3 on this GPU (FP64 has no entry in MEASURED_PEAKS.json)",
                 "launches": dk["launches"]}
     else:
