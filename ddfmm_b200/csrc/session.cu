@@ -643,6 +643,7 @@ void Session::build() {
     std::unordered_map<uint64_t, int> upmap, dnmap;
     NodeKey nk;
     std::map<int, std::pair<int, int> > uprange, dnrange;  // level -> [begin, end)
+    std::map<int, long long> tmp_up_level;                 // level -> temporary elements of its M2M sums
     long long upeq_total = 0, dnchk_total = 0, tmp_max = 0;
     for (auto& kv : hflevels) {
         double W = T.width(kv.first);
@@ -667,6 +668,7 @@ void Session::build() {
             }
         }
         uprange[kv.first] = std::make_pair(u0, (int)up.size());
+        tmp_up_level[kv.first] = tmp_up;
         dnrange[kv.first] = std::make_pair(d0, (int)dn.size());
         tmp_max = std::max(tmp_max, std::max(tmp_up, tmp_dn));
     }
@@ -996,13 +998,16 @@ void Session::build() {
         Step ms{};
         ms.kind = 4;
         ms.label = "memset";
-        ms.ms = Memset{T0, es * (size_t)tmp_max};
+        ms.ms = Memset{T0, es * (size_t)tmp_up_level[level]};  // this level's sums only
         push_step(ms);
-        // M2M: E3 upchkval = sum_children [E3 ue2uc E1(child)] w_child (src/wave3d_eval.cpp:796-834)
-        for (int ind = 0; ind < 8; ++ind) {
-            std::map<Idx3, int> pid;
+        // M2M: E3 upchkval = sum_children [E3 ue2uc E1(child)] w_child (src/wave3d_eval.cpp:796-834),
+        // one launch for the 8 child positions: a problem per (wedge, child), all adding into
+        // the parents' sums
+        {
+            std::map<std::pair<Idx3, int>, int> pid;
             std::vector<GemmProblem> probs;
             std::vector<std::vector<long long> > xo, yo;
+            for (int ind = 0; ind < 8; ++ind)
             for (int i = ur.first; i < ur.second; ++i) {
                 const Node& u = up[i];
                 int c = T.child(u.box, ind);
@@ -1015,12 +1020,12 @@ void Session::build() {
                     if (cit == upmap.end()) throw std::runtime_error("child has no directional equivalent density");
                     xoff = up[cit->second].off;
                 }
-                auto pit = pid.find(u.dir);
+                auto pit = pid.find(std::make_pair(u.dir, ind));
                 int p;
                 if (pit == pid.end()) {
                     const DirMats& M = m2m_mats.at(std::make_pair(W, u.dir));
                     p = (int)probs.size();
-                    pid[u.dir] = p;
+                    pid[std::make_pair(u.dir, ind)] = p;
                     if (M.cached) {
                         probs.push_back(GemmProblem{nullptr, M.mrows, M.mcols, M.mrows, 0, 0, M.pk[ind]});
                     } else {
@@ -1119,11 +1124,13 @@ void Session::build() {
             xt[p].push_back(d.toff);
         }
         add_gemm(p2, xa, xt, hf_dnchk, T1, GEMM_SET, width_label("hf_dc2de", W));
-        // L2L into the children's (pdir) u, or LF dnchkval at W=1 (src/wave3d_eval.cpp:950-991)
-        for (int ind = 0; ind < 8; ++ind) {
-            std::map<Idx3, int> pid;
+        // L2L into the children's (pdir) u, or LF dnchkval at W=1 (src/wave3d_eval.cpp:950-991),
+        // one launch for the 8 child positions: a problem per (wedge, child)
+        {
+            std::map<std::pair<Idx3, int>, int> pid;
             std::vector<GemmProblem> probs;
             std::vector<std::vector<long long> > xo, yo;
+            for (int ind = 0; ind < 8; ++ind)
             for (int i = dr.first; i < dr.second; ++i) {
                 const Node& d = dn[i];
                 int c = T.child(d.box, ind);
@@ -1136,12 +1143,12 @@ void Session::build() {
                     if (cit == dnmap.end()) throw std::runtime_error("child has no directional check value");
                     yoff = dn[cit->second].off;
                 }
-                auto pit = pid.find(d.dir);
+                auto pit = pid.find(std::make_pair(d.dir, ind));
                 int p;
                 if (pit == pid.end()) {
                     const DirMats& M = l2l_mats.at(std::make_pair(W, d.dir));
                     p = (int)probs.size();
-                    pid[d.dir] = p;
+                    pid[std::make_pair(d.dir, ind)] = p;
                     if (M.cached) {
                         probs.push_back(GemmProblem{nullptr, M.mrows, M.mcols, M.mrows, 0, 0, M.pk[ind]});
                     } else {
