@@ -22,6 +22,7 @@
 #include <stdexcept>
 #include <set>
 #include <unordered_map>
+#include <unordered_set>
 
 namespace ddfmm {
 
@@ -339,6 +340,11 @@ struct NodeKey {
                (uint64_t)(d[2] + 1024);
     }
 };
+// (width, wedge) as one hash key: widths are powers of two, wedge components |d| < 1024
+uint64_t wedge_key(double W, const Idx3& d) {
+    const uint64_t wl = (uint64_t)(std::lround(std::log2(W)) + 32);
+    return (wl << 33) | ((uint64_t)(d[0] + 1024) << 22) | ((uint64_t)(d[1] + 1024) << 11) | (uint64_t)(d[2] + 1024);
+}
 Pt3 shifted_point(int ind, double W) {  // ShiftedPoint, src/mlib3d.cpp:21-30
     int a = (ind & 4) >> 2, b = (ind & 2) >> 1, c = ind & 1;
     return Pt3{{(a - 0.5) * W / 2, (b - 0.5) * W / 2, (c - 0.5) * W / 2}};
@@ -617,10 +623,14 @@ void Session::build() {
         int r1, r2, canon;
     };
     std::map<std::pair<double, Idx3>, DirPts> dirpts;
+    std::unordered_map<uint64_t, const DirPts*> dirfast;  // hash index into dirpts (node addresses are stable)
     auto get_dir = [&](double W, const Idx3& dir) -> const DirPts& {
+        const uint64_t fk = wedge_key(W, dir);
+        auto ft = dirfast.find(fk);
+        if (ft != dirfast.end()) return *ft->second;
         auto key = std::make_pair(W, dir);
         auto it = dirpts.find(key);
-        if (it != dirpts.end()) return it->second;
+        if (it != dirpts.end()) return *(dirfast[fk] = &it->second);
         Idx3 sgn, pv;
         int c = get_canon(W, dir, sgn, pv);
         const HighFreqOp& op = *hfcanon[c].op;
@@ -632,7 +642,9 @@ void Session::build() {
         d.dep = upload(shuffle(op.ucp, pv, sgn, -1.0));
         d.uep = upload(shuffle(op.uep, pv, sgn, 1.0));
         d.dcp = upload(shuffle(op.uep, pv, sgn, -1.0));
-        return dirpts[key] = d;
+        DirPts& stored = dirpts[key] = d;
+        dirfast[fk] = &stored;
+        return stored;
     };
 
     std::map<int, std::vector<int> > hflevels;  // level -> tree boxes with points, width >= 1
@@ -641,6 +653,18 @@ void Session::build() {
 
     std::vector<Node> up, dn;
     std::unordered_map<uint64_t, int> upmap, dnmap;
+    {
+        size_t nu = 0, nd = 0;
+        for (auto& kv : hflevels)
+            for (int b : kv.second) {
+                nu += T.boxes[b].outdirs.size();
+                nd += T.boxes[b].incdirs.size();
+            }
+        upmap.reserve(nu);
+        dnmap.reserve(nd);
+        up.reserve(nu);
+        dn.reserve(nd);
+    }
     NodeKey nk;
     std::map<int, std::pair<int, int> > uprange, dnrange;  // level -> [begin, end)
     std::map<int, long long> tmp_up_level;                 // level -> temporary elements of its M2M sums
@@ -728,12 +752,13 @@ void Session::build() {
         ccanon = cp.canon;
         return upward ? cp.uep : cp.dcp;
     };
+    std::unordered_set<uint64_t> m2m_seen, l2l_seen;  // wedges already in m2m_mats / l2l_mats
     for (auto& kv : hflevels) {
         double W = T.width(kv.first);
         auto ur = uprange[kv.first], dr = dnrange[kv.first];
         for (int i = ur.first; i < ur.second; ++i) {
+            if (!m2m_seen.insert(wedge_key(W, up[i].dir)).second) continue;
             auto key = std::make_pair(W, up[i].dir);
-            if (m2m_mats.count(key)) continue;
             const DirPts& dp = get_dir(W, up[i].dir);
             DirMats M{};
             child_pts(W, up[i].dir, true, M.mcols, M.ccanon);
@@ -751,8 +776,8 @@ void Session::build() {
             m2m_mats[key] = M;
         }
         for (int i = dr.first; i < dr.second; ++i) {
+            if (!l2l_seen.insert(wedge_key(W, dn[i].dir)).second) continue;
             auto key = std::make_pair(W, dn[i].dir);
-            if (l2l_mats.count(key)) continue;
             const DirPts& dp = get_dir(W, dn[i].dir);
             DirMats M{};
             child_pts(W, dn[i].dir, false, M.mrows, M.ccanon);
@@ -771,7 +796,7 @@ void Session::build() {
         }
     }
     // M2L: canonical offset o_c = S^-1 (c_t - c_s), so M(dir, o) = M(canon, o_c)
-    std::map<std::tuple<int, int, int, int>, int> m2l_id;  // (canon, ox, oy, oz) -> matrix
+    std::unordered_map<uint64_t, int> m2l_id;  // (canon, ox, oy, oz) packed -> matrix
     struct M2LMat {
         size_t raw, tmp, fin;
         int canon, r1;
@@ -786,7 +811,7 @@ void Session::build() {
         int level = kv.first;
         double W = T.width(level);
         auto dr = dnrange[level];
-        std::map<int, int> local;  // matrix id -> local problem index
+        std::vector<int> local;  // matrix id -> local problem index (-1: none yet)
         auto& X = m2l_x[level];
         auto& Y = m2l_y[level];
         auto& Pids = m2l_probs[level];
@@ -804,7 +829,8 @@ void Session::build() {
                 int o[3], oc[3];
                 for (int d = 0; d < 3; ++d) o[d] = tb.idx[d] - sb.idx[d];
                 for (int d = 0; d < 3; ++d) oc[d] = sgn[pv[d]] * o[pv[d]];
-                auto key = std::make_tuple(t.canon, oc[0], oc[1], oc[2]);
+                const uint64_t key = ((uint64_t)t.canon << 33) | ((uint64_t)(oc[0] + 1024) << 22) |
+                                     ((uint64_t)(oc[1] + 1024) << 11) | (uint64_t)(oc[2] + 1024);
                 auto mit = m2l_id.find(key);
                 int gid;
                 if (mit == m2l_id.end()) {
@@ -824,16 +850,14 @@ void Session::build() {
                 } else {
                     gid = mit->second;
                 }
-                auto lit = local.find(gid);
-                int li;
-                if (lit == local.end()) {
+                if ((size_t)gid >= local.size()) local.resize(m2l_mats.size(), -1);
+                int li = local[gid];
+                if (li < 0) {
                     li = (int)Pids.size();
                     local[gid] = li;
                     Pids.push_back(gid);
                     X.emplace_back();
                     Y.emplace_back();
-                } else {
-                    li = lit->second;
                 }
                 X[li].push_back(up[uit->second].off);
                 Y[li].push_back(t.off);
@@ -1004,7 +1028,7 @@ void Session::build() {
         // one launch for the 8 child positions: a problem per (wedge, child), all adding into
         // the parents' sums
         {
-            std::map<std::pair<Idx3, int>, int> pid;
+            std::unordered_map<uint64_t, int> pid;  // (wedge, child) -> problem
             std::vector<GemmProblem> probs;
             std::vector<std::vector<long long> > xo, yo;
             for (int ind = 0; ind < 8; ++ind)
@@ -1020,12 +1044,13 @@ void Session::build() {
                     if (cit == upmap.end()) throw std::runtime_error("child has no directional equivalent density");
                     xoff = up[cit->second].off;
                 }
-                auto pit = pid.find(std::make_pair(u.dir, ind));
+                const uint64_t pk = (wedge_key(W, u.dir) << 3) | (uint64_t)ind;
+                auto pit = pid.find(pk);
                 int p;
                 if (pit == pid.end()) {
                     const DirMats& M = m2m_mats.at(std::make_pair(W, u.dir));
                     p = (int)probs.size();
-                    pid[std::make_pair(u.dir, ind)] = p;
+                    pid[pk] = p;
                     if (M.cached) {
                         probs.push_back(GemmProblem{nullptr, M.mrows, M.mcols, M.mrows, 0, 0, M.pk[ind]});
                     } else {
@@ -1127,7 +1152,7 @@ void Session::build() {
         // L2L into the children's (pdir) u, or LF dnchkval at W=1 (src/wave3d_eval.cpp:950-991),
         // one launch for the 8 child positions: a problem per (wedge, child)
         {
-            std::map<std::pair<Idx3, int>, int> pid;
+            std::unordered_map<uint64_t, int> pid;  // (wedge, child) -> problem
             std::vector<GemmProblem> probs;
             std::vector<std::vector<long long> > xo, yo;
             for (int ind = 0; ind < 8; ++ind)
@@ -1143,12 +1168,13 @@ void Session::build() {
                     if (cit == dnmap.end()) throw std::runtime_error("child has no directional check value");
                     yoff = dn[cit->second].off;
                 }
-                auto pit = pid.find(std::make_pair(d.dir, ind));
+                const uint64_t pk = (wedge_key(W, d.dir) << 3) | (uint64_t)ind;
+                auto pit = pid.find(pk);
                 int p;
                 if (pit == pid.end()) {
                     const DirMats& M = l2l_mats.at(std::make_pair(W, d.dir));
                     p = (int)probs.size();
-                    pid[std::make_pair(d.dir, ind)] = p;
+                    pid[pk] = p;
                     if (M.cached) {
                         probs.push_back(GemmProblem{nullptr, M.mrows, M.mcols, M.mrows, 0, 0, M.pk[ind]});
                     } else {
