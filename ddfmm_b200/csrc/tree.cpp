@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <deque>
 #include <exception>
 #include <stdexcept>
@@ -239,11 +240,19 @@ void Tree::highlist(int bi) {
     }
 }
 
+// Host threads for list construction: DDFMM_HOST_THREADS when set (> 0), else
+// every hardware thread.
+static size_t host_threads() {
+    const char* e = std::getenv("DDFMM_HOST_THREADS");
+    const int v = e ? std::atoi(e) : 0;
+    return v > 0 ? (size_t)v : std::max(1u, std::thread::hardware_concurrency());
+}
+
 // f(i) for i in [0, n) on the host's cores; each i is independent.  The first
 // exception thrown by any call is rethrown here after every thread has joined.
 template <class F>
 static void parallel_for(size_t n, F f) {
-    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t hw = host_threads();
     const size_t nt = std::min<size_t>(std::min<size_t>(hw, 64), (n + 255) / 256);
     if (nt <= 1) {
         for (size_t i = 0; i < n; ++i) f(i);

@@ -33,6 +33,20 @@ def test_tree_adaptive_case_has_all_list_kinds():
     assert any(L["width"] < 1 and L["boxes"] > L["leaves"] for L in st["levels"])
 
 
+def test_tree_lists_independent_of_host_threads(monkeypatch):
+    """The lists are built level by level with the boxes of a level spread over
+    host threads; every count must be the same on one thread and on several
+    (a K=16 sphere: levels large enough to be split)."""
+    from ddfmm_b200 import workloads as wl
+    w = wl.sphere(16, None, accu=2)
+    out = []
+    for n in ("1", "4"):
+        monkeypatch.setenv("DDFMM_HOST_THREADS", n)
+        out.append(_lib.tree_stats(w.points(), 16, 100, w.maxlevel, 8, 4))
+    assert out[0] == out[1]
+    assert sum(L["far_pairs"] for L in out[0]["levels"]) > 0 and sum(L["v_pairs"] for L in out[0]["levels"]) > 0
+
+
 def test_tree_rejects_point_outside_root_box():
     pos = np.array([[0.0, 0.0, 0.0], [2.5, 0.0, 0.0]])
     with pytest.raises(_lib.DDFMMError) as e:
