@@ -16,6 +16,39 @@ namespace ddfmm {
                                      #x + ")");                                                    \
     } while (0)
 
+namespace {
+// Host copies of a tick (densities into pinned staging, values out of it): split
+// into pieces of at most 1 MiB and spread over up to 8 threads; one thread when
+// the tick moves less than 1 MiB.
+struct Copy {
+    void* dst;
+    const void* src;
+    size_t bytes;
+};
+void parallel_copy(const std::vector<Copy>& jobs) {
+    constexpr size_t kPiece = 1 << 20;
+    std::vector<Copy> pieces;
+    size_t total = 0;
+    for (const Copy& c : jobs) {
+        total += c.bytes;
+        for (size_t o = 0; o < c.bytes; o += kPiece)
+            pieces.push_back(Copy{static_cast<char*>(c.dst) + o, static_cast<const char*>(c.src) + o,
+                                  std::min(kPiece, c.bytes - o)});
+    }
+    const size_t nt = std::min<size_t>({8, std::max(1u, std::thread::hardware_concurrency()), pieces.size()});
+    if (total < kPiece || nt <= 1) {
+        for (const Copy& c : pieces) std::memcpy(c.dst, c.src, c.bytes);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (size_t t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            for (size_t i = t; i < pieces.size(); i += nt) std::memcpy(pieces[i].dst, pieces[i].src, pieces[i].bytes);
+        });
+    for (auto& x : th) x.join();
+}
+}  // namespace
+
 double Server::now() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -349,10 +382,15 @@ void Server::serving_loop() {
         std::string err;
         try {
             std::fill(h_active_, h_active_ + slots_.size(), 0);
+            std::vector<Copy> in;
+            for (auto& tr : tick) {
+                Entry& e = *ent[tr.first];
+                in.push_back(Copy{e.h_den, tr.second.den, sizeof(float2) * e.spec.n});
+            }
+            parallel_copy(in);
             for (auto& tr : tick) {
                 const int i = tr.first;
                 Entry& e = *ent[i];
-                std::memcpy(e.h_den, tr.second.den, sizeof(float2) * e.spec.n);
                 SCK(cudaMemcpyAsync(batch_->den(i), e.h_den, sizeof(float2) * e.spec.n, cudaMemcpyHostToDevice,
                                     stream_));
                 h_active_[i] = 1;
@@ -365,10 +403,12 @@ void Server::serving_loop() {
                                     cudaMemcpyDeviceToHost, stream_));
             }
             batch_->check_error(stream_);  // synchronises the stream
+            std::vector<Copy> out;
             for (auto& tr : tick) {
                 Entry& e = *ent[tr.first];
-                std::memcpy(tr.second.val, e.h_val, sizeof(float2) * e.spec.n);
+                out.push_back(Copy{tr.second.val, e.h_val, sizeof(float2) * e.spec.n});
             }
+            parallel_copy(out);
         } catch (const std::exception& ex) {
             err = ex.what();
         }

@@ -4,7 +4,8 @@
 //
 // Continuous batching: the serving thread runs ticks.  A tick takes the
 // oldest pending request of every admitted session that has one, copies
-// their densities in, runs one masked batch matvec (Batch::run_graph: all of
+// their densities in (host copies into pinned staging split over up to 8
+// threads), runs one masked batch matvec (Batch::run_graph: all of
 // the tick's sessions in the same merged launches), copies the values out and
 // completes the requests.  Requests that arrive during a tick are taken by
 // the next one, so work of sessions that become busy at different times
