@@ -163,34 +163,72 @@ def measured_peaks():
         return {}
 
 
-def reference_sample(w, steps, timeout=600):
-    """Time the reference binary (oracle/_ref/ref_eval, built from the
-    reference's sources) on a bounded sample of the workload: the points of
-    the same sphere inside a 1/CAP_FRACTION spherical cap (z >= z0), same K,
-    P, NPQ, ptsmax and maxlevel.  One eval per process (the reference's eval
-    is not re-entrant).  Returns per-step eval seconds and the sample size."""
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
+def cap_directions(n):
+    """n directions spread over the sphere (golden-angle spiral): the centres
+    of the reference's sample caps."""
+    i = np.arange(n) + 0.5
+    z = 1.0 - 2.0 * i / n
+    r = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    phi = np.pi * (3.0 - np.sqrt(5.0)) * i
+    return np.stack([r * np.cos(phi), r * np.sin(phi), z], axis=1)
+
+
+def reference_step(w, nproc, timeout=900):
+    """One step of the reference arm: nproc processes at once, one per host
+    core, each running the reference binary (oracle/_ref/ref_eval, built from
+    the reference's sources; Wave3d::eval timed with a steady clock) on the
+    points of the workload's sphere inside a different 1/CAP_FRACTION
+    spherical cap, with the workload's K, P, NPQ, ptsmax, maxlevel and
+    operator files.  One eval per process (the reference's eval is not
+    re-entrant).  Returns (total sample points, the longest eval seconds)."""
+    from concurrent.futures import ThreadPoolExecutor
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import run_ref
     if not run_ref.available():
         raise RuntimeError("reference binary not built (make -C oracle)")
     pos, den = w.points(), w.densities()
-    R = np.abs(pos).max()
-    m = pos[:, 2] >= R * (1 - 2.0 / CAP_FRACTION)
+    R = np.linalg.norm(pos, axis=1).max()
     ld, hd = w.operators()
-    times = []
-    for _ in range(steps):
+    masks = [pos @ d >= R * (1 - 2.0 / CAP_FRACTION) for d in cap_directions(nproc)]
+
+    def one(m):
         r = run_ref.run(pos[m], den[m], K=w.K, accu=w.accu, kernel=w.kernel, nc=w.nc, maxlevel=w.maxlevel,
                         ld_path=ld, hd_path=hd, ptsmax=w.ptsmax, npq=w.npq, timeout=timeout)
-        times.append(r["eval_s"])
-    return times, int(m.sum())
+        return int(m.sum()), r["eval_s"]
+
+    with ThreadPoolExecutor(nproc) as ex:
+        res = list(ex.map(one, masks))
+    return sum(n for n, _ in res), max(t for _, t in res)
 
 
-def sample_desc(ns, w):
-    return ("reference Wave3d::eval (oracle/_ref, built from the reference sources; 1 process, 1 core: the "
-            "reference has no threads and no MPI is installed) on the points of the same K=%g sphere inside a "
-            "1/%d spherical cap (N_s=%d of %d, same P/NPQ/ptsmax/maxlevel), scaled to the full workload by point "
-            "count; the full workload costs more per point (longer far-field lists), so this favours the "
-            "reference" % (w.K, CAP_FRACTION, ns, w.N))
+def reference_procs():
+    return max(1, min(CAP_FRACTION, host_cores()))
+
+
+def sample_desc(w, nproc, npts):
+    return ("reference Wave3d::eval (oracle/_ref/ref_eval, the reference's own sources built with its "
+            "makeinc/wave4 flags against a one-rank MPI stand-in, an O(n^2) DFT stand-in for FFTW and naive "
+            "BLAS; it has no threads) in %d processes at once, one per host core, each on the points of the "
+            "workload's K=%g sphere inside a different 1/%d spherical cap (%d points in all per step, about %d "
+            "each; same P/NPQ/ptsmax/maxlevel/operators); points/s = those points / the longest eval. Per point "
+            "a cap is cheaper than the whole sphere (shorter far-field lists): one core took 2481 s for the "
+            "whole %d-point matvec (130 points/s, tests/golden/full)"
+            % (nproc, w.K, CAP_FRACTION, npts, npts // max(1, nproc), w.N))
+
+
+def bench_config(w):
+    """The config both arms report: the workload itself."""
+    return {"workload": w.name, "geometry": w.geometry, "K": w.K, "N": w.N, "P": w.P,
+            "kernel": "exp(ir)/r" if w.kernel == 0 else "exp(ir)", "npq": w.npq, "ptsmax": w.ptsmax,
+            "l2": "inputs larger than L2 (one matvec's device working set is many times the 126 MB L2; "
+                  "fresh densities each step, cycled over 4 inputs)"}
 
 
 def run_reference(args):
@@ -198,19 +236,21 @@ def run_reference(args):
     if rank != 0:
         return
     w = workload(args.workload)
-    times, ns = reference_sample(w, args.warmup + args.steps)
-    t = times[args.warmup:] if len(times) > args.warmup else times
-    sec = float(np.median(t))
-    mv = (ns / w.N) / sec  # full-workload matvecs per second at the sample's cost per point
-    line = {"metric": METRIC, "impl": "reference", "value": mv, "unit": "matvec/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec * w.N / ns,
+    nproc = reference_procs()
+    steps = []
+    for i in range(args.warmup + args.steps):
+        steps.append(reference_step(w, nproc))
+    timed = steps[args.warmup:] if len(steps) > args.warmup else steps
+    sec = float(np.median([t for _, t in timed]))
+    npts = timed[0][0]
+    pps = npts / sec
+    line = {"metric": METRIC, "impl": "reference", "value": pps, "unit": "points/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
-            "data": "synthetic", "points_per_sec": mv * w.N,
-            "config": {"workload": w.name, "geometry": w.geometry, "K": w.K, "N": w.N, "P": w.P,
-                       "kernel": "exp(ir)/r", "npq": w.npq, "ptsmax": w.ptsmax},
-            "cpu_baseline": {"value": mv, "unit": "matvec/s", "cores": 1, "kind": "reference",
-                             "sample": sample_desc(ns, w)},
-            "e2e": {"value": mv, "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic", "config": bench_config(w),
+            "cpu_baseline": {"value": pps, "unit": "points/s", "cores": nproc, "kind": "reference",
+                             "sample": sample_desc(w, nproc, npts)},
+            "e2e": {"value": pps, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -319,15 +359,8 @@ def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws, profile_json=None, 
 
 
 def instance_mix(Ks, seed0):
-    """Spheres and ellipsoids (alternating) of the given K, N = 25 pi K^2 points,
-    P=6, seeded: the instances of the batched and served configurations."""
-    from ddfmm_b200 import geometry, workloads as wl
-    out = []
-    for j, K in enumerate(Ks):
-        n = geometry.sphere_n_for(K)
-        seed = seed0 + j
-        out.append(wl.sphere(K, n, accu=2, seed=seed) if j % 2 == 0 else wl.ellipsoid(K, n, accu=2, seed=seed))
-    return out
+    from ddfmm_b200 import workloads as wl
+    return wl.instance_mix(Ks, seed0)
 
 
 def served_workloads():
@@ -598,7 +631,7 @@ def run_ours(args):
         torch.distributed.barrier()
     torch.cuda.synchronize(dev)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    wave.profile(True)
+    # the timed steps run as a caller runs them: no per-launch events
     with ClockSampler(local) as clk:
         for i in range(args.steps):
             with torch.cuda.stream(stream):
@@ -607,8 +640,6 @@ def run_ours(args):
             with torch.cuda.stream(stream):
                 ev[i][1].record(stream)
         stream.synchronize()
-    prof = wave.profile_read(reset=True)
-    wave.profile(False)
     torch.cuda.synchronize(dev)
     if ws > 1:
         torch.distributed.barrier()
@@ -616,6 +647,14 @@ def run_ours(args):
     total_ms = ev[0][0].elapsed_time(ev[-1][1])
     ms_per_step = max_over_ranks(total_ms / args.steps, ws, dev)
     value = whole_job_rate(ms_per_step, ws)
+    # per-pass profile from a separate pass of event-bracketed launches
+    prof_steps = 3
+    wave.profile(True)
+    for i in range(prof_steps):
+        wave.eval_device(den_d[i % n_inputs].data_ptr(), val_d.data_ptr(), sp)
+    stream.synchronize()
+    prof = wave.profile_read(reset=True)
+    wave.profile(False)
     # end to end through the public API with pinned host buffers ---------------
     den_h = torch.from_numpy(np.ascontiguousarray(den).view(np.float64)).pin_memory()
     val_h = torch.empty(2 * w.N, dtype=torch.float64).pin_memory()
@@ -657,19 +696,22 @@ def run_ours(args):
                 "frac": achieved / peak, "traffic": None,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
                 "launches": dk["launches"]}
-    passes = {lab: {"ms_per_step": e["ms"] / args.steps, "launches_per_step": e["launches"] / args.steps,
-                    "gflop_per_step": e["flops"] / args.steps / 1e9, "kernel": e["kernel"]}
+    passes = {lab: {"ms_per_step": e["ms"] / prof_steps, "launches_per_step": e["launches"] / prof_steps,
+                    "gflop_per_step": e["flops"] / prof_steps / 1e9, "kernel": e["kernel"]}
               for lab, e in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])}
-    launches = sum(e["launches"] for lab, e in prof.items() if e["kernel"] != "memset") + 2 * args.steps
+    # kernels of this library per matvec: the passes (memsets are not kernels) plus gather and scatter
+    launches_per_step = sum(e["launches"] for lab, e in prof.items() if e["kernel"] != "memset") // prof_steps + 2
     clocks = clk.summary()
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "large":
+        nproc = reference_procs()
         try:
-            times, ns = reference_sample(w, 1)
-            mv = (ns / w.N) / times[0]
-            cpu = {"value": mv, "unit": "matvec/s", "cores": 1, "kind": "reference", "sample": sample_desc(ns, w)}
+            npts, sec = reference_step(w, nproc)
+            cpu = {"value": npts / sec, "unit": "points/s", "cores": nproc, "kind": "reference",
+                   "sample": "one step: " + sample_desc(w, nproc, npts)}
         except Exception as ex:  # the reference binary travels with the tree; report when it does not
-            cpu = {"value": None, "unit": "matvec/s", "cores": 1, "kind": "reference", "sample": "unavailable: %s" % ex}
+            cpu = {"value": None, "unit": "points/s", "cores": nproc, "kind": "reference",
+                   "sample": "unavailable: %s" % ex}
     mixed = None
     if not args.no_mixed:
         mixed = measure_mixed(w, wave_args=(local,), steps=args.steps, warmup=args.warmup, dev=dev, chk=chk, ws=ws,
@@ -687,18 +729,18 @@ def run_ours(args):
     if args.profile_json and rank == 0:
         json.dump({"passes": passes, "by_kernel": by_kernel, "stats": st}, open(args.profile_json, "w"), indent=1)
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": ws, "steps": args.steps,
+        line = {"metric": METRIC, "value": value * w.N, "unit": "points/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-                "points_per_sec": value * w.N, "relerr_vs_fp64_direct": relerr,
+                "matvec_per_sec": value, "relerr_vs_fp64_direct": relerr,
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
-                "config": {"workload": w.name, "geometry": w.geometry, "K": w.K, "N": w.N, "P": w.P,
-                           "kernel": "exp(ir)/r", "npq": w.npq, "ptsmax": w.ptsmax, "form": "plain FP64",
-                           "l2": "inputs larger than L2 (device working set %.1f GB)" % (st["device_bytes"] / 1e9),
-                           "parallelism": "replicas" if ws > 1 else "single GPU", "setup_s": setup_s},
-                "e2e": {"value": whole_job_rate(1e3 * e2e_s, ws), "unit": "matvec/s", "h2d_bytes_per_step": 16 * w.N,
-                        "d2h_bytes_per_step": 16 * w.N, "rel_diff_vs_device_path": e2e_relerr},
-                "roofline": roof, "gpu_launches": int(round(launches / args.steps)) * args.steps,
+                "config": bench_config(w),
+                "form": "plain FP64", "parallelism": "replicas" if ws > 1 else "single GPU", "setup_s": setup_s,
+                "device_gb": st["device_bytes"] / 1e9,
+                "e2e": {"value": whole_job_rate(1e3 * e2e_s, ws) * w.N, "unit": "points/s",
+                        "h2d_bytes_per_step": 16 * w.N, "d2h_bytes_per_step": 16 * w.N,
+                        "matvec_per_sec": whole_job_rate(1e3 * e2e_s, ws), "rel_diff_vs_device_path": e2e_relerr},
+                "roofline": roof, "gpu_launches": int(launches_per_step * args.steps),
                 "clocks": clocks, "cpu_baseline": cpu, "mixed_form": mixed, "passes": passes}
         if mixed_mma:
             line["mixed_form_mma_sync"] = mixed_mma

@@ -241,6 +241,27 @@ int ddfmm_session_stats(const ddfmm_session* s, ddfmm_stats* out) {
     return DDFMM_OK;
 }
 
+int ddfmm_operators_check(const char* ld_path, const char* hd_path, int accu, int* n_ld_widths, int* n_hd_wedges) {
+    if (!ld_path || !hd_path) return fail(DDFMM_EINVAL, "operator file paths are required");
+    if (accu < 1 || accu > 3) return fail(DDFMM_EINVAL, "ACCU must be 1, 2 or 3");
+    return guarded([&] {
+        ddfmm::OperatorLib ops;
+        ops.load(ld_path, hd_path);
+        ops.validate(accu);
+        if (n_ld_widths) *n_ld_widths = (int)ops.ld.size();
+        if (n_hd_wedges) {
+            long long n = 0;
+            for (const auto& kv : ops.hd) n += (long long)kv.second.size();
+            *n_hd_wedges = (int)n;
+        }
+    });
+}
+
+int ddfmm_session_test_gemm_stall(ddfmm_session* s, double wait_s) {
+    if (!s || !s->impl) return fail(DDFMM_EINVAL, "NULL session");
+    return guarded([&] { s->impl->arm_gemm_stall(wait_s); });
+}
+
 int ddfmm_tree_stats(const double* pos3n, int n, double K, const double* ctr3, int ptsmax, int maxlevel, int ncell,
                      int npq, int* total_boxes, int* empty_boxes, int* nlevels, ddfmm_tree_level* levels) {
     if (!pos3n || n <= 0 || !total_boxes || !empty_boxes || !nlevels || !levels)

@@ -158,9 +158,10 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
-// Wait for the phase of parity `parity`; false after 1 s, 2^26 polls, or once
-// *failed is set by another role.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* failed) {
+// Wait for the phase of parity `parity`; false after limit_ns, 2^26 polls, or
+// once *failed is set by another role.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* failed,
+                                          unsigned long long limit_ns) {
     const uint32_t addr = smem_u32(bar);
     unsigned long long t0 = 0;
     for (uint32_t it = 0; it < U_WAIT_ITERS; ++it) {
@@ -178,7 +179,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
             const unsigned long long t = gtimer();
             if (t0 == 0)
                 t0 = t;
-            else if (t - t0 > U_WAIT_NS)
+            else if (t - t0 > limit_ns)
                 return false;
         }
     }
@@ -390,7 +391,8 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
                                                                  const UmmaSub* __restrict__ gsubs,
                                                                  const int* __restrict__ gprefix, int nsub,
                                                                  int ntiles, const int* __restrict__ active,
-                                                                 int* err) {
+                                                                 int* err, unsigned long long wait_ns,
+                                                                 int withhold) {
     extern __shared__ __align__(1024) unsigned char usm_raw[];
     __shared__ UmmaSub ssubs[MULTI ? U_SUBS_SMEM : 1];
     __shared__ int sprefix[MULTI ? U_SUBS_SMEM + 1 : 1];
@@ -500,7 +502,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
                 if (n >= loaded || *failed) break;
                 const int g = n * UPSETS + set;
                 const int s = g % USTAGES;
-                if (g >= USTAGES && !mbar_wait(&empty[s], ((g / USTAGES) - 1) & 1, failed)) {
+                if (g >= USTAGES && !mbar_wait(&empty[s], ((g / USTAGES) - 1) & 1, failed, wait_ns)) {
                     *failed = 1;
                     break;
                 }
@@ -531,7 +533,9 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
         }
     } else if (warp == W_LOAD_B) {
         // ------------------------------------------------ operator blocks
-        if (lane == 0) {
+        // withhold (failure-path test hook): block 0 issues no operator copy and no
+        // arrival at all, so its MMA issuer's bounded wait on full[0] runs out
+        if (lane == 0 && !(withhold && blockIdx.x == 0)) {
             int g = 0;
             for (int ti = blockIdx.x; ti < ntiles && !*failed; ti += gridDim.x) {
                 const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, active, ti);
@@ -540,7 +544,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
                 const uint32_t blk = (uint32_t)tile_n(T.t.rows) * UBK * 4;
                 for (int kb = 0; kb < T.p.nkb; ++kb, ++g) {
                     const int s = g % USTAGES;
-                    if (g >= USTAGES && !mbar_wait(&empty[s], ((g / USTAGES) - 1) & 1, failed)) {
+                    if (g >= USTAGES && !mbar_wait(&empty[s], ((g / USTAGES) - 1) & 1, failed, wait_ns)) {
                         *failed = 1;
                         break;
                     }
@@ -561,7 +565,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
                 if (!T.on) continue;
                 const uint32_t idesc = idesc_tf32(tile_n(T.t.rows));
                 const int acc = it & 1;
-                if (it >= 2 && !mbar_wait(&tmem_empty[acc], ((it >> 1) - 1) & 1, failed)) {
+                if (it >= 2 && !mbar_wait(&tmem_empty[acc], ((it >> 1) - 1) & 1, failed, wait_ns)) {
                     *failed = 1;
                     break;
                 }
@@ -569,7 +573,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
                 const uint32_t d = tmem + (uint32_t)(acc * 256);
                 for (int kb = 0; kb < T.p.nkb; ++kb, ++g) {
                     const int s = g % USTAGES;
-                    if (!mbar_wait(&full[s], (g / USTAGES) & 1, failed)) {
+                    if (!mbar_wait(&full[s], (g / USTAGES) & 1, failed, wait_ns)) {
                         *failed = 1;
                         break;
                     }
@@ -592,7 +596,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
                 ++it;
             }
             if (*failed && last >= 0)  // let the MMAs already issued finish before TMEM is freed
-                mbar_wait(&empty[last % USTAGES], (last / USTAGES) & 1, nullptr);
+                mbar_wait(&empty[last % USTAGES], (last / USTAGES) & 1, nullptr, wait_ns);
         }
     } else {
         // ------------------------------------------------ epilogue
@@ -620,7 +624,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
             const long long my_yo = mycol < ncol ? __ldg(T.yoff + T.p.col0 + T.t.col0 + mycol) + T.t.row0 : 0;
             float2* const Y = T.Y;
             const int mode = T.mode;
-            bool ok = !*failed && mbar_wait(&tmem_full[acc], (it >> 1) & 1, failed);
+            bool ok = !*failed && mbar_wait(&tmem_full[acc], (it >> 1) & 1, failed, wait_ns);
             ok = __all_sync(0xffffffffu, ok);  // tcgen05.ld is warp-collective
             if (!ok) {
                 *failed = 1;
@@ -688,15 +692,18 @@ void umma_init() {
 }
 
 void launch_umma_cgemm(const UmmaSub* subs, const int* prefix, int nsub, int ntiles, const int* active, int* err,
-                       cudaStream_t s, const UmmaSub* one) {
+                       cudaStream_t s, const UmmaSub* one, unsigned long long wait_ns, int withhold) {
     if (ntiles == 0) return;
     const int sms = g_umma_sms > 0 ? g_umma_sms : 148;
     const int grid = ntiles < sms ? ntiles : sms;
+    if (wait_ns == 0) wait_ns = U_WAIT_NS;
     if (nsub == 1) {
         if (!one) return;  // a single sub-launch is passed by value
-        umma_cgemm_kernel<false><<<grid, UTHREADS, UGEMM_SMEM, s>>>(*one, subs, prefix, nsub, ntiles, active, err);
+        umma_cgemm_kernel<false><<<grid, UTHREADS, UGEMM_SMEM, s>>>(*one, subs, prefix, nsub, ntiles, active, err,
+                                                                     wait_ns, withhold);
     } else {
-        umma_cgemm_kernel<true><<<grid, UTHREADS, UGEMM_SMEM, s>>>(UmmaSub{}, subs, prefix, nsub, ntiles, active, err);
+        umma_cgemm_kernel<true><<<grid, UTHREADS, UGEMM_SMEM, s>>>(UmmaSub{}, subs, prefix, nsub, ntiles, active, err,
+                                                                    wait_ns, withhold);
     }
 }
 

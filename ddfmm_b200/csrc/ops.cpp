@@ -124,6 +124,33 @@ void OperatorLib::load(const std::string& ld_path, const std::string& hd_path) {
     if (b.o != b.buf.size()) throw std::runtime_error("hd file has trailing bytes");
 }
 
+void OperatorLib::validate(int accu) const {
+    if (accu < 1 || accu > 3) throw std::invalid_argument("ACCU must be 1, 2 or 3");
+    const int P = accu == 1 ? 4 : (accu == 2 ? 6 : 8);
+    const int nE = P * P * P - (P - 2) * (P - 2) * (P - 2);
+    auto bad = [](const std::string& what, double W) {
+        std::ostringstream s;
+        s << what << " (width " << W << ")";
+        throw std::runtime_error(s.str());
+    };
+    for (const auto& kv : ld) {
+        const LowFreqOp& o = kv.second;
+        if (o.uep.n != nE || o.ucp.n != nE) bad("ld file: surfaces do not have P^3-(P-2)^3 points for this ACCU", kv.first);
+        const int r = o.v.n;
+        if (o.v.m != nE || o.is.m != r || o.is.n != 1 || o.up.m != r || o.up.n != nE)
+            bad("ld file: uc2ue factors have inconsistent shapes", kv.first);
+        if (o.tdim != 0 && o.tdim != 2 * P) bad("ld file: ue2dc tensors are not (2P)^3 for this ACCU", kv.first);
+    }
+    for (const auto& kv : hd)
+        for (const auto& dk : kv.second) {
+            const HighFreqOp& o = dk.second;
+            const int r1 = o.uep.n, r2 = o.ucp.n;
+            if (o.E1.m != r1 || o.E1.n != r1 || o.E2.m != r1 || o.E2.n != r2 || o.E3.m != r2 || o.E3.n != r2)
+                bad("hd file: E1/E2/E3 shapes do not match the skeleton point counts", kv.first);
+            if (r1 > 400 || r2 > 400) bad("hd file: skeleton rank exceeds DVMAX=400", kv.first);
+        }
+}
+
 const LowFreqOp& OperatorLib::low(double W) const {
     auto it = ld.find(W);
     if (it == ld.end()) {

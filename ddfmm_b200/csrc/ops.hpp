@@ -48,6 +48,12 @@ struct OperatorLib {
     std::map<double, LowFreqOp> ld;
     std::map<double, std::map<Idx3, HighFreqOp> > hd;
     void load(const std::string& ld_path, const std::string& hd_path);
+    // Shapes every entry must have for accuracy level `accu` (P = 4/6/8): LF
+    // surfaces of P^3 - (P-2)^3 points, uc2ue factors v (n x r), 1/sigma (r x 1),
+    // U^H (r x n), ue2dc tensors of edge 2P (or empty); HF factors E1 (r1 x r1),
+    // E2 (r1 x r2), E3 (r2 x r2) for r1 / r2 skeleton points, r1, r2 <= 400
+    // (DVMAX, src/wave3d_eval.cpp:25).  Throws with the first violation.
+    void validate(int accu) const;
     const LowFreqOp& low(double W) const;
     const HighFreqOp& high(double W, const Idx3& canon) const;
 };

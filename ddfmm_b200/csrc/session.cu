@@ -73,12 +73,14 @@ Session::Session(const double* pos3n, int n, const SessionParams& p, const std::
     : prm_(p), npts_(n) {
     if (n <= 0) throw std::runtime_error("no points");
     auto t0 = std::chrono::steady_clock::now();
-    CK(cudaSetDevice(p.device));
-    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-    pos_.assign(pos3n, pos3n + 3 * (size_t)n);
+    // operator files first (Mlib3d::setup): a bad file is reported before any device work
     ld_path_ = ld_path;
     hd_path_ = hd_path;
     ops_.load(ld_path, hd_path);
+    ops_.validate(p.accu);
+    CK(cudaSetDevice(p.device));
+    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    pos_.assign(pos3n, pos3n + 3 * (size_t)n);
     tree_.build(pos_.data(), n, p.tree);
     build();
     autotune();
@@ -256,6 +258,12 @@ void Session::check_device_error() {
         CK(cudaStreamSynchronize(stream_));
         throw std::runtime_error("CUDA error: a tensor-core GEMM block timed out waiting on its pipeline");
     }
+}
+
+void Session::arm_gemm_stall(double wait_s) {
+    if (!umma()) throw std::invalid_argument("the GEMM stall hook needs a DDFMM_MIXED (tcgen05) session");
+    if (!(wait_s > 0 && wait_s <= 1.0)) throw std::invalid_argument("stall wait must be in (0, 1] seconds");
+    stall_wait_ns_ = (unsigned long long)(wait_s * 1e9);
 }
 
 const char* Session::width_label(const char* pass, double W) {
@@ -1438,9 +1446,13 @@ void Session::launch_step(const Step& st, cudaStream_t s, double2* spec) {
         case 4:
             CK(cudaMemsetAsync(st.ms.p, 0, st.ms.bytes, s));
             break;
-        case 5:
-            launch_umma_cgemm(static_cast<const UmmaSub*>(st.msubs), st.mpre, 1, st.mtotal, nullptr, d_err_, s, &st.hu);
+        case 5: {
+            const unsigned long long wait_ns = stall_wait_ns_;
+            stall_wait_ns_ = 0;  // one launch only
+            launch_umma_cgemm(static_cast<const UmmaSub*>(st.msubs), st.mpre, 1, st.mtotal, nullptr, d_err_, s, &st.hu,
+                              wait_ns, wait_ns ? 1 : 0);
             break;
+        }
     }
 }
 

@@ -59,6 +59,11 @@ public:
     // Throws if a tensor-core GEMM gave up waiting on its pipeline since the last
     // check (the flag is reset); synchronises the session's stream.
     void check_device_error();
+    // Failure-path test hook (tcgen05 sessions): the next eval's first
+    // tensor-core GEMM launch runs with its pipeline waits bounded by wait_s and
+    // withholds the operator copies of its block 0, so that block's wait runs
+    // out and the session reports the timeout at its next synchronous call.
+    void arm_gemm_stall(double wait_s);
     // Same matvec with the V-list spectra in caller-provided scratch of
     // `capacity` double2 (must hold spectra_elems()); nothing is allocated.
     void eval_device_scratch(const double2* den, double2* val, cudaStream_t s, double2* spec, size_t capacity);
@@ -190,6 +195,7 @@ private:
     double2* d_val_io_ = nullptr;
     std::vector<Memset> zero_at_start_;
     int* d_err_ = nullptr;  // set by a tensor-core GEMM that timed out
+    unsigned long long stall_wait_ns_ = 0;  // armed failure-path hook (0: none)
     std::map<std::pair<const void*, long long>, const float*> packed_;  // (operator, m k) -> packed copy
     std::vector<UmmaPackJob> pack_jobs_;                                 // packing still to launch
     // packed operators (tcgen05 form): the chunk being filled, the operators this

@@ -91,6 +91,18 @@ def cluster(K, N, accu=1, kernel=0, seed=0, ptsmax=8):
                     "cluster", float(K), int(N), accu, kernel, ptsmax, 4, seed)
 
 
+def instance_mix(Ks, seed0, accu=2):
+    """Spheres and ellipsoids (alternating) of the given K, N = 25 pi K^2
+    points, P=6 by default, seeded from seed0 on: the instances of the
+    batched (64 uneven instances) and served (16 sessions) configurations."""
+    out = []
+    for j, K in enumerate(Ks):
+        n = geometry.sphere_n_for(K)
+        seed = seed0 + j
+        out.append(sphere(K, n, accu=accu, seed=seed) if j % 2 == 0 else ellipsoid(K, n, accu=accu, seed=seed))
+    return out
+
+
 # the small plain-method case the reference binary runs in seconds
 SMALL = sphere(8, 5000, accu=1)
 # the large single instance (about 25 points per square wavelength)

@@ -94,21 +94,28 @@ int ddfmm_eval_device_c64(ddfmm_session* s, const void* den_dev, void* val_dev, 
  * own stream.  Returns after enqueueing; the caller synchronises. */
 int ddfmm_eval_device(ddfmm_session* s, const void* den_dev, void* val_dev, void* stream);
 
-/* No counterpart in the reference.  ddfmm_eval_device for callers that must
- * not allocate device memory per call site, e.g. code that owns a fixed
- * device-memory budget or records its matvecs into a CUDA graph, where the
- * per-eval V-list spectra cannot come from a growing pool.  The spectra (one
- * (2P)^3 complex FFT per low-frequency box) go to one fixed, statically sized
- * device array of 16 MiB that every GPU loading this library holds until the
- * process exits; nothing else changes and the call allocates nothing.
- * Limits and rules:
+/* No counterpart in the reference.  ddfmm_eval_device for callers that
+ * cannot allocate device memory while they run: a solver embedded in a host
+ * application whose own allocator owns all of the GPU's memory (cudaMalloc
+ * there fails or is forbidden once the application has started), or a
+ * real-time loop with a device-memory budget fixed up front, where an
+ * allocation at the call would break the budget or stall on the driver.
+ * The session's per-eval V-list spectra (one (2P)^3 complex FFT per
+ * low-frequency box) go to one fixed, statically sized device array of
+ * 16 MiB that every GPU loading this library holds until the process exits,
+ * instead of session memory; nothing else changes and the call allocates
+ * nothing.  Limits and rules:
  *  - sessions whose spectra exceed 16 MiB (about 2000 low-frequency boxes at
  *    ACCU 1, 600 at ACCU 2, 250 at ACCU 3) get DDFMM_EINVAL and a message;
  *  - the first call on each device resolves the array's device address
- *    (cudaGetSymbolAddress) with that device current: make it before any
- *    stream capture;
+ *    (cudaGetSymbolAddress) with that device current and keeps it for the
+ *    life of the process; a cudaDeviceReset invalidates it, so do not use
+ *    this call after resetting a device;
  *  - every call and every session on a device share the one array: calls
- *    whose work overlaps on the GPU race (use one stream, or serialise);
+ *    whose work overlaps on the GPU race.  stream == NULL means the session's
+ *    own private stream, so two sessions both called with NULL overlap: with
+ *    several sessions, pass one explicit shared stream, or synchronise between
+ *    calls;
  *  - each call writes every spectrum it reads, so no zeroing is needed and a
  *    previous call's leftovers are never used.
  * den_dev / val_dev / stream as in ddfmm_eval_device. */
@@ -119,6 +126,25 @@ int ddfmm_eval_device_noalloc(ddfmm_session* s, const void* den_dev, void* val_d
 int ddfmm_direct(ddfmm_session* s, const double* den, const int* ids, int nids, double* out);
 
 int ddfmm_session_stats(const ddfmm_session* s, ddfmm_stats* out);
+
+/* Host-only (no GPU): Mlib3d::setup (src/mlib3d.cpp:70-103) without a
+ * session -- read the ld / hd operator files and check every entry's shapes
+ * against accuracy level accu (surfaces of P^3-(P-2)^3 points, uc2ue factor
+ * shapes, ue2dc tensors of edge 2P, E1/E2/E3 against the skeleton counts,
+ * ranks <= 400).  DDFMM_ESETUP for an unreadable, truncated, trailing-byte
+ * or inconsistent file (the reference throws from deserialize or a CHECK
+ * there); DDFMM_EINVAL for bad arguments.  Optional outputs: the number of
+ * low-frequency widths and of (width, canonical wedge) entries. */
+int ddfmm_operators_check(const char* ld_path, const char* hd_path, int accu, int* n_ld_widths, int* n_hd_wedges);
+
+/* Failure-path test hook, no counterpart in the reference.  On a DDFMM_MIXED
+ * session: the next eval's first tensor-core GEMM launch bounds its pipeline
+ * waits by wait_s (0 < wait_s <= 1) and its first block withholds the copies
+ * that block waits on, so that wait runs out; the block then drains its work,
+ * frees its tensor memory and flags the session, whose next synchronous call
+ * (ddfmm_eval and the like) returns DDFMM_ECUDA.  Nothing faults and the
+ * context stays usable.  DDFMM_EINVAL on other sessions. */
+int ddfmm_session_test_gemm_stall(ddfmm_session* s, double wait_s);
 
 /* Host-only (no GPU): build the octree and interaction lists of
  * Wave3d::setup (src/wave3d_setup.cpp:100-299) and report, per level, what

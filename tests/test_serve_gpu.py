@@ -144,3 +144,66 @@ def test_admission_by_device_memory_budget(cases):
     sa = _add(sv, a)
     assert sv.wait_admitted([sa]) == [sv.REJECTED]
     sv.close()
+
+
+def test_k64_sphere_in_the_mix():
+    """The served configuration's largest session -- the K=64 sphere, 321,699
+    points -- admitted under the 30 GB budget next to K=8, 16 and 32 sessions:
+    bursts and random arrivals from one client per session, every result
+    equal to the same session's matvec evaluated alone."""
+    from ddfmm_b200 import workloads as wl
+    ws = [wl.LARGE] + wl.instance_mix([8, 16, 32], 1)
+    rng = np.random.default_rng(17)
+    dens = [[(rng.standard_normal(w.N) + 1j * rng.standard_normal(w.N)).astype(np.complex64) for _ in range(3)]
+            for w in ws]
+    alone = []
+    for w, ds in zip(ws, dens):
+        m = wave3d.from_workload(w, precision=_lib.MIXED)
+        out = []
+        for d in ds:
+            v = np.zeros(w.N, dtype=np.complex64)
+            m.eval(d, v)
+            out.append(v)
+        m.close()
+        alone.append(out)
+    sv = wave3d.Server(budget_bytes=30e9)
+    sids = [sv.add_workload(w) for w in ws]
+    assert sv.wait_admitted(sids) == [sv.ADMITTED] * len(sids)
+    vals, tickets = {}, []
+    for k, sid in enumerate(sids):
+        for r, d in enumerate(dens[k]):
+            v = np.zeros(len(d), dtype=np.complex64)
+            vals[(k, r)] = v
+            tickets.append(sv.submit(sid, d, v))
+    for t in tickets:
+        assert sv.wait(t, 120.0)
+    burst = sv.stats(reset=True)
+    print("K=64 mix burst: %d requests in %d ticks (mean batch %.2f), p50 %.2f ms p99 %.2f ms"
+          % (burst["requests"], burst["ticks"], burst["mean_batch"], burst["p50_ms"], burst["p99_ms"]))
+    assert burst["mean_batch"] >= 2.0
+    for (k, r), v in vals.items():
+        assert _rel(v, alone[k][r]) <= TOL, (k, r, _rel(v, alone[k][r]))
+    errs = []
+
+    def client(k, sid):
+        crng = np.random.default_rng(200 + k)
+        for rep in range(2):
+            for r, d in enumerate(dens[k]):
+                time.sleep(crng.exponential(0.005))
+                v = np.zeros(len(d), dtype=np.complex64)
+                if not sv.wait(sv.submit(sid, d, v), 120.0):
+                    errs.append((k, r, "timeout"))
+                    continue
+                if _rel(v, alone[k][r]) > TOL:
+                    errs.append((k, r, _rel(v, alone[k][r])))
+
+    th = [threading.Thread(target=client, args=(k, sid)) for k, sid in enumerate(sids)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    mix = sv.stats()
+    print("K=64 mix random arrivals: %d requests, mean batch %.2f, p50 %.2f ms p99 %.2f ms"
+          % (mix["requests"], mix["mean_batch"], mix["p50_ms"], mix["p99_ms"]))
+    assert not errs, errs
+    sv.close()
