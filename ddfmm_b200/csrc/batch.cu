@@ -111,7 +111,7 @@ Batch::Batch(const std::vector<Session*>& sessions) : sessions_(sessions) {
                     for (auto& e : kk.second) tpi = std::max(tpi, e.second->tpi ? e.second->tpi : 32);
                     launches_.back().tpi = tpi;
                 }
-            } else if (kind == 2 || kind == 3) {
+            } else if (kind == 2 || kind == 3 || kind == 6) {
                 // V-list launches are templated on the grid size: one launch per G
                 std::map<int, std::vector<std::pair<int, const Session::Step*> > > by_g;
                 for (auto& e : kk.second) by_g[e.second->v.L.G].push_back(e);
@@ -126,16 +126,26 @@ Batch::Batch(const std::vector<Session*>& sessions) : sessions_(sessions) {
                             n.push_back(u.nbox);
                         }
                         add(VFWD, subs, n, gg.first);
-                    } else {
+                    } else if (kind == 3) {
                         std::vector<VaSub> subs;
                         std::vector<int> n;
                         for (auto& e : gg.second) {
                             VaSub u = e.second->hva;
                             u.inst = e.first;
                             subs.push_back(u);
-                            n.push_back(u.ntrg);
+                            n.push_back(u.ngroups);
                         }
                         add(VACC, subs, n, gg.first);
+                    } else {
+                        std::vector<ViSub> subs;
+                        std::vector<int> n;
+                        for (auto& e : gg.second) {
+                            ViSub u = e.second->hvi;
+                            u.inst = e.first;
+                            subs.push_back(u);
+                            n.push_back(u.ntrg);
+                        }
+                        add(VINV, subs, n, gg.first);
                     }
                 }
             } else if (kind == 4) {
@@ -202,8 +212,12 @@ void Batch::run(const int* active, cudaStream_t s) {
                                        (int)L.total, L.G, active, nullptr, s, L.nsub == 1 ? reinterpret_cast<const VfSub*>(L.one) : nullptr);
                 break;
             case VACC:
-                launch_vlist_accum32(static_cast<const VaSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub,
+                launch_vlist_group32(static_cast<const VaSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub,
                                      (int)L.total, L.G, active, nullptr, s, L.nsub == 1 ? reinterpret_cast<const VaSub*>(L.one) : nullptr);
+                break;
+            case VINV:
+                launch_vlist_inverse32(static_cast<const ViSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub,
+                                       (int)L.total, L.G, active, s, L.nsub == 1 ? reinterpret_cast<const ViSub*>(L.one) : nullptr);
                 break;
         }
     }

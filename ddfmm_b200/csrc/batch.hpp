@@ -41,7 +41,7 @@ public:
     void check_error(cudaStream_t s);
 
 private:
-    enum Kind { ZERO, GATHER, SCATTER, GEMM, PT, VFWD, VACC };
+    enum Kind { ZERO, GATHER, SCATTER, GEMM, PT, VFWD, VACC, VINV };
     struct Launch {
         Kind kind;
         void* subs;

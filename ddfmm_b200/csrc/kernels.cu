@@ -86,10 +86,13 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(c[0]), "+d"(c[1])
-                 : "d"(a), "d"(b));
+// D (16 x 8) += A (16 x 8, rows g and g + 8 at k = tig and tig + 4) * B (8 x 8,
+// k = tig and tig + 4 at column g); D element q: row g + 8 (q >> 1), column 2 tig + (q & 1)
+__device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
 __global__ void __launch_bounds__(256, 2) zgemm_kernel(const GemmProblem* __restrict__ probs,
@@ -130,11 +133,12 @@ __global__ void __launch_bounds__(256, 2) zgemm_kernel(const GemmProblem* __rest
             cp_async16(&Xs[col * BKP + kk], ok ? (const void*)(X + xo[col] + gk) : (const void*)X, ok ? 16 : 0);
         }
     };
-    double cr[2][4][2], ci[2][4][2], cs[2][4][2];
+    // accumulators of the four 16x8 output blocks j: element q = 2h + e is row g + 8h, column 2 tig + e
+    double cr[4][4], ci[4][4], cs[4][4];
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 4; ++j)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = cs[i][j][0] = cs[i][j][1] = 0.0;
+        for (int q = 0; q < 4; ++q) cr[j][q] = ci[j][q] = cs[j][q] = 0.0;
     const int nk = (p.k + BK - 1) / BK;
 #pragma unroll
     for (int s = 0; s < GSTAGES - 1; ++s) {
@@ -153,30 +157,38 @@ __global__ void __launch_bounds__(256, 2) zgemm_kernel(const GemmProblem* __rest
             const double2* As = gsm + (it % GSTAGES) * GSTAGE + tig * BM + ((wm * 16 + g) ^ (tig << 1));
             const double2* Xs = gsm + (it % GSTAGES) * GSTAGE + BK * BM + (wn * 32 + g) * BKP + tig;
 #pragma unroll
-            for (int ks = 0; ks < BK / 4; ++ks) {
-                double2 a[2], b[4];
+            for (int ks = 0; ks < BK / 8; ++ks) {
+                // m16n8k8 fragments: A rows g, g+8 at k = tig, tig + 4; B k = tig, tig + 4 at column g
+                double2 a[4], b[4][2];
 #pragma unroll
-                for (int i = 0; i < 2; ++i) a[i] = As[ks * 4 * BM + i * 8];
+                for (int q = 0; q < 4; ++q) a[q] = As[(ks * 8 + 4 * (q >> 1)) * BM + 8 * (q & 1)];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) b[j] = Xs[j * 8 * BKP + ks * 4];
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) b[j][h] = Xs[j * 8 * BKP + ks * 8 + 4 * h];
                 // three real products: cr = ArXr, ci = AiXi, cs = (Ar+Ai)(Xr+Xi)
+                double ar[4], ai[4], as[4];
 #pragma unroll
-                for (int i = 0; i < 2; ++i)
+                for (int q = 0; q < 4; ++q) {
+                    ar[q] = a[q].x;
+                    ai[q] = a[q].y;
+                    as[q] = a[q].x + a[q].y;
+                }
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) dmma(cr[i][j], a[i].x, b[j].x);
+                for (int j = 0; j < 4; ++j) {
+                    const double br[2] = {b[j][0].x, b[j][1].x};
+                    dmma16(cr[j], ar, br);
+                }
 #pragma unroll
-                for (int i = 0; i < 2; ++i)
+                for (int j = 0; j < 4; ++j) {
+                    const double bi[2] = {b[j][0].y, b[j][1].y};
+                    dmma16(ci[j], ai, bi);
+                }
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) dmma(ci[i][j], a[i].y, b[j].y);
-                double as[2], bs[4];
-#pragma unroll
-                for (int i = 0; i < 2; ++i) as[i] = a[i].x + a[i].y;
-#pragma unroll
-                for (int j = 0; j < 4; ++j) bs[j] = b[j].x + b[j].y;
-#pragma unroll
-                for (int i = 0; i < 2; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) dmma(cs[i][j], as[i], bs[j]);
+                for (int j = 0; j < 4; ++j) {
+                    const double bs[2] = {b[j][0].x + b[j][0].y, b[j][1].x + b[j][1].y};
+                    dmma16(cs[j], as, bs);
+                }
             }
         }
     }
@@ -193,7 +205,8 @@ __global__ void __launch_bounds__(256, 2) zgemm_kernel(const GemmProblem* __rest
             for (int i = 0; i < 2; ++i) {
                 int row = wm * 16 + i * 8 + g;
                 if (row >= rows) continue;
-                double2 v = make_double2(cr[i][j][e] - ci[i][j][e], cs[i][j][e] - cr[i][j][e] - ci[i][j][e]);
+                const int q = 2 * i + e;
+                double2 v = make_double2(cr[j][q] - ci[j][q], cs[j][q] - cr[j][q] - ci[j][q]);
                 if (mode == GEMM_SET) {
                     y[row] = v;
                 } else if (mode == GEMM_ADD) {
@@ -312,34 +325,62 @@ __global__ void vlist_forward_kernel(VlistLevel L, const int* __restrict__ boxes
     }
 }
 
+// The pointwise products of the V list, by target parent: warp w of a block
+// takes target parent blockIdx.x * VGROUP_WARPS + w and lane l frequency
+// 32 blockIdx.y + l of the G^3 grid, with one accumulator per child position.
+// The loop over the parent's source entries is the same for the 32 lanes, so
+// the child mask branches are warp-uniform; a source's spectrum value is
+// loaded once and used by every child that has it in its V list.  Blocks of
+// one frequency chunk run together (blockIdx.x varies fastest), so the
+// translation tensors' 32-frequency slices of that chunk (316 x 512 bytes)
+// stay in the SM's L1 while the chunk lasts, and the source spectra's slices
+// (32 MB over all boxes at the bench workload) in L2.
+__host__ __device__ constexpr int child_voff(int c) { return ((c >> 2) & 1) + 7 * ((c >> 1) & 1) + 49 * (c & 1); }
+
 template <int G>
-__global__ void __launch_bounds__(256) vlist_accum_kernel(VlistLevel L, const int* __restrict__ trg,
-                                                          const int* __restrict__ vptr, const int* __restrict__ vsrc,
-                                                          const int* __restrict__ voff,
+__global__ void __launch_bounds__(256) vlist_group_kernel(const int* __restrict__ gptr, const int2* __restrict__ gsrc,
+                                                          const int* __restrict__ gtrg, int ngroups,
                                                           const double2* __restrict__ spec,
-                                                          double2* __restrict__ dnchk, const double2* __restrict__ twb) {
+                                                          const double2* __restrict__ tns, double2* __restrict__ tsp) {
+    constexpr int G3 = G * G * G;
+    const int grp = blockIdx.x * VGROUP_WARPS + (threadIdx.x >> 5);
+    if (grp >= ngroups) return;
+    const int f = blockIdx.y * 32 + (threadIdx.x & 31);
+    double2 acc[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[c] = make_double2(0.0, 0.0);
+    const int e1 = __ldg(gptr + grp + 1);
+    for (int e = __ldg(gptr + grp); e < e1; ++e) {
+        const int2 ent = __ldg(gsrc + e);
+        const double2 S = __ldg(spec + (size_t)ent.x * G3 + f);
+        const int mask = ent.y & 255;
+        const double2* tb = tns + (size_t)(ent.y >> 8) * G3 + f;
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+            if (mask & (1 << c)) cfma(acc[c], __ldg(tb + (size_t)child_voff(c) * G3), S);
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const int t = __ldg(gtrg + 8 * grp + c);
+        if (t >= 0) tsp[(size_t)t * G3 + f] = acc[c];
+    }
+}
+
+// Pruned inverse DFT of one target's summed spectrum (one block per target):
+// G^2 P, G P^2 and P^3 outputs of G-term sums, then the corner-cube nodes
+// scaled by 1/G^3 are added into the target's check values.
+template <int G>
+__global__ void __launch_bounds__(256) vlist_inverse_kernel(VlistLevel L, const int* __restrict__ trg,
+                                                            const double2* __restrict__ tsp,
+                                                            double2* __restrict__ dnchk,
+                                                            const double2* __restrict__ twb) {
     extern __shared__ double2 sm[];
-    constexpr int P = G / 2, PP = P * P, G3 = G * G * G, NE = (G3 + 255) / 256;
-    double2* grid = sm;          // G^3 accumulated spectrum, later [c'][b'][ka]
+    constexpr int P = G / 2, PP = P * P, G3 = G * G * G;
+    double2* grid = sm;          // G^3 summed spectrum, later [c'][b'][ka]
     double2* c1 = sm + G3;       // [c'][kb][ka], later the P^3 cube
     const int ti = blockIdx.x, t = trg[ti];
-    double2 acc[NE];
-#pragma unroll
-    for (int q = 0; q < NE; ++q) acc[q] = make_double2(0.0, 0.0);
-    for (int v = vptr[ti]; v < vptr[ti + 1]; ++v) {
-        const double2* sp = spec + (size_t)vsrc[v] * G3;
-        const double2* tn = L.tns + (size_t)voff[v] * G3;
-#pragma unroll
-        for (int q = 0; q < NE; ++q) {
-            int e = threadIdx.x + 256 * q;
-            if (e < G3) cfma(acc[q], __ldg(sp + e), __ldg(tn + e));
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < NE; ++q) {
-        int e = threadIdx.x + 256 * q;
-        if (e < G3) grid[e] = acc[q];
-    }
+    const double2* src = tsp + (size_t)ti * G3;
+    for (int e = threadIdx.x; e < G3; e += blockDim.x) grid[e] = __ldg(src + e);
     __syncthreads();
     for (int e = threadIdx.x; e < G * G * P; e += blockDim.x) {  // z: outputs c' < P
         int kab = e % (G * G), c = e / (G * G);
@@ -373,14 +414,14 @@ __global__ void __launch_bounds__(256) vlist_accum_kernel(VlistLevel L, const in
 }
 
 static size_t vfwd_smem(int G, int P) { return sizeof(double2) * (P * P * P + G * P * P + G * G * P); }
-static size_t vacc_smem(int G, int P) { return sizeof(double2) * (G * G * G + G * G * P); }
+static size_t vinv_smem(int G, int P) { return sizeof(double2) * (G * G * G + G * G * P); }
 
 void vlist_init(int G) {
     int P = G / 2;
     cudaFuncSetAttribute(vlist_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vfwd_smem(G, P));
-    cudaFuncSetAttribute(vlist_accum_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vacc_smem(8, 4));
-    cudaFuncSetAttribute(vlist_accum_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vacc_smem(12, 6));
-    cudaFuncSetAttribute(vlist_accum_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vacc_smem(16, 8));
+    cudaFuncSetAttribute(vlist_inverse_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vinv_smem(8, 4));
+    cudaFuncSetAttribute(vlist_inverse_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vinv_smem(12, 6));
+    cudaFuncSetAttribute(vlist_inverse_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vinv_smem(16, 8));
 }
 
 void launch_vlist_forward(const VlistLevel& L, const int* boxes, int nbox, const double2* upeq, double2* spec,
@@ -389,14 +430,26 @@ void launch_vlist_forward(const VlistLevel& L, const int* boxes, int nbox, const
     vlist_forward_kernel<<<nbox, 256, vfwd_smem(L.G, L.P), s>>>(L, boxes, upeq, spec, L.twf);
 }
 
-void launch_vlist_accum(const VlistLevel& L, const int* trg, int ntrg, const int* vptr, const int* vsrc,
-                        const int* voff, const double2* spec, double2* dnchk, cudaStream_t s) {
-    if (ntrg == 0) return;
-    size_t sm = vacc_smem(L.G, L.P);
+void launch_vlist_group(const VlistLevel& L, const VlistGroups& V, const double2* spec, double2* tsp,
+                        cudaStream_t s) {
+    if (V.ngroups == 0) return;
+    const dim3 grid((V.ngroups + VGROUP_WARPS - 1) / VGROUP_WARPS, L.G * L.G * L.G / 32);
     switch (L.G) {
-        case 8: vlist_accum_kernel<8><<<ntrg, 256, sm, s>>>(L, trg, vptr, vsrc, voff, spec, dnchk, L.twb); break;
-        case 12: vlist_accum_kernel<12><<<ntrg, 256, sm, s>>>(L, trg, vptr, vsrc, voff, spec, dnchk, L.twb); break;
-        case 16: vlist_accum_kernel<16><<<ntrg, 256, sm, s>>>(L, trg, vptr, vsrc, voff, spec, dnchk, L.twb); break;
+        case 8: vlist_group_kernel<8><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
+        case 12: vlist_group_kernel<12><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
+        case 16: vlist_group_kernel<16><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
+        default: break;
+    }
+}
+
+void launch_vlist_inverse(const VlistLevel& L, const int* trg, int ntrg, const double2* tsp, double2* dnchk,
+                          cudaStream_t s) {
+    if (ntrg == 0) return;
+    const size_t sm = vinv_smem(L.G, L.P);
+    switch (L.G) {
+        case 8: vlist_inverse_kernel<8><<<ntrg, 256, sm, s>>>(L, trg, tsp, dnchk, L.twb); break;
+        case 12: vlist_inverse_kernel<12><<<ntrg, 256, sm, s>>>(L, trg, tsp, dnchk, L.twb); break;
+        case 16: vlist_inverse_kernel<16><<<ntrg, 256, sm, s>>>(L, trg, tsp, dnchk, L.twb); break;
         default: break;
     }
 }

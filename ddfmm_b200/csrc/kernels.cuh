@@ -77,9 +77,28 @@ struct VlistLevel {
 void vlist_init(int G);
 void launch_vlist_forward(const VlistLevel& L, const int* boxes, int nbox, const double2* upeq,
                           double2* spec, cudaStream_t s);
-void launch_vlist_accum(const VlistLevel& L, const int* trg, int ntrg, const int* vptr,
-                        const int* vsrc, const int* voff, const double2* spec, double2* dnchk,
+// The V-list sums in Fourier space, by target parent: the target boxes of a
+// level are grouped by their parent (the groups in Morton order of the
+// parents); a group lists the union of its targets' V-list sources, each as
+//   {spectrum row of the source, (tbase << 8) | mask}
+// where bit c of mask says that the child at position c = 4a + 2b + c' of
+// the parent (offset (a, b, c') from twice the parent's index) has the
+// source in its V list, and tbase is the translation-tensor index of that
+// pair for child position 0; child position c adds a + 7b + 49c'.
+// tsp[t] (G^3 per target, rows in group order) receives the summed spectrum
+// of target t, overwritten each eval.
+constexpr int VGROUP_WARPS = 8;  // target parents per block of the accumulation
+struct VlistGroups {
+    const int* gptr;   // ngroups + 1: the source entries of each group
+    const int2* gsrc;  // the source entries
+    const int* gtrg;   // ngroups x 8: row of tsp of each child position, -1 where none
+    int ngroups;
+};
+void launch_vlist_group(const VlistLevel& L, const VlistGroups& V, const double2* spec, double2* tsp,
                         cudaStream_t s);
+// dnchk[trg[t]] += pruned inverse DFT of tsp[t] / G^3 at the corner-cube nodes
+void launch_vlist_inverse(const VlistLevel& L, const int* trg, int ntrg, const double2* tsp, double2* dnchk,
+                          cudaStream_t s);
 
 // mixed-precision form (kernels_mixed.cu): complex FP32 data behind the same
 // descriptors; GemmProblem::A, PtItem::out, PtSrc::den and VlistLevel::tns /
@@ -111,13 +130,20 @@ struct VfSub {  // V-list source spectra, one work item per source box
     int nbox;
     int inst;
 };
-struct VaSub {  // V-list accumulation, one work item per target box
+struct VaSub {  // V-list sums by target parent (VlistGroups), one work item per group
+    VlistLevel L;
+    const int* gptr;
+    const int2* gsrc;
+    const int* gtrg;
+    const float2* spec;
+    float2* tsp;
+    int ngroups;
+    int inst;
+};
+struct ViSub {  // V-list inverse transforms, one work item per target box
     VlistLevel L;
     const int* trg;
-    const int* vptr;
-    const int* vsrc;
-    const int* voff;
-    const float2* spec;
+    const float2* tsp;
     float2* dnchk;
     int ntrg;
     int inst;
@@ -142,8 +168,11 @@ void vlist32_init(int G);
 // a kernel parameter); `subs` / `prefix` are then not read.
 void launch_vlist_forward32(const VfSub* subs, const int* prefix, int nsub, int nbox, int G, const int* active,
                             void* spec_override, cudaStream_t s, const VfSub* one);
-void launch_vlist_accum32(const VaSub* subs, const int* prefix, int nsub, int ntrg, int G, const int* active,
+// work items: groups (launch_vlist_group32) or targets (launch_vlist_inverse32)
+void launch_vlist_group32(const VaSub* subs, const int* prefix, int nsub, int ngroups, int G, const int* active,
                           const void* spec_override, cudaStream_t s, const VaSub* one);
+void launch_vlist_inverse32(const ViSub* subs, const int* prefix, int nsub, int ntrg, int G, const int* active,
+                            cudaStream_t s, const ViSub* one);
 void launch_move32(const MoveSub* subs, const int* prefix, int nsub, int n, const int* active, int scatter,
                    cudaStream_t s);
 void launch_zero(const ZeroSub* subs, const long long* prefix, int nsub, long long n8, const int* active,

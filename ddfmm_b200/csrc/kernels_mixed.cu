@@ -356,59 +356,66 @@ __device__ __forceinline__ void vlist_forward32_body(const VfSub& S, int local, 
     }
 }
 
-template <int G>
-__device__ __forceinline__ void vlist_accum32_body(const VaSub& S, int local, const float2* spec_override);
+// V-list sums by target parent (see vlist_group_kernel in kernels.cu): warp =
+// one group (target parent), lane = one frequency of a 32-frequency chunk
+// (blockIdx.y).  MULTI: each warp finds its own sub-launch from the prefix
+// sums of the groups; spec_override replaces the source spectra (single
+// instance).
+__host__ __device__ constexpr int child_voff32(int c) { return ((c >> 2) & 1) + 7 * ((c >> 1) & 1) + 49 * (c & 1); }
 
 template <int G, bool MULTI>
-__global__ void __launch_bounds__(256) vlist_accum32_kernel(const VaSub one, const VaSub* __restrict__ subs,
-                                                            const int* __restrict__ prefix, int nsub,
+__global__ void __launch_bounds__(256) vlist_group32_kernel(const VaSub one, const VaSub* __restrict__ subs,
+                                                            const int* __restrict__ prefix, int nsub, int ngroups,
                                                             const int* __restrict__ active,
                                                             const float2* spec_override) {
-    if (!MULTI) {
-        vlist_accum32_body<G>(one, blockIdx.x, spec_override);
-        return;
+    constexpr int G3 = G * G * G;
+    const int g = blockIdx.x * VGROUP_WARPS + (threadIdx.x >> 5);
+    if (g >= ngroups) return;
+    int j = 0, grp = g;
+    if (MULTI) {
+        j = find_sub(prefix, nsub, g);
+        grp = g - __ldg(prefix + j);
     }
-    __shared__ VaSub Sm;
-    __shared__ int lm;
-    if (threadIdx.x == 0) {
-        const int j = find_sub(prefix, nsub, (int)blockIdx.x);
-        Sm = subs[j];
-        lm = blockIdx.x - prefix[j];
+    const VaSub& S = MULTI ? subs[j] : one;
+    if (MULTI && active && !active[S.inst]) return;
+    const float2* __restrict__ spec = spec_override ? spec_override : S.spec;
+    const float2* __restrict__ tns = reinterpret_cast<const float2*>(S.L.tns);
+    const int f = blockIdx.y * 32 + (threadIdx.x & 31);
+    float2 acc[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[c] = make_float2(0.f, 0.f);
+    const int e1 = __ldg(S.gptr + grp + 1);
+    for (int e = __ldg(S.gptr + grp); e < e1; ++e) {
+        const int2 ent = __ldg(S.gsrc + e);
+        const float2 sv = __ldg(spec + (size_t)ent.x * G3 + f);
+        const int mask = ent.y & 255;
+        const float2* tb = tns + (size_t)(ent.y >> 8) * G3 + f;
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+            if (mask & (1 << c)) cfma32(acc[c], __ldg(tb + (size_t)child_voff32(c) * G3), sv);
     }
-    __syncthreads();
-    if (active && !active[Sm.inst]) return;
-    vlist_accum32_body<G>(Sm, lm, spec_override);
+    float2* tsp = S.tsp;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const int t = __ldg(S.gtrg + 8 * grp + c);
+        if (t >= 0) tsp[(size_t)t * G3 + f] = acc[c];
+    }
 }
 
+// Pruned inverse DFT of one target's summed spectrum, one block per target
+// (vlist_inverse_kernel in kernels.cu in complex FP32).
 template <int G>
-__device__ __forceinline__ void vlist_accum32_body(const VaSub& S, int local, const float2* spec_override) {
+__device__ __forceinline__ void vlist_inverse32_body(const ViSub& S, int ti) {
     extern __shared__ float2 sm32[];
-    constexpr int P = G / 2, PP = P * P, G3 = G * G * G, NE = (G3 + 255) / 256;
+    constexpr int P = G / 2, PP = P * P, G3 = G * G * G;
     const VlistLevel& L = S.L;
     const float2* twb = reinterpret_cast<const float2*>(L.twb);
-    const float2* spec = spec_override ? spec_override : S.spec;
     float2* dnchk = S.dnchk;
     float2* grid = sm32;
     float2* c1 = sm32 + G3;
-    const float2* tns = reinterpret_cast<const float2*>(L.tns);
-    const int ti = local, t = S.trg[ti];
-    float2 acc[NE];
-#pragma unroll
-    for (int q = 0; q < NE; ++q) acc[q] = make_float2(0.f, 0.f);
-    for (int v = S.vptr[ti]; v < S.vptr[ti + 1]; ++v) {
-        const float2* sp = spec + (size_t)S.vsrc[v] * G3;
-        const float2* tn = tns + (size_t)S.voff[v] * G3;
-#pragma unroll
-        for (int q = 0; q < NE; ++q) {
-            int e = threadIdx.x + 256 * q;
-            if (e < G3) cfma32(acc[q], __ldg(sp + e), __ldg(tn + e));
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < NE; ++q) {
-        int e = threadIdx.x + 256 * q;
-        if (e < G3) grid[e] = acc[q];
-    }
+    const int t = S.trg[ti];
+    const float2* src = S.tsp + (size_t)ti * G3;
+    for (int e = threadIdx.x; e < G3; e += blockDim.x) grid[e] = __ldg(src + e);
     __syncthreads();
     for (int e = threadIdx.x; e < G * G * P; e += blockDim.x) {
         int kab = e % (G * G), c = e / (G * G);
@@ -439,21 +446,41 @@ __device__ __forceinline__ void vlist_accum32_body(const VaSub& S, int local, co
     }
 }
 
+template <int G, bool MULTI>
+__global__ void __launch_bounds__(256) vlist_inverse32_kernel(const ViSub one, const ViSub* __restrict__ subs,
+                                                              const int* __restrict__ prefix, int nsub,
+                                                              const int* __restrict__ active) {
+    if (!MULTI) {
+        vlist_inverse32_body<G>(one, blockIdx.x);
+        return;
+    }
+    __shared__ ViSub Sm;
+    __shared__ int lm;
+    if (threadIdx.x == 0) {
+        const int j = find_sub(prefix, nsub, (int)blockIdx.x);
+        Sm = subs[j];
+        lm = blockIdx.x - prefix[j];
+    }
+    __syncthreads();
+    if (active && !active[Sm.inst]) return;
+    vlist_inverse32_body<G>(Sm, lm);
+}
+
 static size_t vfwd32_smem(int G, int P) { return sizeof(float2) * (P * P * P + G * P * P + G * G * P); }
-static size_t vacc32_smem(int G, int P) { return sizeof(float2) * (G * G * G + G * G * P); }
+static size_t vinv32_smem(int G, int P) { return sizeof(float2) * (G * G * G + G * G * P); }
 
 void vlist32_init(int G) {
     int P = G / 2;
     const int fs = (int)vfwd32_smem(G, P);
     cudaFuncSetAttribute(vlist_forward32_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, fs);
     cudaFuncSetAttribute(vlist_forward32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, fs);
-    const int a8 = (int)vacc32_smem(8, 4), a12 = (int)vacc32_smem(12, 6), a16 = (int)vacc32_smem(16, 8);
-    cudaFuncSetAttribute(vlist_accum32_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a8);
-    cudaFuncSetAttribute(vlist_accum32_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, a8);
-    cudaFuncSetAttribute(vlist_accum32_kernel<12, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a12);
-    cudaFuncSetAttribute(vlist_accum32_kernel<12, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, a12);
-    cudaFuncSetAttribute(vlist_accum32_kernel<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a16);
-    cudaFuncSetAttribute(vlist_accum32_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, a16);
+    const int a8 = (int)vinv32_smem(8, 4), a12 = (int)vinv32_smem(12, 6), a16 = (int)vinv32_smem(16, 8);
+    cudaFuncSetAttribute(vlist_inverse32_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a8);
+    cudaFuncSetAttribute(vlist_inverse32_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, a8);
+    cudaFuncSetAttribute(vlist_inverse32_kernel<12, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a12);
+    cudaFuncSetAttribute(vlist_inverse32_kernel<12, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, a12);
+    cudaFuncSetAttribute(vlist_inverse32_kernel<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a16);
+    cudaFuncSetAttribute(vlist_inverse32_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, a16);
 }
 
 // L.tns, L.twf, L.twb hold float2 data in this form.
@@ -473,28 +500,51 @@ void launch_vlist_forward32(const VfSub* subs, const int* prefix, int nsub, int 
         vlist_forward32_kernel<true><<<nbox, 256, sm, s>>>(o, subs, prefix, nsub, active, so);
 }
 
-void launch_vlist_accum32(const VaSub* subs, const int* prefix, int nsub, int ntrg, int G, const int* active,
+void launch_vlist_group32(const VaSub* subs, const int* prefix, int nsub, int ngroups, int G, const int* active,
                           const void* spec_override, cudaStream_t s, const VaSub* one) {
-    if (ntrg == 0) return;
+    if (ngroups == 0) return;
     VaSub o{};
     if (nsub == 1) {
         if (!one) return;  // a single sub-launch is passed by value
         o = *one;
     }
-    const size_t sm = vacc32_smem(G, G / 2);
+    const dim3 grid((ngroups + VGROUP_WARPS - 1) / VGROUP_WARPS, G * G * G / 32);
     const float2* so = static_cast<const float2*>(spec_override);
-#define DDFMM_VACC(g)                                                                          \
-    if (nsub == 1)                                                                             \
-        vlist_accum32_kernel<g, false><<<ntrg, 256, sm, s>>>(o, subs, prefix, nsub, active, so); \
-    else                                                                                       \
-        vlist_accum32_kernel<g, true><<<ntrg, 256, sm, s>>>(o, subs, prefix, nsub, active, so);
+#define DDFMM_VGRP(g)                                                                                             \
+    if (nsub == 1)                                                                                                \
+        vlist_group32_kernel<g, false><<<grid, 32 * VGROUP_WARPS, 0, s>>>(o, subs, prefix, nsub, ngroups, active, so); \
+    else                                                                                                          \
+        vlist_group32_kernel<g, true><<<grid, 32 * VGROUP_WARPS, 0, s>>>(o, subs, prefix, nsub, ngroups, active, so);
     switch (G) {
-        case 8: DDFMM_VACC(8) break;
-        case 12: DDFMM_VACC(12) break;
-        case 16: DDFMM_VACC(16) break;
+        case 8: DDFMM_VGRP(8) break;
+        case 12: DDFMM_VGRP(12) break;
+        case 16: DDFMM_VGRP(16) break;
         default: break;
     }
-#undef DDFMM_VACC
+#undef DDFMM_VGRP
+}
+
+void launch_vlist_inverse32(const ViSub* subs, const int* prefix, int nsub, int ntrg, int G, const int* active,
+                            cudaStream_t s, const ViSub* one) {
+    if (ntrg == 0) return;
+    ViSub o{};
+    if (nsub == 1) {
+        if (!one) return;  // a single sub-launch is passed by value
+        o = *one;
+    }
+    const size_t sm = vinv32_smem(G, G / 2);
+#define DDFMM_VINV(g)                                                                          \
+    if (nsub == 1)                                                                             \
+        vlist_inverse32_kernel<g, false><<<ntrg, 256, sm, s>>>(o, subs, prefix, nsub, active); \
+    else                                                                                       \
+        vlist_inverse32_kernel<g, true><<<ntrg, 256, sm, s>>>(o, subs, prefix, nsub, active);
+    switch (G) {
+        case 8: DDFMM_VINV(8) break;
+        case 12: DDFMM_VINV(12) break;
+        case 16: DDFMM_VINV(16) break;
+        default: break;
+    }
+#undef DDFMM_VINV
 }
 
 // Batch I/O: complex64 densities in point-id order into leaf order (gather),

@@ -217,8 +217,8 @@ void Session::push_step(Step st) {
     // step types in the order the blocks emit them
     static const char* const order[] = {"lf_s2m",   "lf_m2m",       "lf_uc2ue",     "memset",   "hf_m2m",
                                         "hf_uc2ue", "hf_m2l",       "hf_dc2de",     "hf_l2l",   "lf_vlist_fft",
-                                        "lf_vlist_m2l", "lf_xlist", "lf_ulist",     "lf_wlist", "lf_dc2de",
-                                        "lf_l2t",   "lf_l2l"};
+                                        "lf_vlist_m2l", "lf_vlist_inv", "lf_xlist", "lf_ulist", "lf_wlist",
+                                        "lf_dc2de", "lf_l2t",       "lf_l2l"};
     std::string base(st.label);
     const size_t u = base.rfind("_w");
     if (u != std::string::npos && u + 2 < base.size() && std::isdigit((unsigned char)base[u + 2]))
@@ -1208,35 +1208,65 @@ void Session::build() {
         const auto& ids = kv.second;
         double W = L.W;
         begin_block(3, W);
-        // V list: FFT M2L (src/wave3d_eval.cpp:602-661)
+        // V list: FFT M2L (src/wave3d_eval.cpp:602-661).  The pointwise sums run by
+        // target parent (kernels.cuh, VlistGroups): the targets of a parent share one
+        // pass over the union of their V-list sources; then one inverse transform
+        // per target.
         {
-            std::vector<int> trg, vptr(1, 0), vsrc, voff;
             std::vector<char> is_src(nLF, 0);
-            // targets in Morton order, so blocks in flight share source spectra in L2
-            std::vector<int> mids(ids);
-            auto morton = [&](int l) {
-                const Idx3& x = T.boxes[lfbox[l]].idx;
+            auto morton = [](const Idx3& x) {
                 uint64_t m = 0;
                 for (int bit = 0; bit < 21; ++bit)
                     for (int d = 0; d < 3; ++d) m |= (uint64_t)((x[d] >> bit) & 1) << (3 * bit + d);
                 return m;
             };
-            std::stable_sort(mids.begin(), mids.end(), [&](int a2, int b2) { return morton(a2) < morton(b2); });
-            for (int l : mids) {
+            // (parent Morton key, child position, lf id) of every target
+            std::vector<std::pair<uint64_t, std::pair<int, int> > > tlist;
+            for (int l : ids) {
                 const Box& B = T.boxes[lfbox[l]];
                 if (B.vlist.empty()) continue;
-                Pt3 tc = T.center(B);
-                trg.push_back(l);
-                for (int s : B.vlist) {
-                    Pt3 sc = T.center(T.boxes[s]);
-                    int o[3];
-                    for (int d = 0; d < 3; ++d) o[d] = (int)std::round((tc[d] - sc[d]) / W);
-                    vsrc.push_back(lfidx[s]);
-                    voff.push_back((o[0] + 3) + 7 * ((o[1] + 3) + 7 * (o[2] + 3)));
-                    is_src[lfidx[s]] = 1;
-                    stats_.v_pairs++;
+                const Idx3 par{{B.idx[0] >> 1, B.idx[1] >> 1, B.idx[2] >> 1}};
+                const int ct = 4 * (B.idx[0] & 1) + 2 * (B.idx[1] & 1) + (B.idx[2] & 1);
+                tlist.push_back(std::make_pair(morton(par), std::make_pair(ct, l)));
+            }
+            std::sort(tlist.begin(), tlist.end());
+            std::vector<int> trg, gptr(1, 0), gtrg;
+            std::vector<int2> gsrc;
+            std::vector<std::pair<int, int> > ent;  // (source lf id, (tbase << 8) | mask) of the current group
+            for (size_t i = 0; i < tlist.size();) {
+                size_t j = i;
+                while (j < tlist.size() && tlist[j].first == tlist[i].first) ++j;  // one parent: [i, j)
+                const size_t g0 = gtrg.size();
+                gtrg.resize(g0 + 8, -1);
+                std::map<int, int> srcs;  // source lf id -> (tbase << 8) | mask
+                for (size_t k = i; k < j; ++k) {
+                    const int ct = tlist[k].second.first, l = tlist[k].second.second;
+                    const Box& B = T.boxes[lfbox[l]];
+                    gtrg[g0 + ct] = (int)trg.size();
+                    trg.push_back(l);
+                    for (int s : B.vlist) {
+                        const Box& SB = T.boxes[s];
+                        int rel[3], o[3];
+                        for (int d = 0; d < 3; ++d) {
+                            rel[d] = SB.idx[d] - 2 * (B.idx[d] >> 1);
+                            o[d] = B.idx[d] - SB.idx[d];
+                            if (SB.level != B.level || rel[d] < -2 || rel[d] > 3)
+                                throw std::runtime_error("V-list source outside the parent's neighbourhood");
+                        }
+                        const int tbase = (3 - rel[0]) + 7 * ((3 - rel[1]) + 7 * (3 - rel[2]));
+                        // the kernel's offset index for this pair: tbase + a + 7b + 49c
+                        const int voff = (o[0] + 3) + 7 * ((o[1] + 3) + 7 * (o[2] + 3));
+                        if (tbase + ((ct >> 2) & 1) + 7 * ((ct >> 1) & 1) + 49 * (ct & 1) != voff)
+                            throw std::logic_error("V-list offset bookkeeping");
+                        int& e = srcs[lfidx[s]];
+                        e = (tbase << 8) | (e & 255) | (1 << ct);
+                        is_src[lfidx[s]] = 1;
+                        stats_.v_pairs++;
+                    }
                 }
-                vptr.push_back((int)vsrc.size());
+                for (auto& kv : srcs) gsrc.push_back(make_int2(kv.first, kv.second));
+                gptr.push_back((int)gsrc.size());
+                i = j;
             }
             if (!trg.empty()) {
                 std::vector<int> srcb;
@@ -1259,26 +1289,46 @@ void Session::build() {
                     set_multi(f, f.hvf, f.v.nsrc);
                 }
                 push_step(f);
+                // summed target spectra: the high-frequency temporary T0 when it is large
+                // enough (every high-frequency pass has run before this low-frequency
+                // downward step, so T0 is free), else a buffer of their own
+                const size_t tsp_elems = trg.size() * (size_t)G3;
+                double2* tsp = tsp_elems <= (size_t)tmp_max ? T0 : salloc(tsp_elems);
+                const int ngroups = (int)gptr.size() - 1;
+                long long npairs = 0;
+                for (const int2& e2 : gsrc) npairs += __builtin_popcount(e2.y & 255);
                 Step a{};
                 a.kind = 3;
                 a.label = "lf_vlist_m2l";
-                a.flops = 8.0 * (double)G3 * vsrc.size() + 8.0 * 3 * (double)G3 * G * trg.size();
-                // compulsory: each source spectrum, the 316 tensors, each target's check values
-                a.bytes = 16.0 * ((double)G3 * srcb.size() + 316.0 * G3 + 2.0 * nE * trg.size());
+                a.flops = 8.0 * (double)G3 * npairs;
+                // compulsory: each source spectrum, the 316 tensors, each target's summed spectrum
+                a.bytes = 16.0 * ((double)G3 * srcb.size() + 316.0 * G3 + (double)G3 * trg.size());
                 a.v.L = VL;
-                a.v.trg = upload(trg);
-                a.v.vptr = upload(vptr);
-                a.v.vsrc = upload(vsrc);
-                a.v.voff = upload(voff);
-                a.v.ntrg = (int)trg.size();
+                a.v.grp = VlistGroups{upload(gptr), upload(gsrc), upload(gtrg), ngroups};
                 a.v.spec = lf_spec;
-                a.v.dnchk = lf_dnchk;
+                a.v.tsp = tsp;
                 if (mixed) {
-                    a.hva = VaSub{VL, a.v.trg, a.v.vptr, a.v.vsrc, a.v.voff, reinterpret_cast<const float2*>(lf_spec),
-                                  reinterpret_cast<float2*>(lf_dnchk), a.v.ntrg, 0};
-                    set_multi(a, a.hva, a.v.ntrg);
+                    a.hva = VaSub{VL, a.v.grp.gptr, a.v.grp.gsrc, a.v.grp.gtrg, reinterpret_cast<const float2*>(lf_spec),
+                                  reinterpret_cast<float2*>(tsp), ngroups, 0};
+                    set_multi(a, a.hva, ngroups);
                 }
                 push_step(a);
+                Step iv{};
+                iv.kind = 6;
+                iv.label = "lf_vlist_inv";
+                iv.flops = 8.0 * (double)G * ((double)G * G * P + G * P * P + P * P * P) * trg.size();
+                iv.bytes = 16.0 * ((double)G3 + 2.0 * nE) * trg.size();
+                iv.v.L = VL;
+                iv.v.trg = upload(trg);
+                iv.v.ntrg = (int)trg.size();
+                iv.v.tsp = tsp;
+                iv.v.dnchk = lf_dnchk;
+                if (mixed) {
+                    iv.hvi = ViSub{VL, iv.v.trg, reinterpret_cast<const float2*>(tsp), reinterpret_cast<float2*>(lf_dnchk),
+                                   iv.v.ntrg, 0};
+                    set_multi(iv, iv.hvi, iv.v.ntrg);
+                }
+                push_step(iv);
             }
         }
         // X list (src/wave3d_eval.cpp:663-686), into dnchk or, for small leaves, into extval
@@ -1408,7 +1458,8 @@ static const char* kernel_name(int kind) {
         case 0: return "zgemm_kernel";
         case 1: return "pt_kernel";
         case 2: return "vlist_forward_kernel";
-        case 3: return "vlist_accum_kernel";
+        case 3: return "vlist_group_kernel";
+        case 6: return "vlist_inverse_kernel";
         case 5: return "umma_cgemm_kernel";
         default: return "memset";
     }
@@ -1438,10 +1489,17 @@ void Session::launch_step(const Step& st, cudaStream_t s, double2* spec) {
             break;
         case 3:
             if (m)
-                launch_vlist_accum32(static_cast<const VaSub*>(st.msubs), st.mpre, 1, st.mtotal, st.v.L.G, nullptr,
+                launch_vlist_group32(static_cast<const VaSub*>(st.msubs), st.mpre, 1, st.mtotal, st.v.L.G, nullptr,
                                      spec != st.v.spec ? spec : nullptr, s, &st.hva);
             else
-                launch_vlist_accum(st.v.L, st.v.trg, st.v.ntrg, st.v.vptr, st.v.vsrc, st.v.voff, spec, st.v.dnchk, s);
+                launch_vlist_group(st.v.L, st.v.grp, spec, st.v.tsp, s);
+            break;
+        case 6:
+            if (m)
+                launch_vlist_inverse32(static_cast<const ViSub*>(st.msubs), st.mpre, 1, st.mtotal, st.v.L.G, nullptr, s,
+                                       &st.hvi);
+            else
+                launch_vlist_inverse(st.v.L, st.v.trg, st.v.ntrg, st.v.tsp, st.v.dnchk, s);
             break;
         case 4:
             CK(cudaMemsetAsync(st.ms.p, 0, st.ms.bytes, s));

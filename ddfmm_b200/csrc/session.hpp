@@ -107,15 +107,14 @@ private:
     };
     struct VLaunch {
         VlistLevel L;
-        int* src_boxes = nullptr;
+        int* src_boxes = nullptr;  // forward transforms: the source boxes
         int nsrc = 0;
-        int* trg = nullptr;
-        int* vptr = nullptr;
-        int* vsrc = nullptr;
-        int* voff = nullptr;
+        VlistGroups grp{};         // sums by target parent
+        int* trg = nullptr;        // inverse transforms: the target boxes (rows of tsp)
         int ntrg = 0;
         const double2* upeq = nullptr;
         double2* spec = nullptr;
+        double2* tsp = nullptr;    // summed target spectra
         double2* dnchk = nullptr;
     };
     struct Memset {
@@ -124,7 +123,7 @@ private:
     };
     // one step of the eval: exactly one of these is used
     struct Step {
-        int kind;  // 0 gemm, 1 pt, 2 vfwd, 3 vacc, 4 memset, 5 tcgen05 gemm
+        int kind;  // 0 gemm, 1 pt, 2 vfwd, 3 V-list sums, 4 memset, 5 tcgen05 gemm, 6 V-list inverse
         const char* label;  // pass name for profiling
         double flops;       // algorithmic flops of the launch
         double bytes;       // algorithmic DRAM bytes of the launch
@@ -146,6 +145,7 @@ private:
         PtSub hp;
         VfSub hvf;
         VaSub hva;
+        ViSub hvi;
     };
     friend class Batch;
 
