@@ -107,8 +107,13 @@ Batch::Batch(const std::vector<Session*>& sessions) : sessions_(sessions) {
                 }
                 add(PT, subs, n);
                 if (!launches_.empty() && launches_.back().kind == PT) {
-                    int tpi = 4;  // the widest shape any of the merged steps was tuned to
-                    for (auto& e : kk.second) tpi = std::max(tpi, e.second->tpi ? e.second->tpi : 32);
+                    // the shape the session with the most items of the merged steps was tuned to
+                    int tpi = 32, most = -1;
+                    for (auto& e : kk.second)
+                        if (e.second->hp.nitems > most) {
+                            most = e.second->hp.nitems;
+                            tpi = e.second->tpi ? e.second->tpi : 32;
+                        }
                     launches_.back().tpi = tpi;
                 }
             } else if (kind == 2 || kind == 3 || kind == 6) {
@@ -133,7 +138,7 @@ Batch::Batch(const std::vector<Session*>& sessions) : sessions_(sessions) {
                             VaSub u = e.second->hva;
                             u.inst = e.first;
                             subs.push_back(u);
-                            n.push_back(u.ngroups);
+                            n.push_back(vgroup_blocks(u.ngroups));
                         }
                         add(VACC, subs, n, gg.first);
                     } else {

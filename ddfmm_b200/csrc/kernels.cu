@@ -265,8 +265,143 @@ __global__ void pt_kernel(const PtItem* __restrict__ items, int nitems, const Pt
     }
 }
 
+// Warp-tiled point interactions (launch shapes PT_WARP_TARGETS / _SOURCES):
+// one warp per item, its source points staged PTW_TILE at a time in shared
+// memory (scaled and shifted once, not once per target), segment descriptors
+// 32 at a time with their point counts prefix-summed across the warp.  MODE 0:
+// lane = target (up to PTW_TPL per lane), sources read by broadcast; MODE 1:
+// PTW_TT targets per pass, lane = every 32nd source, per-target sums reduced
+// with warp shuffles.
+constexpr int PTW_WARPS = 8, PTW_TILE = 64, PTW_TPL = 4, PTW_TT = 8;
+
+template <int MODE>
+__global__ void __launch_bounds__(32 * PTW_WARPS) ptw_kernel(const PtItem* __restrict__ items, int nitems,
+                                                             const PtSrc* __restrict__ srcs, int kernel) {
+    __shared__ double sx[PTW_WARPS][PTW_TILE], sy[PTW_WARPS][PTW_TILE], sz[PTW_WARPS][PTW_TILE];
+    __shared__ double2 sd[PTW_WARPS][PTW_TILE];
+    __shared__ PtSrc seg[PTW_WARPS][32];
+    __shared__ int soff[PTW_WARPS][33];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = blockIdx.x * PTW_WARPS + warp;
+    if (w >= nitems) return;  // whole warps only: the kernel syncs nothing wider than a warp
+    const PtItem it = items[w];
+    const PtSet& T = it.trg;
+    constexpr int NT = MODE == 0 ? PTW_TPL : PTW_TT;
+    constexpr int TCH = MODE == 0 ? 32 * PTW_TPL : PTW_TT;  // targets per pass
+    for (int t0 = 0; t0 < T.n; t0 += TCH) {
+        double tx[NT], ty[NT], tz[NT];
+        double2 acc[NT];
+#pragma unroll
+        for (int i = 0; i < NT; ++i) {
+            const int t = MODE == 0 ? t0 + lane + 32 * i : t0 + i;
+            tx[i] = ty[i] = tz[i] = 0.0;
+            if (t < T.n) {
+                const double* tp = T.x + 3 * t;
+                tx[i] = T.scale * tp[0] + T.shift[0];
+                ty[i] = T.scale * tp[1] + T.shift[1];
+                tz[i] = T.scale * tp[2] + T.shift[2];
+            }
+            acc[i] = make_double2(0.0, 0.0);
+        }
+        for (int sb = it.src_begin; sb < it.src_end; sb += 32) {
+            const int nseg = min(32, it.src_end - sb);
+            int n_i = 0;
+            if (lane < nseg) {
+                seg[warp][lane] = srcs[sb + lane];
+                n_i = seg[warp][lane].src.n;
+            }
+            int incl = n_i;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += y;
+            }
+            soff[warp][lane + 1] = incl;
+            if (lane == 0) soff[warp][0] = 0;
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            __syncwarp();
+            for (int p0 = 0; p0 < total; p0 += PTW_TILE) {
+                const int cnt = min(PTW_TILE, total - p0);
+                for (int p = lane; p < cnt; p += 32) {
+                    const int gp = p0 + p;
+                    int lo = 0, hi = nseg - 1;  // the segment holding staged point gp
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (soff[warp][mid] <= gp)
+                            lo = mid;
+                        else
+                            hi = mid - 1;
+                    }
+                    const PtSrc& Q = seg[warp][lo];
+                    const int q = gp - soff[warp][lo];
+                    const double* xp = Q.src.x + 3 * q;
+                    sx[warp][p] = Q.src.scale * xp[0] + Q.src.shift[0];
+                    sy[warp][p] = Q.src.scale * xp[1] + Q.src.shift[1];
+                    sz[warp][p] = Q.src.scale * xp[2] + Q.src.shift[2];
+                    sd[warp][p] = Q.den[q];
+                }
+                __syncwarp();
+                if (MODE == 0) {
+                    for (int p = 0; p < cnt; ++p) {
+                        const double px = sx[warp][p], py = sy[warp][p], pz = sz[warp][p];
+                        const double2 dv = sd[warp][p];
+#pragma unroll
+                        for (int i = 0; i < NT; ++i) cfma(acc[i], kfun(tx[i] - px, ty[i] - py, tz[i] - pz, kernel), dv);
+                    }
+                } else {
+                    for (int p = lane; p < cnt; p += 32) {
+                        const double px = sx[warp][p], py = sy[warp][p], pz = sz[warp][p];
+                        const double2 dv = sd[warp][p];
+#pragma unroll
+                        for (int i = 0; i < NT; ++i)
+                            if (t0 + i < T.n) cfma(acc[i], kfun(tx[i] - px, ty[i] - py, tz[i] - pz, kernel), dv);
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        if (MODE == 0) {
+#pragma unroll
+            for (int i = 0; i < NT; ++i) {
+                const int t = t0 + lane + 32 * i;
+                if (t < T.n) {
+                    double2 o = it.out[t];
+                    o.x += acc[i].x;
+                    o.y += acc[i].y;
+                    it.out[t] = o;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < NT; ++i) {
+#pragma unroll
+                for (int d = 16; d > 0; d >>= 1) {
+                    acc[i].x += __shfl_xor_sync(0xffffffffu, acc[i].x, d);
+                    acc[i].y += __shfl_xor_sync(0xffffffffu, acc[i].y, d);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < NT; ++i)
+                if (lane == i && t0 + i < T.n) {
+                    double2 o = it.out[t0 + i];
+                    o.x += acc[i].x;
+                    o.y += acc[i].y;
+                    it.out[t0 + i] = o;
+                }
+        }
+    }
+}
+
 void launch_pt(const PtItem* items, int nitems, const PtSrc* srcs, int kernel, cudaStream_t s, int tpi) {
     if (nitems == 0) return;
+    if (tpi == PT_WARP_TARGETS || tpi == PT_WARP_SOURCES) {
+        const int blocks = (nitems + PTW_WARPS - 1) / PTW_WARPS;
+        if (tpi == PT_WARP_TARGETS)
+            ptw_kernel<0><<<blocks, 32 * PTW_WARPS, 0, s>>>(items, nitems, srcs, kernel);
+        else
+            ptw_kernel<1><<<blocks, 32 * PTW_WARPS, 0, s>>>(items, nitems, srcs, kernel);
+        return;
+    }
     const int blocks = (int)(((long long)nitems * tpi + 255) / 256);
     switch (tpi) {
         case 4: pt_kernel<4><<<blocks, 256, 0, s>>>(items, nitems, srcs, kernel); break;
@@ -289,123 +424,202 @@ void launch_pt(const PtItem* items, int nitems, const PtSrc* srcs, int kernel, c
 // sums), about a third of the work of full G^3 transforms.  Signs follow
 // FFTW: forward exp(-2 pi i jk/G), backward exp(+2 pi i jk/G), unnormalised.
 
-__global__ void vlist_forward_kernel(VlistLevel L, const int* __restrict__ boxes,
-                                     const double2* __restrict__ upeq, double2* __restrict__ spec,
-                                     const double2* __restrict__ twf) {
-    extern __shared__ double2 sm[];
-    const int G = L.G, P = L.P, PP = P * P;
-    double2* cube = sm;             // [c'][b'][a'], a', b', c' < P
+// Forward transform of one source box per block, in three passes of P-term
+// sums (x, then y, then z), each thread taking whole lines: it loads the P
+// inputs of its line once and produces the line's G outputs, the twiddle
+// factors W[k][a] = exp(-2 pi i (P + a) k / G) read from shared memory.
+template <int G>
+__global__ void __launch_bounds__(vt_threads(G)) vlist_forward_kernel(VlistLevel L, const int* __restrict__ boxes,
+                                                                      const double2* __restrict__ upeq,
+                                                                      double2* __restrict__ spec,
+                                                                      const double2* __restrict__ twf) {
+    constexpr int P = G / 2, PP = P * P, G2 = G * G;
+    extern __shared__ double2 vsm[];
+    double2* W = vsm;               // W[k * P + a]
+    double2* cube = W + G * P;      // [c'][b'][a']
     double2* b1 = cube + PP * P;    // [c'][b'][ka]
-    double2* b2 = b1 + G * PP;      // [c'][kb][ka]
+    double2* b2 = b1 + PP * G;      // [c'][kb][ka]
+    const int tid = threadIdx.x, nt = blockDim.x;
     const int b = boxes[blockIdx.x];
-    for (int e = threadIdx.x; e < PP * P; e += blockDim.x) cube[e] = make_double2(0.0, 0.0);
+    for (int e = tid; e < G * P; e += nt) W[e] = twf[((P + e % P) * (e / P)) % G];
+    for (int e = tid; e < PP * P; e += nt) cube[e] = make_double2(0.0, 0.0);
     __syncthreads();
-    for (int k = threadIdx.x; k < L.nE; k += blockDim.x) cube[L.cube_idx[k]] = upeq[(size_t)b * L.nE + k];
+    for (int k = tid; k < L.nE; k += nt) cube[L.cube_idx[k]] = upeq[(size_t)b * L.nE + k];
     __syncthreads();
-    for (int e = threadIdx.x; e < G * PP; e += blockDim.x) {
-        int ka = e % G, line = e / G;
-        double2 acc = make_double2(0.0, 0.0);
-        for (int a = 0; a < P; ++a) cfma(acc, cube[line * P + a], twf[((P + a) * ka) % G]);
-        b1[e] = acc;
+    if (const int line = tid; line < PP) {  // x: line (c', b'); one line per thread, nt >= G^2
+        double2 x[P];
+#pragma unroll
+        for (int a = 0; a < P; ++a) x[a] = cube[line * P + a];
+#pragma unroll 1
+        for (int k = 0; k < G; ++k) {
+            double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int a = 0; a < P; ++a) cfma(acc, x[a], W[k * P + a]);
+            b1[line * G + k] = acc;
+        }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < G * G * P; e += blockDim.x) {
-        int ka = e % G, kb = (e / G) % G, c = e / (G * G);
-        double2 acc = make_double2(0.0, 0.0);
-        for (int bb = 0; bb < P; ++bb) cfma(acc, b1[(c * P + bb) * G + ka], twf[((P + bb) * kb) % G]);
-        b2[e] = acc;
+    if (const int e = tid; e < P * G) {  // y: line (c', ka)
+        const int c = e / G, ka = e % G;
+        double2 x[P];
+#pragma unroll
+        for (int bb = 0; bb < P; ++bb) x[bb] = b1[(c * P + bb) * G + ka];
+#pragma unroll 1
+        for (int k = 0; k < G; ++k) {
+            double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int bb = 0; bb < P; ++bb) cfma(acc, x[bb], W[k * P + bb]);
+            b2[(c * G + k) * G + ka] = acc;
+        }
     }
     __syncthreads();
-    double2* o = spec + (size_t)b * G * G * G;
-    for (int e = threadIdx.x; e < G * G * G; e += blockDim.x) {
-        int kab = e % (G * G), kc = e / (G * G);
-        double2 acc = make_double2(0.0, 0.0);
-        for (int c = 0; c < P; ++c) cfma(acc, b2[c * G * G + kab], twf[((P + c) * kc) % G]);
-        o[e] = acc;
+    double2* o = spec + (size_t)b * G2 * G;
+    if (const int kab = tid; kab < G2) {  // z: line (ka, kb), the box's spectrum
+        double2 x[P];
+#pragma unroll
+        for (int c = 0; c < P; ++c) x[c] = b2[c * G2 + kab];
+#pragma unroll 1
+        for (int k = 0; k < G; ++k) {
+            double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int c = 0; c < P; ++c) cfma(acc, x[c], W[k * P + c]);
+            o[k * G2 + kab] = acc;
+        }
     }
 }
 
 // The pointwise products of the V list, by target parent: warp w of a block
-// takes target parent blockIdx.x * VGROUP_WARPS + w and lane l frequency
-// 32 blockIdx.y + l of the G^3 grid, with one accumulator per child position.
-// The loop over the parent's source entries is the same for the 32 lanes, so
-// the child mask branches are warp-uniform; a source's spectrum value is
-// loaded once and used by every child that has it in its V list.  Blocks of
-// one frequency chunk run together (blockIdx.x varies fastest), so the
-// translation tensors' 32-frequency slices of that chunk (316 x 512 bytes)
-// stay in the SM's L1 while the chunk lasts, and the source spectra's slices
-// (32 MB over all boxes at the bench workload) in L2.
+// takes target parent (blockIdx.x VGROUP_ROUNDS + r) VGROUP_WARPS + w in round
+// r, lane l frequency 32 blockIdx.y + l of the G^3 grid, with one accumulator
+// per child position.  The block first copies the chunk's slice of all 343
+// translation tensors (343 x 32 values) into shared memory, so every tensor
+// value of a product is a conflict-free shared load.  The loop over a
+// parent's source entries is the same for the 32 lanes: entries are read 32
+// at a time (one per lane) and broadcast by shuffles, the child-mask branches
+// are warp-uniform, and the source spectrum values are loaded four entries
+// ahead.  A source value is loaded once and used by every child that lists
+// it.  Blocks of one chunk run together (blockIdx.x varies fastest), so the
+// chunk's slice of every source spectrum stays in L2 while the chunk lasts.
 __host__ __device__ constexpr int child_voff(int c) { return ((c >> 2) & 1) + 7 * ((c >> 1) & 1) + 49 * (c & 1); }
+constexpr int VT_OFFSETS = 343;
 
 template <int G>
-__global__ void __launch_bounds__(256) vlist_group_kernel(const int* __restrict__ gptr, const int2* __restrict__ gsrc,
-                                                          const int* __restrict__ gtrg, int ngroups,
-                                                          const double2* __restrict__ spec,
-                                                          const double2* __restrict__ tns, double2* __restrict__ tsp) {
+__global__ void __launch_bounds__(32 * VGROUP_WARPS) vlist_group_kernel(const int* __restrict__ gptr,
+                                                                        const int2* __restrict__ gsrc,
+                                                                        const int* __restrict__ gtrg, int ngroups,
+                                                                        const double2* __restrict__ spec,
+                                                                        const double2* __restrict__ tns,
+                                                                        double2* __restrict__ tsp) {
     constexpr int G3 = G * G * G;
-    const int grp = blockIdx.x * VGROUP_WARPS + (threadIdx.x >> 5);
-    if (grp >= ngroups) return;
-    const int f = blockIdx.y * 32 + (threadIdx.x & 31);
-    double2 acc[8];
+    extern __shared__ double2 tsm[];  // [offset][lane]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int chunk = blockIdx.y, f = chunk * 32 + lane;
+    for (int i = threadIdx.x; i < VT_OFFSETS * 32; i += blockDim.x)
+        tsm[i] = __ldg(tns + (size_t)(i >> 5) * G3 + chunk * 32 + (i & 31));
+    __syncthreads();
+    for (int r = 0; r < VGROUP_ROUNDS; ++r) {
+        const int grp = (blockIdx.x * VGROUP_ROUNDS + r) * VGROUP_WARPS + warp;
+        if (grp >= ngroups) break;  // warp-uniform; no block-wide sync below
+        double2 acc[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) acc[c] = make_double2(0.0, 0.0);
-    const int e1 = __ldg(gptr + grp + 1);
-    for (int e = __ldg(gptr + grp); e < e1; ++e) {
-        const int2 ent = __ldg(gsrc + e);
-        const double2 S = __ldg(spec + (size_t)ent.x * G3 + f);
-        const int mask = ent.y & 255;
-        const double2* tb = tns + (size_t)(ent.y >> 8) * G3 + f;
+        for (int c = 0; c < 8; ++c) acc[c] = make_double2(0.0, 0.0);
+        const int e0 = __ldg(gptr + grp), e1 = __ldg(gptr + grp + 1);
+        for (int base = e0; base < e1; base += 32) {
+            const int n = min(32, e1 - base);
+            const int2 mine = lane < n ? __ldg(gsrc + base + lane) : make_int2(0, 0);
+            double2 sv[4];
 #pragma unroll
-        for (int c = 0; c < 8; ++c)
-            if (mask & (1 << c)) cfma(acc[c], __ldg(tb + (size_t)child_voff(c) * G3), S);
-    }
+            for (int u = 0; u < 4; ++u)
+                if (u < n) sv[u] = __ldg(spec + (size_t)__shfl_sync(0xffffffffu, mine.x, u) * G3 + f);
+            for (int k = 0; k < n; k += 4) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        const int t = __ldg(gtrg + 8 * grp + c);
-        if (t >= 0) tsp[(size_t)t * G3 + f] = acc[c];
+                for (int u = 0; u < 4; ++u) {
+                    const int kk = k + u;
+                    if (kk < n) {
+                        const int y = __shfl_sync(0xffffffffu, mine.y, kk);
+                        const double2 sval = sv[u];
+                        if (kk + 4 < n) sv[u] = __ldg(spec + (size_t)__shfl_sync(0xffffffffu, mine.x, kk + 4) * G3 + f);
+                        const int mask = y & 255;
+                        const double2* tb = tsm + (y >> 8) * 32 + lane;
+#pragma unroll
+                        for (int c = 0; c < 8; ++c)
+                            if (mask & (1 << c)) cfma(acc[c], tb[child_voff(c) * 32], sval);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int t = __ldg(gtrg + 8 * grp + c);
+            if (t >= 0) tsp[(size_t)t * G3 + f] = acc[c];
+        }
     }
 }
 
-// Pruned inverse DFT of one target's summed spectrum (one block per target):
-// G^2 P, G P^2 and P^3 outputs of G-term sums, then the corner-cube nodes
-// scaled by 1/G^3 are added into the target's check values.
+// Pruned inverse DFT of one target's summed spectrum per block: P outputs
+// of G-term sums along z (each thread one (ka, kb) line, its G inputs read
+// straight from the summed spectrum), then y, then x; the corner-cube nodes
+// scaled by 1/G^3 are added into the target's check values.  Twiddles
+// W[a][k] = exp(+2 pi i (P + a) k / G) from shared memory.
 template <int G>
-__global__ void __launch_bounds__(256) vlist_inverse_kernel(VlistLevel L, const int* __restrict__ trg,
-                                                            const double2* __restrict__ tsp,
-                                                            double2* __restrict__ dnchk,
-                                                            const double2* __restrict__ twb) {
-    extern __shared__ double2 sm[];
-    constexpr int P = G / 2, PP = P * P, G3 = G * G * G;
-    double2* grid = sm;          // G^3 summed spectrum, later [c'][b'][ka]
-    double2* c1 = sm + G3;       // [c'][kb][ka], later the P^3 cube
+__global__ void __launch_bounds__(vt_threads(G)) vlist_inverse_kernel(VlistLevel L, const int* __restrict__ trg,
+                                                                      const double2* __restrict__ tsp,
+                                                                      double2* __restrict__ dnchk,
+                                                                      const double2* __restrict__ twb) {
+    constexpr int P = G / 2, PP = P * P, G2 = G * G, G3 = G2 * G;
+    extern __shared__ double2 vsm[];
+    double2* W = vsm;               // W[a * G + k]
+    double2* c1 = W + P * G;        // [c'][kb][ka]
+    double2* c2 = c1 + P * G2;      // [c'][b'][ka]
+    double2* c3 = c2 + PP * G;      // [c'][b'][a']
+    const int tid = threadIdx.x, nt = blockDim.x;
     const int ti = blockIdx.x, t = trg[ti];
+    for (int e = tid; e < P * G; e += nt) W[e] = twb[((P + e / G) * (e % G)) % G];
+    __syncthreads();
     const double2* src = tsp + (size_t)ti * G3;
-    for (int e = threadIdx.x; e < G3; e += blockDim.x) grid[e] = __ldg(src + e);
-    __syncthreads();
-    for (int e = threadIdx.x; e < G * G * P; e += blockDim.x) {  // z: outputs c' < P
-        int kab = e % (G * G), c = e / (G * G);
-        double2 s = make_double2(0.0, 0.0);
-        for (int kc = 0; kc < G; ++kc) cfma(s, grid[kc * G * G + kab], twb[((P + c) * kc) % G]);
-        c1[e] = s;
+    if (const int kab = tid; kab < G2) {  // z
+        double2 x[G];
+#pragma unroll
+        for (int k = 0; k < G; ++k) x[k] = __ldg(src + k * G2 + kab);
+#pragma unroll 1
+        for (int c = 0; c < P; ++c) {
+            double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int k = 0; k < G; ++k) cfma(acc, x[k], W[c * G + k]);
+            c1[c * G2 + kab] = acc;
+        }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < G * PP; e += blockDim.x) {  // y: outputs b' < P
-        int ka = e % G, bb = (e / G) % P, c = e / (G * P);
-        double2 s = make_double2(0.0, 0.0);
-        for (int kb = 0; kb < G; ++kb) cfma(s, c1[(c * G + kb) * G + ka], twb[((P + bb) * kb) % G]);
-        grid[e] = s;  // [c'][b'][ka]
+    if (const int e = tid; e < P * G) {  // y: line (c', ka)
+        const int c = e / G, ka = e % G;
+        double2 x[G];
+#pragma unroll
+        for (int k = 0; k < G; ++k) x[k] = c1[(c * G + k) * G + ka];
+#pragma unroll 1
+        for (int bb = 0; bb < P; ++bb) {
+            double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int k = 0; k < G; ++k) cfma(acc, x[k], W[bb * G + k]);
+            c2[(c * P + bb) * G + ka] = acc;
+        }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < PP * P; e += blockDim.x) {  // x: outputs a' < P
-        int a = e % P, line = e / P;
-        double2 s = make_double2(0.0, 0.0);
-        for (int ka = 0; ka < G; ++ka) cfma(s, grid[line * G + ka], twb[((P + a) * ka) % G]);
-        c1[e] = s;  // [c'][b'][a']
+    if (const int line = tid; line < PP) {  // x: line (c', b'); one line per thread, nt >= G^2
+        double2 x[G];
+#pragma unroll
+        for (int k = 0; k < G; ++k) x[k] = c2[line * G + k];
+#pragma unroll 1
+        for (int a = 0; a < P; ++a) {
+            double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int k = 0; k < G; ++k) cfma(acc, x[k], W[a * G + k]);
+            c3[line * P + a] = acc;
+        }
     }
     __syncthreads();
     const double coef = 1.0 / (double)G3;
-    for (int k = threadIdx.x; k < L.nE; k += blockDim.x) {
-        double2 v = c1[L.cube_idx[k]];
+    for (int k = tid; k < L.nE; k += nt) {
+        double2 v = c3[L.cube_idx[k]];
         double2 o = dnchk[(size_t)t * L.nE + k];
         o.x += v.x * coef;
         o.y += v.y * coef;
@@ -413,31 +627,45 @@ __global__ void __launch_bounds__(256) vlist_inverse_kernel(VlistLevel L, const 
     }
 }
 
-static size_t vfwd_smem(int G, int P) { return sizeof(double2) * (P * P * P + G * P * P + G * G * P); }
-static size_t vinv_smem(int G, int P) { return sizeof(double2) * (G * G * G + G * G * P); }
+size_t vt_smem(int G, size_t es) {
+    const size_t P = G / 2;
+    return es * (G * P + P * P * P + P * P * G + P * G * G);
+}
 
-void vlist_init(int G) {
-    int P = G / 2;
-    cudaFuncSetAttribute(vlist_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vfwd_smem(G, P));
-    cudaFuncSetAttribute(vlist_inverse_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vinv_smem(8, 4));
-    cudaFuncSetAttribute(vlist_inverse_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vinv_smem(12, 6));
-    cudaFuncSetAttribute(vlist_inverse_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vinv_smem(16, 8));
+void vlist_init(int) {
+    const int gs = (int)(sizeof(double2) * VT_OFFSETS * 32);
+    cudaFuncSetAttribute(vlist_group_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
+    cudaFuncSetAttribute(vlist_group_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
+    cudaFuncSetAttribute(vlist_group_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
+    cudaFuncSetAttribute(vlist_forward_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(8, 16));
+    cudaFuncSetAttribute(vlist_forward_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(12, 16));
+    cudaFuncSetAttribute(vlist_forward_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(16, 16));
+    cudaFuncSetAttribute(vlist_inverse_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(8, 16));
+    cudaFuncSetAttribute(vlist_inverse_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(12, 16));
+    cudaFuncSetAttribute(vlist_inverse_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(16, 16));
 }
 
 void launch_vlist_forward(const VlistLevel& L, const int* boxes, int nbox, const double2* upeq, double2* spec,
                           cudaStream_t s) {
     if (nbox == 0) return;
-    vlist_forward_kernel<<<nbox, 256, vfwd_smem(L.G, L.P), s>>>(L, boxes, upeq, spec, L.twf);
+    const size_t sm = vt_smem(L.G, sizeof(double2));
+    switch (L.G) {
+        case 8: vlist_forward_kernel<8><<<nbox, vt_threads(8), sm, s>>>(L, boxes, upeq, spec, L.twf); break;
+        case 12: vlist_forward_kernel<12><<<nbox, vt_threads(12), sm, s>>>(L, boxes, upeq, spec, L.twf); break;
+        case 16: vlist_forward_kernel<16><<<nbox, vt_threads(16), sm, s>>>(L, boxes, upeq, spec, L.twf); break;
+        default: break;
+    }
 }
 
 void launch_vlist_group(const VlistLevel& L, const VlistGroups& V, const double2* spec, double2* tsp,
                         cudaStream_t s) {
     if (V.ngroups == 0) return;
-    const dim3 grid((V.ngroups + VGROUP_WARPS - 1) / VGROUP_WARPS, L.G * L.G * L.G / 32);
+    const dim3 grid(vgroup_blocks(V.ngroups), L.G * L.G * L.G / 32);
+    const size_t sm = sizeof(double2) * VT_OFFSETS * 32;
     switch (L.G) {
-        case 8: vlist_group_kernel<8><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
-        case 12: vlist_group_kernel<12><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
-        case 16: vlist_group_kernel<16><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
+        case 8: vlist_group_kernel<8><<<grid, 32 * VGROUP_WARPS, sm, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
+        case 12: vlist_group_kernel<12><<<grid, 32 * VGROUP_WARPS, sm, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
+        case 16: vlist_group_kernel<16><<<grid, 32 * VGROUP_WARPS, sm, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
         default: break;
     }
 }
@@ -445,11 +673,11 @@ void launch_vlist_group(const VlistLevel& L, const VlistGroups& V, const double2
 void launch_vlist_inverse(const VlistLevel& L, const int* trg, int ntrg, const double2* tsp, double2* dnchk,
                           cudaStream_t s) {
     if (ntrg == 0) return;
-    const size_t sm = vinv_smem(L.G, L.P);
+    const size_t sm = vt_smem(L.G, sizeof(double2));
     switch (L.G) {
-        case 8: vlist_inverse_kernel<8><<<ntrg, 256, sm, s>>>(L, trg, tsp, dnchk, L.twb); break;
-        case 12: vlist_inverse_kernel<12><<<ntrg, 256, sm, s>>>(L, trg, tsp, dnchk, L.twb); break;
-        case 16: vlist_inverse_kernel<16><<<ntrg, 256, sm, s>>>(L, trg, tsp, dnchk, L.twb); break;
+        case 8: vlist_inverse_kernel<8><<<ntrg, vt_threads(8), sm, s>>>(L, trg, tsp, dnchk, L.twb); break;
+        case 12: vlist_inverse_kernel<12><<<ntrg, vt_threads(12), sm, s>>>(L, trg, tsp, dnchk, L.twb); break;
+        case 16: vlist_inverse_kernel<16><<<ntrg, vt_threads(16), sm, s>>>(L, trg, tsp, dnchk, L.twb); break;
         default: break;
     }
 }

@@ -62,7 +62,12 @@ void launch_kmat(const KmatJob* jobs_dev, int njobs, long long total, int kernel
 void launch_gemm(const GemmProblem* probs_dev, const GemmTile* tiles_dev, int ntiles,
                  const long long* xoff, const long long* yoff, const double2* X, double2* Y, int mode,
                  cudaStream_t s);
-// tpi: threads per item (4, 8, 16 or 32), chosen per launch by the session's autotuner
+// tpi: the launch shape, chosen per step by the session's autotuner: 4, 8, 16 or
+// 32 threads per item, each thread taking targets and walking the sources in
+// global memory; or one warp per item with the item's sources staged in
+// shared memory, lanes over targets (PT_WARP_TARGETS) or over sources with a
+// warp-shuffle reduction per target (PT_WARP_SOURCES)
+constexpr int PT_WARP_TARGETS = 1001, PT_WARP_SOURCES = 1002;
 void launch_pt(const PtItem* items_dev, int nitems, const PtSrc* srcs_dev, int kernel, cudaStream_t s, int tpi = 32);
 
 // FFT-based low-frequency M2L on a G^3 grid (G = 2P), see kernels.cu.
@@ -75,6 +80,11 @@ struct VlistLevel {
     const double2* twb;     // G backward twiddles exp(+2 pi i m / G)
 };
 void vlist_init(int G);
+// The forward and inverse transforms take one box per block and one thread per
+// (ka, kb) line of the grid; their shared memory holds the twiddles (G P) and
+// the three partial transforms (P^3, P^2 G, P G^2 elements of es bytes).
+__host__ __device__ constexpr int vt_threads(int G) { return ((G * G + 31) / 32) * 32; }
+size_t vt_smem(int G, size_t es);
 void launch_vlist_forward(const VlistLevel& L, const int* boxes, int nbox, const double2* upeq,
                           double2* spec, cudaStream_t s);
 // The V-list sums in Fourier space, by target parent: the target boxes of a
@@ -87,7 +97,12 @@ void launch_vlist_forward(const VlistLevel& L, const int* boxes, int nbox, const
 // pair for child position 0; child position c adds a + 7b + 49c'.
 // tsp[t] (G^3 per target, rows in group order) receives the summed spectrum
 // of target t, overwritten each eval.
-constexpr int VGROUP_WARPS = 8;  // target parents per block of the accumulation
+// A block of the sums takes VGROUP_WARPS x VGROUP_ROUNDS consecutive groups
+// (one per warp and round) of one instance and one 32-frequency chunk.
+constexpr int VGROUP_WARPS = 16, VGROUP_ROUNDS = 4;
+inline int vgroup_blocks(int ngroups) {
+    return (ngroups + VGROUP_WARPS * VGROUP_ROUNDS - 1) / (VGROUP_WARPS * VGROUP_ROUNDS);
+}
 struct VlistGroups {
     const int* gptr;   // ngroups + 1: the source entries of each group
     const int2* gsrc;  // the source entries
@@ -168,8 +183,9 @@ void vlist32_init(int G);
 // a kernel parameter); `subs` / `prefix` are then not read.
 void launch_vlist_forward32(const VfSub* subs, const int* prefix, int nsub, int nbox, int G, const int* active,
                             void* spec_override, cudaStream_t s, const VfSub* one);
-// work items: groups (launch_vlist_group32) or targets (launch_vlist_inverse32)
-void launch_vlist_group32(const VaSub* subs, const int* prefix, int nsub, int ngroups, int G, const int* active,
+// work items: blocks of groups, vgroup_blocks(ngroups) per sub-launch (launch_vlist_group32),
+// or targets (launch_vlist_inverse32)
+void launch_vlist_group32(const VaSub* subs, const int* prefix, int nsub, int nblocks, int G, const int* active,
                           const void* spec_override, cudaStream_t s, const VaSub* one);
 void launch_vlist_inverse32(const ViSub* subs, const int* prefix, int nsub, int ntrg, int G, const int* active,
                             cudaStream_t s, const ViSub* one);

@@ -275,9 +275,167 @@ __global__ void pt32_kernel(const PtSub* __restrict__ subs, const int* __restric
     }
 }
 
+// Warp-tiled point interactions: one warp per item.  The item's source points
+// are staged in shared memory, PTW_TILE at a time, as FP32 coordinates
+// relative to a reference point of the item (its first target, in FP64): all
+// points of an item lie within a few boxes of it, so the FP32 differences and
+// the phase 2 pi r stay accurate wherever the item sits.  MODE 0: each lane
+// owns up to PTW_TPL targets (lane + 32 i) and walks the staged sources
+// (broadcast reads); MODE 1: the targets go PTW_TT at a time, each lane takes
+// every 32nd staged source and the per-target sums are reduced across the
+// warp with shuffles.  Segment descriptors are read 32 at a time into shared
+// memory; their point counts, prefix-summed across the warp, map a staged
+// point to its segment.
+constexpr int PTW_WARPS = 8, PTW_TILE = 64, PTW_TPL = 4, PTW_TT = 8;
+
+__device__ __forceinline__ float2 kfun32f(float x, float y, float z, int kernel) {
+    float r2 = x * x + y * y + z * z;
+    if (r2 < 1e-16f) r2 = 1.0f;
+    float r = sqrtf(r2);
+    float s, c;
+    sincospif(2.0f * r, &s, &c);
+    if (kernel == KERNEL_HELM) {
+        float ir = 1.0f / r;
+        return make_float2(c * ir, s * ir);
+    }
+    return make_float2(c, s);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(32 * PTW_WARPS) pt32w_kernel(const PtSub* __restrict__ subs,
+                                                               const int* __restrict__ prefix, int nsub, int nitems,
+                                                               const int* __restrict__ active) {
+    __shared__ float4 sp[PTW_WARPS][PTW_TILE];
+    __shared__ float2 sd[PTW_WARPS][PTW_TILE];
+    __shared__ PtSrc seg[PTW_WARPS][32];
+    __shared__ int soff[PTW_WARPS][33];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = blockIdx.x * PTW_WARPS + warp;
+    if (w >= nitems) return;  // whole warps only: the kernel syncs nothing wider than a warp
+    const int j = find_sub(prefix, nsub, w);
+    const PtSub S = subs[j];
+    if (active && !active[S.inst]) return;
+    const PtItem it = S.items[w - prefix[j]];
+    float2* out = reinterpret_cast<float2*>(it.out);
+    const PtSet& T = it.trg;
+    if (T.n <= 0) return;
+    const double cx = T.scale * T.x[0] + T.shift[0], cy = T.scale * T.x[1] + T.shift[1],
+                 cz = T.scale * T.x[2] + T.shift[2];
+    auto trg_rel = [&](int t, float& x, float& y, float& z) {
+        const double* tp = T.x + 3 * t;
+        x = (float)(T.scale * tp[0] + T.shift[0] - cx);
+        y = (float)(T.scale * tp[1] + T.shift[1] - cy);
+        z = (float)(T.scale * tp[2] + T.shift[2] - cz);
+    };
+    constexpr int TCH = MODE == 0 ? 32 * PTW_TPL : PTW_TT;  // targets per pass
+    for (int t0 = 0; t0 < T.n; t0 += TCH) {
+        float tx[MODE == 0 ? PTW_TPL : PTW_TT], ty[MODE == 0 ? PTW_TPL : PTW_TT], tz[MODE == 0 ? PTW_TPL : PTW_TT];
+        float2 acc[MODE == 0 ? PTW_TPL : PTW_TT];
+        constexpr int NT = MODE == 0 ? PTW_TPL : PTW_TT;
+#pragma unroll
+        for (int i = 0; i < NT; ++i) {
+            const int t = MODE == 0 ? t0 + lane + 32 * i : t0 + i;
+            tx[i] = ty[i] = tz[i] = 0.f;
+            if (t < T.n) trg_rel(t, tx[i], ty[i], tz[i]);
+            acc[i] = make_float2(0.f, 0.f);
+        }
+        for (int sb = it.src_begin; sb < it.src_end; sb += 32) {
+            const int nseg = min(32, it.src_end - sb);
+            int n_i = 0;
+            if (lane < nseg) {
+                seg[warp][lane] = S.srcs[sb + lane];
+                n_i = seg[warp][lane].src.n;
+            }
+            int incl = n_i;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += y;
+            }
+            soff[warp][lane + 1] = incl;
+            if (lane == 0) soff[warp][0] = 0;
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            __syncwarp();
+            for (int p0 = 0; p0 < total; p0 += PTW_TILE) {
+                const int cnt = min(PTW_TILE, total - p0);
+                for (int p = lane; p < cnt; p += 32) {
+                    const int gp = p0 + p;
+                    int lo = 0, hi = nseg - 1;  // the segment holding staged point gp
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (soff[warp][mid] <= gp)
+                            lo = mid;
+                        else
+                            hi = mid - 1;
+                    }
+                    const PtSrc& Q = seg[warp][lo];
+                    const int q = gp - soff[warp][lo];
+                    const double* xp = Q.src.x + 3 * q;
+                    sp[warp][p] = make_float4((float)(Q.src.scale * xp[0] + Q.src.shift[0] - cx),
+                                              (float)(Q.src.scale * xp[1] + Q.src.shift[1] - cy),
+                                              (float)(Q.src.scale * xp[2] + Q.src.shift[2] - cz), 0.f);
+                    sd[warp][p] = reinterpret_cast<const float2*>(Q.den)[q];
+                }
+                __syncwarp();
+                if (MODE == 0) {
+                    for (int p = 0; p < cnt; ++p) {
+                        const float4 s = sp[warp][p];
+                        const float2 dv = sd[warp][p];
+#pragma unroll
+                        for (int i = 0; i < NT; ++i)
+                            cfma32(acc[i], kfun32f(tx[i] - s.x, ty[i] - s.y, tz[i] - s.z, S.kernel), dv);
+                    }
+                } else {
+                    for (int p = lane; p < cnt; p += 32) {
+                        const float4 s = sp[warp][p];
+                        const float2 dv = sd[warp][p];
+#pragma unroll
+                        for (int i = 0; i < NT; ++i)
+                            if (t0 + i < T.n) cfma32(acc[i], kfun32f(tx[i] - s.x, ty[i] - s.y, tz[i] - s.z, S.kernel), dv);
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        if (MODE == 0) {
+#pragma unroll
+            for (int i = 0; i < NT; ++i) {
+                const int t = t0 + lane + 32 * i;
+                if (t < T.n) {
+                    const float2 o = out[t];
+                    out[t] = make_float2(o.x + acc[i].x, o.y + acc[i].y);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < NT; ++i) {
+#pragma unroll
+                for (int d = 16; d > 0; d >>= 1) {
+                    acc[i].x += __shfl_xor_sync(0xffffffffu, acc[i].x, d);
+                    acc[i].y += __shfl_xor_sync(0xffffffffu, acc[i].y, d);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < NT; ++i)
+                if (lane == i && t0 + i < T.n) {
+                    const float2 o = out[t0 + i];
+                    out[t0 + i] = make_float2(o.x + acc[i].x, o.y + acc[i].y);
+                }
+        }
+    }
+}
+
 void launch_pt32(const PtSub* subs, const int* prefix, int nsub, int nitems, const int* active, cudaStream_t s,
                  int tpi) {
     if (nitems == 0) return;
+    if (tpi == PT_WARP_TARGETS || tpi == PT_WARP_SOURCES) {
+        const int blocks = (nitems + PTW_WARPS - 1) / PTW_WARPS;
+        if (tpi == PT_WARP_TARGETS)
+            pt32w_kernel<0><<<blocks, 32 * PTW_WARPS, 0, s>>>(subs, prefix, nsub, nitems, active);
+        else
+            pt32w_kernel<1><<<blocks, 32 * PTW_WARPS, 0, s>>>(subs, prefix, nsub, nitems, active);
+        return;
+    }
     const int blocks = (int)(((long long)nitems * tpi + 255) / 256);
     switch (tpi) {
         case 4: pt32_kernel<4><<<blocks, 256, 0, s>>>(subs, prefix, nsub, nitems, active); break;
@@ -294,15 +452,16 @@ void launch_pt32(const PtSub* subs, const int* prefix, int nsub, int nitems, con
 // spectra array (fixed-scratch entry point, single instance).
 // MULTI = false: the single sub-launch `one` (kernel parameter space, as a
 // one-instance launch); MULTI = true: the block's sub-launch from `subs`.
-template <bool MULTI>
+template <int G>
 __device__ __forceinline__ void vlist_forward32_body(const VfSub& S, int local, float2* spec_override);
 
-template <bool MULTI>
-__global__ void __launch_bounds__(256) vlist_forward32_kernel(const VfSub one, const VfSub* __restrict__ subs,
-                                                              const int* __restrict__ prefix, int nsub,
-                                                              const int* __restrict__ active, float2* spec_override) {
+template <int G, bool MULTI>
+__global__ void __launch_bounds__(vt_threads(G)) vlist_forward32_kernel(const VfSub one, const VfSub* __restrict__ subs,
+                                                                        const int* __restrict__ prefix, int nsub,
+                                                                        const int* __restrict__ active,
+                                                                        float2* spec_override) {
     if (!MULTI) {
-        vlist_forward32_body<MULTI>(one, blockIdx.x, spec_override);
+        vlist_forward32_body<G>(one, blockIdx.x, spec_override);
         return;
     }
     __shared__ VfSub Sm;
@@ -314,140 +473,216 @@ __global__ void __launch_bounds__(256) vlist_forward32_kernel(const VfSub one, c
     }
     __syncthreads();
     if (active && !active[Sm.inst]) return;
-    vlist_forward32_body<MULTI>(Sm, lm, spec_override);
+    vlist_forward32_body<G>(Sm, lm, spec_override);
 }
 
-template <bool MULTI>
+// The forward transform of kernels.cu (vlist_forward_kernel) in complex FP32.
+template <int G>
 __device__ __forceinline__ void vlist_forward32_body(const VfSub& S, int local, float2* spec_override) {
+    constexpr int P = G / 2, PP = P * P, G2 = G * G;
     extern __shared__ float2 sm32[];
+    float2* W = sm32;               // W[k * P + a]
+    float2* cube = W + G * P;       // [c'][b'][a']
+    float2* b1 = cube + PP * P;     // [c'][b'][ka]
+    float2* b2 = b1 + PP * G;       // [c'][kb][ka]
     const VlistLevel& L = S.L;
     const float2* twf = reinterpret_cast<const float2*>(L.twf);
     const float2* upeq = S.upeq;
     float2* spec = spec_override ? spec_override : S.spec;
-    const int G = L.G, P = L.P, PP = P * P;
-    float2* cube = sm32;
-    float2* b1 = cube + PP * P;
-    float2* b2 = b1 + G * PP;
+    const int tid = threadIdx.x, nt = blockDim.x;
     const int b = S.boxes[local];
-    for (int e = threadIdx.x; e < PP * P; e += blockDim.x) cube[e] = make_float2(0.f, 0.f);
+    for (int e = tid; e < G * P; e += nt) W[e] = twf[((P + e % P) * (e / P)) % G];
+    for (int e = tid; e < PP * P; e += nt) cube[e] = make_float2(0.f, 0.f);
     __syncthreads();
-    for (int k = threadIdx.x; k < L.nE; k += blockDim.x) cube[L.cube_idx[k]] = upeq[(size_t)b * L.nE + k];
+    for (int k = tid; k < L.nE; k += nt) cube[L.cube_idx[k]] = upeq[(size_t)b * L.nE + k];
     __syncthreads();
-    for (int e = threadIdx.x; e < G * PP; e += blockDim.x) {
-        int ka = e % G, line = e / G;
-        float2 acc = make_float2(0.f, 0.f);
-        for (int a = 0; a < P; ++a) cfma32(acc, cube[line * P + a], twf[((P + a) * ka) % G]);
-        b1[e] = acc;
+    if (const int line = tid; line < PP) {  // one line per thread: nt >= G^2
+        float2 x[P];
+#pragma unroll
+        for (int a = 0; a < P; ++a) x[a] = cube[line * P + a];
+#pragma unroll
+        for (int k = 0; k < G; ++k) {
+            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int a = 0; a < P; ++a) cfma32(acc, x[a], W[k * P + a]);
+            b1[line * G + k] = acc;
+        }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < G * G * P; e += blockDim.x) {
-        int ka = e % G, kb = (e / G) % G, c = e / (G * G);
-        float2 acc = make_float2(0.f, 0.f);
-        for (int bb = 0; bb < P; ++bb) cfma32(acc, b1[(c * P + bb) * G + ka], twf[((P + bb) * kb) % G]);
-        b2[e] = acc;
+    if (const int e = tid; e < P * G) {
+        const int c = e / G, ka = e % G;
+        float2 x[P];
+#pragma unroll
+        for (int bb = 0; bb < P; ++bb) x[bb] = b1[(c * P + bb) * G + ka];
+#pragma unroll
+        for (int k = 0; k < G; ++k) {
+            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int bb = 0; bb < P; ++bb) cfma32(acc, x[bb], W[k * P + bb]);
+            b2[(c * G + k) * G + ka] = acc;
+        }
     }
     __syncthreads();
-    float2* o = spec + (size_t)b * G * G * G;
-    for (int e = threadIdx.x; e < G * G * G; e += blockDim.x) {
-        int kab = e % (G * G), kc = e / (G * G);
-        float2 acc = make_float2(0.f, 0.f);
-        for (int c = 0; c < P; ++c) cfma32(acc, b2[c * G * G + kab], twf[((P + c) * kc) % G]);
-        o[e] = acc;
+    float2* o = spec + (size_t)b * G2 * G;
+    if (const int kab = tid; kab < G2) {
+        float2 x[P];
+#pragma unroll
+        for (int c = 0; c < P; ++c) x[c] = b2[c * G2 + kab];
+#pragma unroll
+        for (int k = 0; k < G; ++k) {
+            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int c = 0; c < P; ++c) cfma32(acc, x[c], W[k * P + c]);
+            o[k * G2 + kab] = acc;
+        }
     }
 }
 
-// V-list sums by target parent (see vlist_group_kernel in kernels.cu): warp =
-// one group (target parent), lane = one frequency of a 32-frequency chunk
-// (blockIdx.y).  MULTI: each warp finds its own sub-launch from the prefix
-// sums of the groups; spec_override replaces the source spectra (single
-// instance).
+// V-list sums by target parent (vlist_group_kernel in kernels.cu) in complex
+// FP32: the chunk's slice of the 343 translation tensors in shared memory,
+// warp = one group per round, lane = one frequency of the block's chunk, source
+// values loaded four entries ahead.  A block's groups belong to one sub-launch
+// (the work items of a launch are blocks, vgroup_blocks(ngroups) per
+// sub-launch); spec_override replaces the source spectra (single instance).
 __host__ __device__ constexpr int child_voff32(int c) { return ((c >> 2) & 1) + 7 * ((c >> 1) & 1) + 49 * (c & 1); }
+constexpr int VT_OFFSETS32 = 343;
 
 template <int G, bool MULTI>
-__global__ void __launch_bounds__(256) vlist_group32_kernel(const VaSub one, const VaSub* __restrict__ subs,
-                                                            const int* __restrict__ prefix, int nsub, int ngroups,
-                                                            const int* __restrict__ active,
-                                                            const float2* spec_override) {
+__global__ void __launch_bounds__(32 * VGROUP_WARPS) vlist_group32_kernel(const VaSub one,
+                                                                          const VaSub* __restrict__ subs,
+                                                                          const int* __restrict__ prefix, int nsub,
+                                                                          const int* __restrict__ active,
+                                                                          const float2* spec_override) {
     constexpr int G3 = G * G * G;
-    const int g = blockIdx.x * VGROUP_WARPS + (threadIdx.x >> 5);
-    if (g >= ngroups) return;
-    int j = 0, grp = g;
+    extern __shared__ float2 tsm32[];  // [offset][lane]
+    __shared__ VaSub Sm;
+    __shared__ int lb;
     if (MULTI) {
-        j = find_sub(prefix, nsub, g);
-        grp = g - __ldg(prefix + j);
+        if (threadIdx.x == 0) {
+            const int j = find_sub(prefix, nsub, (int)blockIdx.x);
+            Sm = subs[j];
+            lb = blockIdx.x - prefix[j];
+        }
+        __syncthreads();
     }
-    const VaSub& S = MULTI ? subs[j] : one;
-    if (MULTI && active && !active[S.inst]) return;
-    const float2* __restrict__ spec = spec_override ? spec_override : S.spec;
+    const VaSub& S = MULTI ? Sm : one;
+    const int b = MULTI ? lb : blockIdx.x;
+    if (MULTI && active && !active[S.inst]) return;  // the whole block
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int chunk = blockIdx.y, f = chunk * 32 + lane;
     const float2* __restrict__ tns = reinterpret_cast<const float2*>(S.L.tns);
-    const int f = blockIdx.y * 32 + (threadIdx.x & 31);
-    float2 acc[8];
+    for (int i = threadIdx.x; i < VT_OFFSETS32 * 32; i += blockDim.x)
+        tsm32[i] = __ldg(tns + (size_t)(i >> 5) * G3 + chunk * 32 + (i & 31));
+    __syncthreads();
+    const float2* __restrict__ spec = spec_override ? spec_override : S.spec;
+    for (int r = 0; r < VGROUP_ROUNDS; ++r) {
+        const int grp = (b * VGROUP_ROUNDS + r) * VGROUP_WARPS + warp;
+        if (grp >= S.ngroups) break;  // warp-uniform; no block-wide sync below
+        float2 acc[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) acc[c] = make_float2(0.f, 0.f);
-    const int e1 = __ldg(S.gptr + grp + 1);
-    for (int e = __ldg(S.gptr + grp); e < e1; ++e) {
-        const int2 ent = __ldg(S.gsrc + e);
-        const float2 sv = __ldg(spec + (size_t)ent.x * G3 + f);
-        const int mask = ent.y & 255;
-        const float2* tb = tns + (size_t)(ent.y >> 8) * G3 + f;
+        for (int c = 0; c < 8; ++c) acc[c] = make_float2(0.f, 0.f);
+        const int e0 = __ldg(S.gptr + grp), e1 = __ldg(S.gptr + grp + 1);
+        for (int base = e0; base < e1; base += 32) {
+            const int n = min(32, e1 - base);
+            const int2 mine = lane < n ? __ldg(S.gsrc + base + lane) : make_int2(0, 0);
+            float2 sv[4];
 #pragma unroll
-        for (int c = 0; c < 8; ++c)
-            if (mask & (1 << c)) cfma32(acc[c], __ldg(tb + (size_t)child_voff32(c) * G3), sv);
-    }
-    float2* tsp = S.tsp;
+            for (int u = 0; u < 4; ++u)
+                if (u < n) sv[u] = __ldg(spec + (size_t)__shfl_sync(0xffffffffu, mine.x, u) * G3 + f);
+            for (int k = 0; k < n; k += 4) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        const int t = __ldg(S.gtrg + 8 * grp + c);
-        if (t >= 0) tsp[(size_t)t * G3 + f] = acc[c];
+                for (int u = 0; u < 4; ++u) {
+                    const int kk = k + u;
+                    if (kk < n) {
+                        const int y = __shfl_sync(0xffffffffu, mine.y, kk);
+                        const float2 sval = sv[u];
+                        if (kk + 4 < n) sv[u] = __ldg(spec + (size_t)__shfl_sync(0xffffffffu, mine.x, kk + 4) * G3 + f);
+                        const int mask = y & 255;
+                        const float2* tb = tsm32 + (y >> 8) * 32 + lane;
+#pragma unroll
+                        for (int c = 0; c < 8; ++c)
+                            if (mask & (1 << c)) cfma32(acc[c], tb[child_voff32(c) * 32], sval);
+                    }
+                }
+            }
+        }
+        float2* tsp = S.tsp;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int t = __ldg(S.gtrg + 8 * grp + c);
+            if (t >= 0) tsp[(size_t)t * G3 + f] = acc[c];
+        }
     }
 }
 
-// Pruned inverse DFT of one target's summed spectrum, one block per target
-// (vlist_inverse_kernel in kernels.cu in complex FP32).
+// The inverse transform of kernels.cu (vlist_inverse_kernel) in complex FP32,
+// one block per target.
 template <int G>
 __device__ __forceinline__ void vlist_inverse32_body(const ViSub& S, int ti) {
+    constexpr int P = G / 2, PP = P * P, G2 = G * G, G3 = G2 * G;
     extern __shared__ float2 sm32[];
-    constexpr int P = G / 2, PP = P * P, G3 = G * G * G;
+    float2* W = sm32;               // W[a * G + k]
+    float2* c1 = W + P * G;         // [c'][kb][ka]
+    float2* c2 = c1 + P * G2;       // [c'][b'][ka]
+    float2* c3 = c2 + PP * G;       // [c'][b'][a']
     const VlistLevel& L = S.L;
     const float2* twb = reinterpret_cast<const float2*>(L.twb);
     float2* dnchk = S.dnchk;
-    float2* grid = sm32;
-    float2* c1 = sm32 + G3;
+    const int tid = threadIdx.x, nt = blockDim.x;
     const int t = S.trg[ti];
+    for (int e = tid; e < P * G; e += nt) W[e] = twb[((P + e / G) * (e % G)) % G];
+    __syncthreads();
     const float2* src = S.tsp + (size_t)ti * G3;
-    for (int e = threadIdx.x; e < G3; e += blockDim.x) grid[e] = __ldg(src + e);
-    __syncthreads();
-    for (int e = threadIdx.x; e < G * G * P; e += blockDim.x) {
-        int kab = e % (G * G), c = e / (G * G);
-        float2 s = make_float2(0.f, 0.f);
-        for (int kc = 0; kc < G; ++kc) cfma32(s, grid[kc * G * G + kab], twb[((P + c) * kc) % G]);
-        c1[e] = s;
+    if (const int kab = tid; kab < G2) {
+        float2 x[G];
+#pragma unroll
+        for (int k = 0; k < G; ++k) x[k] = __ldg(src + k * G2 + kab);
+#pragma unroll
+        for (int c = 0; c < P; ++c) {
+            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < G; ++k) cfma32(acc, x[k], W[c * G + k]);
+            c1[c * G2 + kab] = acc;
+        }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < G * PP; e += blockDim.x) {
-        int ka = e % G, bb = (e / G) % P, c = e / (G * P);
-        float2 s = make_float2(0.f, 0.f);
-        for (int kb = 0; kb < G; ++kb) cfma32(s, c1[(c * G + kb) * G + ka], twb[((P + bb) * kb) % G]);
-        grid[e] = s;
+    if (const int e = tid; e < P * G) {
+        const int c = e / G, ka = e % G;
+        float2 x[G];
+#pragma unroll
+        for (int k = 0; k < G; ++k) x[k] = c1[(c * G + k) * G + ka];
+#pragma unroll
+        for (int bb = 0; bb < P; ++bb) {
+            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < G; ++k) cfma32(acc, x[k], W[bb * G + k]);
+            c2[(c * P + bb) * G + ka] = acc;
+        }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < PP * P; e += blockDim.x) {
-        int a = e % P, line = e / P;
-        float2 s = make_float2(0.f, 0.f);
-        for (int ka = 0; ka < G; ++ka) cfma32(s, grid[line * G + ka], twb[((P + a) * ka) % G]);
-        c1[e] = s;
+    if (const int line = tid; line < PP) {  // one line per thread: nt >= G^2
+        float2 x[G];
+#pragma unroll
+        for (int k = 0; k < G; ++k) x[k] = c2[line * G + k];
+#pragma unroll
+        for (int a = 0; a < P; ++a) {
+            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < G; ++k) cfma32(acc, x[k], W[a * G + k]);
+            c3[line * P + a] = acc;
+        }
     }
     __syncthreads();
     const float coef = 1.0f / (float)G3;
-    for (int k = threadIdx.x; k < L.nE; k += blockDim.x) {
-        float2 v = c1[L.cube_idx[k]];
+    for (int k = tid; k < L.nE; k += nt) {
+        float2 v = c3[L.cube_idx[k]];
         float2 o = dnchk[(size_t)t * L.nE + k];
         dnchk[(size_t)t * L.nE + k] = make_float2(o.x + v.x * coef, o.y + v.y * coef);
     }
 }
 
 template <int G, bool MULTI>
-__global__ void __launch_bounds__(256) vlist_inverse32_kernel(const ViSub one, const ViSub* __restrict__ subs,
+__global__ void __launch_bounds__(vt_threads(G)) vlist_inverse32_kernel(const ViSub one, const ViSub* __restrict__ subs,
                                                               const int* __restrict__ prefix, int nsub,
                                                               const int* __restrict__ active) {
     if (!MULTI) {
@@ -466,21 +701,24 @@ __global__ void __launch_bounds__(256) vlist_inverse32_kernel(const ViSub one, c
     vlist_inverse32_body<G>(Sm, lm);
 }
 
-static size_t vfwd32_smem(int G, int P) { return sizeof(float2) * (P * P * P + G * P * P + G * G * P); }
-static size_t vinv32_smem(int G, int P) { return sizeof(float2) * (G * G * G + G * G * P); }
-
-void vlist32_init(int G) {
-    int P = G / 2;
-    const int fs = (int)vfwd32_smem(G, P);
-    cudaFuncSetAttribute(vlist_forward32_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, fs);
-    cudaFuncSetAttribute(vlist_forward32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, fs);
-    const int a8 = (int)vinv32_smem(8, 4), a12 = (int)vinv32_smem(12, 6), a16 = (int)vinv32_smem(16, 8);
-    cudaFuncSetAttribute(vlist_inverse32_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a8);
-    cudaFuncSetAttribute(vlist_inverse32_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, a8);
-    cudaFuncSetAttribute(vlist_inverse32_kernel<12, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a12);
-    cudaFuncSetAttribute(vlist_inverse32_kernel<12, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, a12);
-    cudaFuncSetAttribute(vlist_inverse32_kernel<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, a16);
-    cudaFuncSetAttribute(vlist_inverse32_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, a16);
+void vlist32_init(int) {
+    const int gs = (int)(sizeof(float2) * VT_OFFSETS32 * 32);
+    cudaFuncSetAttribute(vlist_group32_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
+    cudaFuncSetAttribute(vlist_group32_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
+    cudaFuncSetAttribute(vlist_group32_kernel<12, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
+    cudaFuncSetAttribute(vlist_group32_kernel<12, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
+    cudaFuncSetAttribute(vlist_group32_kernel<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
+    cudaFuncSetAttribute(vlist_group32_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
+#define DDFMM_VT_ATTR(k, g)                                                                      \
+    cudaFuncSetAttribute(k<g, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(g, 8)); \
+    cudaFuncSetAttribute(k<g, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(g, 8));
+    DDFMM_VT_ATTR(vlist_forward32_kernel, 8)
+    DDFMM_VT_ATTR(vlist_forward32_kernel, 12)
+    DDFMM_VT_ATTR(vlist_forward32_kernel, 16)
+    DDFMM_VT_ATTR(vlist_inverse32_kernel, 8)
+    DDFMM_VT_ATTR(vlist_inverse32_kernel, 12)
+    DDFMM_VT_ATTR(vlist_inverse32_kernel, 16)
+#undef DDFMM_VT_ATTR
 }
 
 // L.tns, L.twf, L.twb hold float2 data in this form.
@@ -492,29 +730,38 @@ void launch_vlist_forward32(const VfSub* subs, const int* prefix, int nsub, int 
         if (!one) return;  // a single sub-launch is passed by value
         o = *one;
     }
-    const size_t sm = vfwd32_smem(G, G / 2);
+    const size_t sm = vt_smem(G, sizeof(float2));
     float2* so = static_cast<float2*>(spec_override);
-    if (nsub == 1)
-        vlist_forward32_kernel<false><<<nbox, 256, sm, s>>>(o, subs, prefix, nsub, active, so);
-    else
-        vlist_forward32_kernel<true><<<nbox, 256, sm, s>>>(o, subs, prefix, nsub, active, so);
+#define DDFMM_VFWD(g)                                                                                   \
+    if (nsub == 1)                                                                                      \
+        vlist_forward32_kernel<g, false><<<nbox, vt_threads(g), sm, s>>>(o, subs, prefix, nsub, active, so); \
+    else                                                                                                \
+        vlist_forward32_kernel<g, true><<<nbox, vt_threads(g), sm, s>>>(o, subs, prefix, nsub, active, so);
+    switch (G) {
+        case 8: DDFMM_VFWD(8) break;
+        case 12: DDFMM_VFWD(12) break;
+        case 16: DDFMM_VFWD(16) break;
+        default: break;
+    }
+#undef DDFMM_VFWD
 }
 
-void launch_vlist_group32(const VaSub* subs, const int* prefix, int nsub, int ngroups, int G, const int* active,
+void launch_vlist_group32(const VaSub* subs, const int* prefix, int nsub, int nblocks, int G, const int* active,
                           const void* spec_override, cudaStream_t s, const VaSub* one) {
-    if (ngroups == 0) return;
+    if (nblocks == 0) return;
     VaSub o{};
     if (nsub == 1) {
         if (!one) return;  // a single sub-launch is passed by value
         o = *one;
     }
-    const dim3 grid((ngroups + VGROUP_WARPS - 1) / VGROUP_WARPS, G * G * G / 32);
+    const dim3 grid(nblocks, G * G * G / 32);
+    const size_t sm = sizeof(float2) * VT_OFFSETS32 * 32;
     const float2* so = static_cast<const float2*>(spec_override);
-#define DDFMM_VGRP(g)                                                                                             \
-    if (nsub == 1)                                                                                                \
-        vlist_group32_kernel<g, false><<<grid, 32 * VGROUP_WARPS, 0, s>>>(o, subs, prefix, nsub, ngroups, active, so); \
-    else                                                                                                          \
-        vlist_group32_kernel<g, true><<<grid, 32 * VGROUP_WARPS, 0, s>>>(o, subs, prefix, nsub, ngroups, active, so);
+#define DDFMM_VGRP(g)                                                                                                \
+    if (nsub == 1)                                                                                                   \
+        vlist_group32_kernel<g, false><<<grid, 32 * VGROUP_WARPS, sm, s>>>(o, subs, prefix, nsub, active, so);       \
+    else                                                                                                             \
+        vlist_group32_kernel<g, true><<<grid, 32 * VGROUP_WARPS, sm, s>>>(o, subs, prefix, nsub, active, so);
     switch (G) {
         case 8: DDFMM_VGRP(8) break;
         case 12: DDFMM_VGRP(12) break;
@@ -532,12 +779,12 @@ void launch_vlist_inverse32(const ViSub* subs, const int* prefix, int nsub, int 
         if (!one) return;  // a single sub-launch is passed by value
         o = *one;
     }
-    const size_t sm = vinv32_smem(G, G / 2);
-#define DDFMM_VINV(g)                                                                          \
-    if (nsub == 1)                                                                             \
-        vlist_inverse32_kernel<g, false><<<ntrg, 256, sm, s>>>(o, subs, prefix, nsub, active); \
-    else                                                                                       \
-        vlist_inverse32_kernel<g, true><<<ntrg, 256, sm, s>>>(o, subs, prefix, nsub, active);
+    const size_t sm = vt_smem(G, sizeof(float2));
+#define DDFMM_VINV(g)                                                                                   \
+    if (nsub == 1)                                                                                      \
+        vlist_inverse32_kernel<g, false><<<ntrg, vt_threads(g), sm, s>>>(o, subs, prefix, nsub, active); \
+    else                                                                                                \
+        vlist_inverse32_kernel<g, true><<<ntrg, vt_threads(g), sm, s>>>(o, subs, prefix, nsub, active);
     switch (G) {
         case 8: DDFMM_VINV(8) break;
         case 12: DDFMM_VINV(12) break;

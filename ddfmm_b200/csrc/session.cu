@@ -1310,7 +1310,7 @@ void Session::build() {
                 if (mixed) {
                     a.hva = VaSub{VL, a.v.grp.gptr, a.v.grp.gsrc, a.v.grp.gtrg, reinterpret_cast<const float2*>(lf_spec),
                                   reinterpret_cast<float2*>(tsp), ngroups, 0};
-                    set_multi(a, a.hva, ngroups);
+                    set_multi(a, a.hva, vgroup_blocks(ngroups));
                 }
                 push_step(a);
                 Step iv{};
@@ -1524,7 +1524,7 @@ void Session::autotune() {
         if (st.kind != 1) continue;
         float best = 0.f;
         int best_tpi = 32;
-        for (int tpi : {32, 16, 8, 4}) {
+        for (int tpi : {32, 16, 8, 4, PT_WARP_TARGETS, PT_WARP_SOURCES}) {
             st.tpi = tpi;
             launch_step(st, stream_, st.v.spec);  // warm-up
             CK(cudaEventRecord(a, stream_));

@@ -135,7 +135,7 @@ private:
         // that play the same part (phase, width, step type, occurrence): a Batch
         // merges the steps of its sessions that share a key into one launch.
         long long key;
-        int tpi;  // point interactions: threads per item (0 = 32), set by autotune()
+        int tpi;  // point interactions: launch shape (launch_pt; 0 = 32 threads per item), set by autotune()
         // mixed form: the step as a one-instance launch (device sub-launch array and
         // prefix sums) and the host copy of its sub-launch
         void* msubs;
