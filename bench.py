@@ -44,8 +44,8 @@ def parse():
     ap.add_argument("--profile-json", default=None, help="write the per-pass profile here")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form measurement")
     ap.add_argument("--no-served", action="store_true", help="skip the continuous-batching server measurement")
-    ap.add_argument("--batched", action="store_true",
-                    help="also measure 64 uneven instances evaluated as one batch (about two minutes of setup)")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the 64 uneven instances evaluated as one batch")
     ap.add_argument("--ellipsoid-table", default=None,
                     help="only tabulate the mixed form on the ellipsoid (K=128, N=900k by default) for the given "
                          "ACCU levels and kernels, optionally K and the form (mixed or plain), e.g. '1,2:0,1' or "
@@ -379,7 +379,7 @@ def measure_served(large_plain_e2e_s, budget_gb=30.0, closed_s=4.0, poisson_s=4.
     t0 = time.perf_counter()
     sv = wave3d.Server(budget_bytes=budget_gb * 1e9)
     sids = [sv.add_workload(w) for w in ws_list]
-    states = sv.wait_admitted(sids)
+    states = sv.wait_admitted(sids, timeout=240.0)
     admit_s = time.perf_counter() - t0
     live = [(sid, w) for sid, w, st in zip(sids, ws_list, states) if st == sv.ADMITTED]
     rng = np.random.default_rng(5)
@@ -472,6 +472,22 @@ def measure_served(large_plain_e2e_s, budget_gb=30.0, closed_s=4.0, poisson_s=4.
             "io": "host complex64 arrays in and out of the server (pinned staging, H2D/D2H inside each request)"}
 
 
+def create_sessions(ws_list, precision, workers=8):
+    """Sessions for every workload, created by a pool of threads (the C calls
+    release the interpreter lock); the widest instance first and alone, so
+    that the others find its translation operators in the shared cache."""
+    from concurrent.futures import ThreadPoolExecutor
+    from ddfmm_b200 import wave3d
+    first = max(range(len(ws_list)), key=lambda i: ws_list[i].K)
+    out = [None] * len(ws_list)
+    out[first] = wave3d.from_workload(ws_list[first], precision=precision)
+    with ThreadPoolExecutor(workers) as ex:
+        futs = {i: ex.submit(wave3d.from_workload, w, 0, precision) for i, w in enumerate(ws_list) if i != first}
+        for i, f in futs.items():
+            out[i] = f.result()
+    return out
+
+
 def measure_batched(steps=5):
     """64 independent instances (K drawn from 4, 8, 16, 32; spheres and
     ellipsoids; N = 25 pi K^2; P=6) evaluated as one batch (merged
@@ -483,7 +499,7 @@ def measure_batched(steps=5):
     Ks = [int(k) for k in rng.choice([4, 8, 16, 32], 64)]
     ws_list = instance_mix(Ks, 100)
     t0 = time.perf_counter()
-    waves = [wave3d.from_workload(w, precision=_lib.MIXED) for w in ws_list]
+    waves = create_sessions(ws_list, _lib.MIXED)
     setup_s = time.perf_counter() - t0
     dev_gb = sum(wv.stats()["device_bytes"] for wv in waves) / 1e9
     b = wave3d.Batch(waves)
@@ -521,23 +537,28 @@ def measure_batched(steps=5):
     b.close()
     for wv in waves:
         wv.close()
-    # one after another, plain FP64 (sessions created one at a time)
+    # one after another, plain FP64 (created three at a time ahead of their timing, then closed)
+    from concurrent.futures import ThreadPoolExecutor
     plain_ms = 0.0
-    for w in ws_list:
-        p = wave3d.from_workload(w, precision=_lib.PLAIN_FP64)
-        d = torch.from_numpy(w.densities().view(np.float64)).cuda()
-        v = torch.empty_like(d)
-        p.eval_device(d.data_ptr(), v.data_ptr(), st.cuda_stream)
-        st.synchronize()
-        with torch.cuda.stream(st):
-            e0.record(st)
-        for _ in range(steps):
+    with ThreadPoolExecutor(3) as ex:
+        futs = [ex.submit(wave3d.from_workload, w, 0, _lib.PLAIN_FP64) for w in ws_list[:3]]
+        for i, w in enumerate(ws_list):
+            p = futs[i].result()
+            if i + 3 < len(ws_list):
+                futs.append(ex.submit(wave3d.from_workload, ws_list[i + 3], 0, _lib.PLAIN_FP64))
+            d = torch.from_numpy(w.densities().view(np.float64)).cuda()
+            v = torch.empty_like(d)
             p.eval_device(d.data_ptr(), v.data_ptr(), st.cuda_stream)
-        with torch.cuda.stream(st):
-            e1.record(st)
-        st.synchronize()
-        plain_ms += e0.elapsed_time(e1) / steps
-        p.close()
+            st.synchronize()
+            with torch.cuda.stream(st):
+                e0.record(st)
+            for _ in range(steps):
+                p.eval_device(d.data_ptr(), v.data_ptr(), st.cuda_stream)
+            with torch.cuda.stream(st):
+                e1.record(st)
+            st.synchronize()
+            plain_ms += e0.elapsed_time(e1) / steps
+            p.close()
     n = len(ws_list)
     return {"instances": n, "K_counts": {str(k): Ks.count(k) for k in (4, 8, 16, 32)},
             "points": int(sum(w.N for w in ws_list)), "setup_s": setup_s, "device_gb": dev_gb,
@@ -678,7 +699,7 @@ def run_ours(args):
     dom = max(by_kernel, key=lambda k: by_kernel[k]["ms"])
     dk = by_kernel[dom]
     peaks = measured_peaks()
-    if dom in ("zgemm_kernel", "pt_kernel"):
+    if dom == "zgemm_kernel" or dom.startswith("pt"):
         peak = fp64_peak_tflops(torch, dev)
         achieved = dk["flops"] / (dk["ms"] * 1e-3) / 1e12
         roof = {"bound": "tensor", "pipe": "FP64 DMMA (mma.sync.m8n8k4.f64)", "kernel": dom, "achieved": achieved,
@@ -719,7 +740,7 @@ def run_ours(args):
     served = None
     if not args.no_served and ws == 1 and args.workload == "large":
         served = measure_served(e2e_s)
-    batched = measure_batched() if args.batched and ws == 1 else None
+    batched = measure_batched() if not args.no_batched and ws == 1 and args.workload == "large" else None
     mixed_mma = None
     if args.mixed_mma_sync:
         from ddfmm_b200 import _lib
@@ -736,6 +757,7 @@ def run_ours(args):
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
                 "config": bench_config(w),
                 "form": "plain FP64", "parallelism": "replicas" if ws > 1 else "single GPU", "setup_s": setup_s,
+                "setup_split_s": {k: st[k] for k in ("ops_seconds", "tree_seconds", "plan_seconds", "tune_seconds")},
                 "device_gb": st["device_bytes"] / 1e9,
                 "e2e": {"value": whole_job_rate(1e3 * e2e_s, ws) * w.N, "unit": "points/s",
                         "h2d_bytes_per_step": 16 * w.N, "d2h_bytes_per_step": 16 * w.N,

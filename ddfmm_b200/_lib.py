@@ -41,7 +41,8 @@ class ddfmm_stats(C.Structure):
         ("hf_up_nodes", C.c_longlong), ("hf_down_nodes", C.c_longlong), ("hf_far_pairs", C.c_longlong),
         ("m2l_matrices", C.c_longlong), ("gemm_launches", C.c_longlong), ("kernel_launches", C.c_longlong),
         ("flops_gemm", C.c_double), ("fft_spectra_bytes", C.c_longlong), ("setup_seconds", C.c_double),
-        ("device_bytes", C.c_longlong),
+        ("device_bytes", C.c_longlong), ("ops_seconds", C.c_double), ("tree_seconds", C.c_double),
+        ("plan_seconds", C.c_double), ("tune_seconds", C.c_double),
     ]
 
     def as_dict(self):

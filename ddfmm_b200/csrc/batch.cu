@@ -138,7 +138,7 @@ Batch::Batch(const std::vector<Session*>& sessions) : sessions_(sessions) {
                             VaSub u = e.second->hva;
                             u.inst = e.first;
                             subs.push_back(u);
-                            n.push_back(vgroup_blocks(u.ngroups));
+                            n.push_back(u.ngroups);
                         }
                         add(VACC, subs, n, gg.first);
                     } else {

@@ -237,6 +237,10 @@ int ddfmm_session_stats(const ddfmm_session* s, ddfmm_stats* out) {
     out->flops_gemm = t.flops_gemm;
     out->fft_spectra_bytes = t.fft_spectra_bytes;
     out->setup_seconds = t.setup_seconds;
+    out->ops_seconds = t.ops_seconds;
+    out->tree_seconds = t.tree_seconds;
+    out->plan_seconds = t.plan_seconds;
+    out->tune_seconds = t.tune_seconds;
     out->device_bytes = (long long)t.device_bytes;
     return DDFMM_OK;
 }

@@ -57,9 +57,10 @@ void launch_kmat(const KmatJob* jobs, int njobs, long long total, int kernel, cu
 
 // ---------------------------------------------------------------- gemm
 // Grouped complex FP64 GEMM with gathered input columns and scattered output
-// columns, on the FP64 tensor path (mma.sync m8n8k4 f64).  A 256-thread block
+// columns, on the FP64 tensor path (mma.sync m16n8k8 f64; the m8n8k4 and
+// m16n8k16 shapes reach the same 37 TF/s on B200).  A 256-thread block
 // computes up to 64 rows x 64 columns; warp (wm, wn) owns the 16-row slab wm
-// (two 8-row MMA blocks) and columns wn*32 .. +32 (four 8-column blocks).  A
+// (one 16-row MMA block) and columns wn*32 .. +32 (four 8-column blocks).  A
 // complex block product takes three real MMAs (the three-multiplication form
 // of a complex product, Gauss's trick):
 //   P1 += Ar Br,  P2 += Ai Bi,  P3 += (Ar + Ai)(Br + Bi);
@@ -73,7 +74,8 @@ void launch_kmat(const KmatJob* jobs, int njobs, long long total, int kernel, cu
 // by the copy (src-size 0).  128-bit shared loads are served in 8-lane
 // phases (lanes with g in {2p, 2p+1}, tig 0..3); both fragment layouts put
 // those 8 granules in 8 different bank groups: the operator slice is stored
-// [k][row ^ 2*(k & 3)] and the column slice [col][k] with a 20-granule stride.
+// [k][row ^ 2*(k & 3)] and the column slice [col][k] with a 20-granule stride
+// (k = tig and tig + 4 of a fragment share k & 3, hence the same swizzle).
 constexpr int BM = 64, BN = 64, BK = 16, BKP = 20, GSTAGES = 3;
 constexpr int GSTAGE = BK * BM + BN * BKP;  // double2 per stage
 constexpr int GEMM_SMEM = GSTAGES * GSTAGE * (int)sizeof(double2);
@@ -489,70 +491,43 @@ __global__ void __launch_bounds__(vt_threads(G)) vlist_forward_kernel(VlistLevel
 }
 
 // The pointwise products of the V list, by target parent: warp w of a block
-// takes target parent (blockIdx.x VGROUP_ROUNDS + r) VGROUP_WARPS + w in round
-// r, lane l frequency 32 blockIdx.y + l of the G^3 grid, with one accumulator
-// per child position.  The block first copies the chunk's slice of all 343
-// translation tensors (343 x 32 values) into shared memory, so every tensor
-// value of a product is a conflict-free shared load.  The loop over a
-// parent's source entries is the same for the 32 lanes: entries are read 32
-// at a time (one per lane) and broadcast by shuffles, the child-mask branches
-// are warp-uniform, and the source spectrum values are loaded four entries
-// ahead.  A source value is loaded once and used by every child that lists
-// it.  Blocks of one chunk run together (blockIdx.x varies fastest), so the
-// chunk's slice of every source spectrum stays in L2 while the chunk lasts.
+// takes target parent blockIdx.x * VGROUP_WARPS + w and lane l frequency
+// 32 blockIdx.y + l of the G^3 grid, with one accumulator per child position.
+// The loop over the parent's source entries is the same for the 32 lanes, so
+// the child mask branches are warp-uniform; a source's spectrum value is
+// loaded once and used by every child that has it in its V list.  Blocks of
+// one frequency chunk run together (blockIdx.x varies fastest), so the
+// translation tensors' 32-frequency slices of that chunk (316 x 512 bytes)
+// stay in the SM's L1 while the chunk lasts, and the source spectra's slices
+// (32 MB over all boxes at the bench workload) in L2.
 __host__ __device__ constexpr int child_voff(int c) { return ((c >> 2) & 1) + 7 * ((c >> 1) & 1) + 49 * (c & 1); }
-constexpr int VT_OFFSETS = 343;
 
 template <int G>
-__global__ void __launch_bounds__(32 * VGROUP_WARPS) vlist_group_kernel(const int* __restrict__ gptr,
-                                                                        const int2* __restrict__ gsrc,
-                                                                        const int* __restrict__ gtrg, int ngroups,
-                                                                        const double2* __restrict__ spec,
-                                                                        const double2* __restrict__ tns,
-                                                                        double2* __restrict__ tsp) {
+__global__ void __launch_bounds__(256) vlist_group_kernel(const int* __restrict__ gptr, const int2* __restrict__ gsrc,
+                                                          const int* __restrict__ gtrg, int ngroups,
+                                                          const double2* __restrict__ spec,
+                                                          const double2* __restrict__ tns, double2* __restrict__ tsp) {
     constexpr int G3 = G * G * G;
-    extern __shared__ double2 tsm[];  // [offset][lane]
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int chunk = blockIdx.y, f = chunk * 32 + lane;
-    for (int i = threadIdx.x; i < VT_OFFSETS * 32; i += blockDim.x)
-        tsm[i] = __ldg(tns + (size_t)(i >> 5) * G3 + chunk * 32 + (i & 31));
-    __syncthreads();
-    for (int r = 0; r < VGROUP_ROUNDS; ++r) {
-        const int grp = (blockIdx.x * VGROUP_ROUNDS + r) * VGROUP_WARPS + warp;
-        if (grp >= ngroups) break;  // warp-uniform; no block-wide sync below
-        double2 acc[8];
+    const int grp = blockIdx.x * VGROUP_WARPS + (threadIdx.x >> 5);
+    if (grp >= ngroups) return;
+    const int f = blockIdx.y * 32 + (threadIdx.x & 31);
+    double2 acc[8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) acc[c] = make_double2(0.0, 0.0);
-        const int e0 = __ldg(gptr + grp), e1 = __ldg(gptr + grp + 1);
-        for (int base = e0; base < e1; base += 32) {
-            const int n = min(32, e1 - base);
-            const int2 mine = lane < n ? __ldg(gsrc + base + lane) : make_int2(0, 0);
-            double2 sv[4];
+    for (int c = 0; c < 8; ++c) acc[c] = make_double2(0.0, 0.0);
+    const int e1 = __ldg(gptr + grp + 1);
+    for (int e = __ldg(gptr + grp); e < e1; ++e) {
+        const int2 ent = __ldg(gsrc + e);
+        const double2 S = __ldg(spec + (size_t)ent.x * G3 + f);
+        const int mask = ent.y & 255;
+        const double2* tb = tns + (size_t)(ent.y >> 8) * G3 + f;
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (u < n) sv[u] = __ldg(spec + (size_t)__shfl_sync(0xffffffffu, mine.x, u) * G3 + f);
-            for (int k = 0; k < n; k += 4) {
+        for (int c = 0; c < 8; ++c)
+            if (mask & (1 << c)) cfma(acc[c], __ldg(tb + (size_t)child_voff(c) * G3), S);
+    }
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int kk = k + u;
-                    if (kk < n) {
-                        const int y = __shfl_sync(0xffffffffu, mine.y, kk);
-                        const double2 sval = sv[u];
-                        if (kk + 4 < n) sv[u] = __ldg(spec + (size_t)__shfl_sync(0xffffffffu, mine.x, kk + 4) * G3 + f);
-                        const int mask = y & 255;
-                        const double2* tb = tsm + (y >> 8) * 32 + lane;
-#pragma unroll
-                        for (int c = 0; c < 8; ++c)
-                            if (mask & (1 << c)) cfma(acc[c], tb[child_voff(c) * 32], sval);
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int t = __ldg(gtrg + 8 * grp + c);
-            if (t >= 0) tsp[(size_t)t * G3 + f] = acc[c];
-        }
+    for (int c = 0; c < 8; ++c) {
+        const int t = __ldg(gtrg + 8 * grp + c);
+        if (t >= 0) tsp[(size_t)t * G3 + f] = acc[c];
     }
 }
 
@@ -633,10 +608,6 @@ size_t vt_smem(int G, size_t es) {
 }
 
 void vlist_init(int) {
-    const int gs = (int)(sizeof(double2) * VT_OFFSETS * 32);
-    cudaFuncSetAttribute(vlist_group_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
-    cudaFuncSetAttribute(vlist_group_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
-    cudaFuncSetAttribute(vlist_group_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
     cudaFuncSetAttribute(vlist_forward_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(8, 16));
     cudaFuncSetAttribute(vlist_forward_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(12, 16));
     cudaFuncSetAttribute(vlist_forward_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(16, 16));
@@ -660,12 +631,11 @@ void launch_vlist_forward(const VlistLevel& L, const int* boxes, int nbox, const
 void launch_vlist_group(const VlistLevel& L, const VlistGroups& V, const double2* spec, double2* tsp,
                         cudaStream_t s) {
     if (V.ngroups == 0) return;
-    const dim3 grid(vgroup_blocks(V.ngroups), L.G * L.G * L.G / 32);
-    const size_t sm = sizeof(double2) * VT_OFFSETS * 32;
+    const dim3 grid((V.ngroups + VGROUP_WARPS - 1) / VGROUP_WARPS, L.G * L.G * L.G / 32);
     switch (L.G) {
-        case 8: vlist_group_kernel<8><<<grid, 32 * VGROUP_WARPS, sm, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
-        case 12: vlist_group_kernel<12><<<grid, 32 * VGROUP_WARPS, sm, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
-        case 16: vlist_group_kernel<16><<<grid, 32 * VGROUP_WARPS, sm, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
+        case 8: vlist_group_kernel<8><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
+        case 12: vlist_group_kernel<12><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
+        case 16: vlist_group_kernel<16><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
         default: break;
     }
 }

@@ -97,12 +97,7 @@ void launch_vlist_forward(const VlistLevel& L, const int* boxes, int nbox, const
 // pair for child position 0; child position c adds a + 7b + 49c'.
 // tsp[t] (G^3 per target, rows in group order) receives the summed spectrum
 // of target t, overwritten each eval.
-// A block of the sums takes VGROUP_WARPS x VGROUP_ROUNDS consecutive groups
-// (one per warp and round) of one instance and one 32-frequency chunk.
-constexpr int VGROUP_WARPS = 16, VGROUP_ROUNDS = 4;
-inline int vgroup_blocks(int ngroups) {
-    return (ngroups + VGROUP_WARPS * VGROUP_ROUNDS - 1) / (VGROUP_WARPS * VGROUP_ROUNDS);
-}
+constexpr int VGROUP_WARPS = 8;  // target parents per block of the sums
 struct VlistGroups {
     const int* gptr;   // ngroups + 1: the source entries of each group
     const int2* gsrc;  // the source entries
@@ -183,9 +178,8 @@ void vlist32_init(int G);
 // a kernel parameter); `subs` / `prefix` are then not read.
 void launch_vlist_forward32(const VfSub* subs, const int* prefix, int nsub, int nbox, int G, const int* active,
                             void* spec_override, cudaStream_t s, const VfSub* one);
-// work items: blocks of groups, vgroup_blocks(ngroups) per sub-launch (launch_vlist_group32),
-// or targets (launch_vlist_inverse32)
-void launch_vlist_group32(const VaSub* subs, const int* prefix, int nsub, int nblocks, int G, const int* active,
+// work items: groups (launch_vlist_group32) or targets (launch_vlist_inverse32)
+void launch_vlist_group32(const VaSub* subs, const int* prefix, int nsub, int ngroups, int G, const int* active,
                           const void* spec_override, cudaStream_t s, const VaSub* one);
 void launch_vlist_inverse32(const ViSub* subs, const int* prefix, int nsub, int ntrg, int G, const int* active,
                             cudaStream_t s, const ViSub* one);

@@ -276,36 +276,23 @@ __global__ void pt32_kernel(const PtSub* __restrict__ subs, const int* __restric
 }
 
 // Warp-tiled point interactions: one warp per item.  The item's source points
-// are staged in shared memory, PTW_TILE at a time, as FP32 coordinates
-// relative to a reference point of the item (its first target, in FP64): all
-// points of an item lie within a few boxes of it, so the FP32 differences and
-// the phase 2 pi r stay accurate wherever the item sits.  MODE 0: each lane
-// owns up to PTW_TPL targets (lane + 32 i) and walks the staged sources
-// (broadcast reads); MODE 1: the targets go PTW_TT at a time, each lane takes
-// every 32nd staged source and the per-target sums are reduced across the
-// warp with shuffles.  Segment descriptors are read 32 at a time into shared
-// memory; their point counts, prefix-summed across the warp, map a staged
-// point to its segment.
+// are staged in shared memory, PTW_TILE at a time, scaled and shifted once (in
+// FP64, not once per target); every difference is taken in FP64 and rounded
+// to FP32 before the kernel is evaluated, as in pt32_kernel, so |p_t - p_s|
+// is accurate to FP32 however close the pair (a coincident pair gives exactly
+// zero).  MODE 0: each lane owns up to PTW_TPL targets (lane + 32 i) and walks
+// the staged sources (broadcast reads); MODE 1: the targets go PTW_TT at a
+// time, each lane takes every 32nd staged source and the per-target sums are
+// reduced across the warp with shuffles.  Segment descriptors are read 32 at
+// a time into shared memory; their point counts, prefix-summed across the
+// warp, map a staged point to its segment.
 constexpr int PTW_WARPS = 8, PTW_TILE = 64, PTW_TPL = 4, PTW_TT = 8;
-
-__device__ __forceinline__ float2 kfun32f(float x, float y, float z, int kernel) {
-    float r2 = x * x + y * y + z * z;
-    if (r2 < 1e-16f) r2 = 1.0f;
-    float r = sqrtf(r2);
-    float s, c;
-    sincospif(2.0f * r, &s, &c);
-    if (kernel == KERNEL_HELM) {
-        float ir = 1.0f / r;
-        return make_float2(c * ir, s * ir);
-    }
-    return make_float2(c, s);
-}
 
 template <int MODE>
 __global__ void __launch_bounds__(32 * PTW_WARPS) pt32w_kernel(const PtSub* __restrict__ subs,
                                                                const int* __restrict__ prefix, int nsub, int nitems,
                                                                const int* __restrict__ active) {
-    __shared__ float4 sp[PTW_WARPS][PTW_TILE];
+    __shared__ double sx[PTW_WARPS][PTW_TILE], sy[PTW_WARPS][PTW_TILE], sz[PTW_WARPS][PTW_TILE];
     __shared__ float2 sd[PTW_WARPS][PTW_TILE];
     __shared__ PtSrc seg[PTW_WARPS][32];
     __shared__ int soff[PTW_WARPS][33];
@@ -318,25 +305,21 @@ __global__ void __launch_bounds__(32 * PTW_WARPS) pt32w_kernel(const PtSub* __re
     const PtItem it = S.items[w - prefix[j]];
     float2* out = reinterpret_cast<float2*>(it.out);
     const PtSet& T = it.trg;
-    if (T.n <= 0) return;
-    const double cx = T.scale * T.x[0] + T.shift[0], cy = T.scale * T.x[1] + T.shift[1],
-                 cz = T.scale * T.x[2] + T.shift[2];
-    auto trg_rel = [&](int t, float& x, float& y, float& z) {
-        const double* tp = T.x + 3 * t;
-        x = (float)(T.scale * tp[0] + T.shift[0] - cx);
-        y = (float)(T.scale * tp[1] + T.shift[1] - cy);
-        z = (float)(T.scale * tp[2] + T.shift[2] - cz);
-    };
+    constexpr int NT = MODE == 0 ? PTW_TPL : PTW_TT;
     constexpr int TCH = MODE == 0 ? 32 * PTW_TPL : PTW_TT;  // targets per pass
     for (int t0 = 0; t0 < T.n; t0 += TCH) {
-        float tx[MODE == 0 ? PTW_TPL : PTW_TT], ty[MODE == 0 ? PTW_TPL : PTW_TT], tz[MODE == 0 ? PTW_TPL : PTW_TT];
-        float2 acc[MODE == 0 ? PTW_TPL : PTW_TT];
-        constexpr int NT = MODE == 0 ? PTW_TPL : PTW_TT;
+        double tx[NT], ty[NT], tz[NT];
+        float2 acc[NT];
 #pragma unroll
         for (int i = 0; i < NT; ++i) {
             const int t = MODE == 0 ? t0 + lane + 32 * i : t0 + i;
-            tx[i] = ty[i] = tz[i] = 0.f;
-            if (t < T.n) trg_rel(t, tx[i], ty[i], tz[i]);
+            tx[i] = ty[i] = tz[i] = 0.0;
+            if (t < T.n) {
+                const double* tp = T.x + 3 * t;
+                tx[i] = T.scale * tp[0] + T.shift[0];
+                ty[i] = T.scale * tp[1] + T.shift[1];
+                tz[i] = T.scale * tp[2] + T.shift[2];
+            }
             acc[i] = make_float2(0.f, 0.f);
         }
         for (int sb = it.src_begin; sb < it.src_end; sb += 32) {
@@ -371,27 +354,27 @@ __global__ void __launch_bounds__(32 * PTW_WARPS) pt32w_kernel(const PtSub* __re
                     const PtSrc& Q = seg[warp][lo];
                     const int q = gp - soff[warp][lo];
                     const double* xp = Q.src.x + 3 * q;
-                    sp[warp][p] = make_float4((float)(Q.src.scale * xp[0] + Q.src.shift[0] - cx),
-                                              (float)(Q.src.scale * xp[1] + Q.src.shift[1] - cy),
-                                              (float)(Q.src.scale * xp[2] + Q.src.shift[2] - cz), 0.f);
+                    sx[warp][p] = Q.src.scale * xp[0] + Q.src.shift[0];
+                    sy[warp][p] = Q.src.scale * xp[1] + Q.src.shift[1];
+                    sz[warp][p] = Q.src.scale * xp[2] + Q.src.shift[2];
                     sd[warp][p] = reinterpret_cast<const float2*>(Q.den)[q];
                 }
                 __syncwarp();
                 if (MODE == 0) {
                     for (int p = 0; p < cnt; ++p) {
-                        const float4 s = sp[warp][p];
+                        const double px = sx[warp][p], py = sy[warp][p], pz = sz[warp][p];
                         const float2 dv = sd[warp][p];
 #pragma unroll
                         for (int i = 0; i < NT; ++i)
-                            cfma32(acc[i], kfun32f(tx[i] - s.x, ty[i] - s.y, tz[i] - s.z, S.kernel), dv);
+                            cfma32(acc[i], kfun32(tx[i] - px, ty[i] - py, tz[i] - pz, S.kernel), dv);
                     }
                 } else {
                     for (int p = lane; p < cnt; p += 32) {
-                        const float4 s = sp[warp][p];
+                        const double px = sx[warp][p], py = sy[warp][p], pz = sz[warp][p];
                         const float2 dv = sd[warp][p];
 #pragma unroll
                         for (int i = 0; i < NT; ++i)
-                            if (t0 + i < T.n) cfma32(acc[i], kfun32f(tx[i] - s.x, ty[i] - s.y, tz[i] - s.z, S.kernel), dv);
+                            if (t0 + i < T.n) cfma32(acc[i], kfun32(tx[i] - px, ty[i] - py, tz[i] - pz, S.kernel), dv);
                     }
                 }
                 __syncwarp();
@@ -538,80 +521,49 @@ __device__ __forceinline__ void vlist_forward32_body(const VfSub& S, int local, 
     }
 }
 
-// V-list sums by target parent (vlist_group_kernel in kernels.cu) in complex
-// FP32: the chunk's slice of the 343 translation tensors in shared memory,
-// warp = one group per round, lane = one frequency of the block's chunk, source
-// values loaded four entries ahead.  A block's groups belong to one sub-launch
-// (the work items of a launch are blocks, vgroup_blocks(ngroups) per
-// sub-launch); spec_override replaces the source spectra (single instance).
+// V-list sums by target parent (see vlist_group_kernel in kernels.cu): warp =
+// one group (target parent), lane = one frequency of a 32-frequency chunk
+// (blockIdx.y).  MULTI: each warp finds its own sub-launch from the prefix
+// sums of the groups; spec_override replaces the source spectra (single
+// instance).
 __host__ __device__ constexpr int child_voff32(int c) { return ((c >> 2) & 1) + 7 * ((c >> 1) & 1) + 49 * (c & 1); }
-constexpr int VT_OFFSETS32 = 343;
 
 template <int G, bool MULTI>
-__global__ void __launch_bounds__(32 * VGROUP_WARPS) vlist_group32_kernel(const VaSub one,
-                                                                          const VaSub* __restrict__ subs,
-                                                                          const int* __restrict__ prefix, int nsub,
-                                                                          const int* __restrict__ active,
-                                                                          const float2* spec_override) {
+__global__ void __launch_bounds__(256) vlist_group32_kernel(const VaSub one, const VaSub* __restrict__ subs,
+                                                            const int* __restrict__ prefix, int nsub, int ngroups,
+                                                            const int* __restrict__ active,
+                                                            const float2* spec_override) {
     constexpr int G3 = G * G * G;
-    extern __shared__ float2 tsm32[];  // [offset][lane]
-    __shared__ VaSub Sm;
-    __shared__ int lb;
+    const int g = blockIdx.x * VGROUP_WARPS + (threadIdx.x >> 5);
+    if (g >= ngroups) return;
+    int j = 0, grp = g;
     if (MULTI) {
-        if (threadIdx.x == 0) {
-            const int j = find_sub(prefix, nsub, (int)blockIdx.x);
-            Sm = subs[j];
-            lb = blockIdx.x - prefix[j];
-        }
-        __syncthreads();
+        j = find_sub(prefix, nsub, g);
+        grp = g - __ldg(prefix + j);
     }
-    const VaSub& S = MULTI ? Sm : one;
-    const int b = MULTI ? lb : blockIdx.x;
-    if (MULTI && active && !active[S.inst]) return;  // the whole block
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int chunk = blockIdx.y, f = chunk * 32 + lane;
-    const float2* __restrict__ tns = reinterpret_cast<const float2*>(S.L.tns);
-    for (int i = threadIdx.x; i < VT_OFFSETS32 * 32; i += blockDim.x)
-        tsm32[i] = __ldg(tns + (size_t)(i >> 5) * G3 + chunk * 32 + (i & 31));
-    __syncthreads();
+    const VaSub& S = MULTI ? subs[j] : one;
+    if (MULTI && active && !active[S.inst]) return;
     const float2* __restrict__ spec = spec_override ? spec_override : S.spec;
-    for (int r = 0; r < VGROUP_ROUNDS; ++r) {
-        const int grp = (b * VGROUP_ROUNDS + r) * VGROUP_WARPS + warp;
-        if (grp >= S.ngroups) break;  // warp-uniform; no block-wide sync below
-        float2 acc[8];
+    const float2* __restrict__ tns = reinterpret_cast<const float2*>(S.L.tns);
+    const int f = blockIdx.y * 32 + (threadIdx.x & 31);
+    float2 acc[8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) acc[c] = make_float2(0.f, 0.f);
-        const int e0 = __ldg(S.gptr + grp), e1 = __ldg(S.gptr + grp + 1);
-        for (int base = e0; base < e1; base += 32) {
-            const int n = min(32, e1 - base);
-            const int2 mine = lane < n ? __ldg(S.gsrc + base + lane) : make_int2(0, 0);
-            float2 sv[4];
+    for (int c = 0; c < 8; ++c) acc[c] = make_float2(0.f, 0.f);
+    const int e1 = __ldg(S.gptr + grp + 1);
+    for (int e = __ldg(S.gptr + grp); e < e1; ++e) {
+        const int2 ent = __ldg(S.gsrc + e);
+        const float2 sv = __ldg(spec + (size_t)ent.x * G3 + f);
+        const int mask = ent.y & 255;
+        const float2* tb = tns + (size_t)(ent.y >> 8) * G3 + f;
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (u < n) sv[u] = __ldg(spec + (size_t)__shfl_sync(0xffffffffu, mine.x, u) * G3 + f);
-            for (int k = 0; k < n; k += 4) {
+        for (int c = 0; c < 8; ++c)
+            if (mask & (1 << c)) cfma32(acc[c], __ldg(tb + (size_t)child_voff32(c) * G3), sv);
+    }
+    float2* tsp = S.tsp;
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int kk = k + u;
-                    if (kk < n) {
-                        const int y = __shfl_sync(0xffffffffu, mine.y, kk);
-                        const float2 sval = sv[u];
-                        if (kk + 4 < n) sv[u] = __ldg(spec + (size_t)__shfl_sync(0xffffffffu, mine.x, kk + 4) * G3 + f);
-                        const int mask = y & 255;
-                        const float2* tb = tsm32 + (y >> 8) * 32 + lane;
-#pragma unroll
-                        for (int c = 0; c < 8; ++c)
-                            if (mask & (1 << c)) cfma32(acc[c], tb[child_voff32(c) * 32], sval);
-                    }
-                }
-            }
-        }
-        float2* tsp = S.tsp;
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int t = __ldg(S.gtrg + 8 * grp + c);
-            if (t >= 0) tsp[(size_t)t * G3 + f] = acc[c];
-        }
+    for (int c = 0; c < 8; ++c) {
+        const int t = __ldg(S.gtrg + 8 * grp + c);
+        if (t >= 0) tsp[(size_t)t * G3 + f] = acc[c];
     }
 }
 
@@ -702,13 +654,6 @@ __global__ void __launch_bounds__(vt_threads(G)) vlist_inverse32_kernel(const Vi
 }
 
 void vlist32_init(int) {
-    const int gs = (int)(sizeof(float2) * VT_OFFSETS32 * 32);
-    cudaFuncSetAttribute(vlist_group32_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
-    cudaFuncSetAttribute(vlist_group32_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
-    cudaFuncSetAttribute(vlist_group32_kernel<12, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
-    cudaFuncSetAttribute(vlist_group32_kernel<12, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
-    cudaFuncSetAttribute(vlist_group32_kernel<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
-    cudaFuncSetAttribute(vlist_group32_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs);
 #define DDFMM_VT_ATTR(k, g)                                                                      \
     cudaFuncSetAttribute(k<g, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(g, 8)); \
     cudaFuncSetAttribute(k<g, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(g, 8));
@@ -746,22 +691,21 @@ void launch_vlist_forward32(const VfSub* subs, const int* prefix, int nsub, int 
 #undef DDFMM_VFWD
 }
 
-void launch_vlist_group32(const VaSub* subs, const int* prefix, int nsub, int nblocks, int G, const int* active,
+void launch_vlist_group32(const VaSub* subs, const int* prefix, int nsub, int ngroups, int G, const int* active,
                           const void* spec_override, cudaStream_t s, const VaSub* one) {
-    if (nblocks == 0) return;
+    if (ngroups == 0) return;
     VaSub o{};
     if (nsub == 1) {
         if (!one) return;  // a single sub-launch is passed by value
         o = *one;
     }
-    const dim3 grid(nblocks, G * G * G / 32);
-    const size_t sm = sizeof(float2) * VT_OFFSETS32 * 32;
+    const dim3 grid((ngroups + VGROUP_WARPS - 1) / VGROUP_WARPS, G * G * G / 32);
     const float2* so = static_cast<const float2*>(spec_override);
-#define DDFMM_VGRP(g)                                                                                                \
-    if (nsub == 1)                                                                                                   \
-        vlist_group32_kernel<g, false><<<grid, 32 * VGROUP_WARPS, sm, s>>>(o, subs, prefix, nsub, active, so);       \
-    else                                                                                                             \
-        vlist_group32_kernel<g, true><<<grid, 32 * VGROUP_WARPS, sm, s>>>(o, subs, prefix, nsub, active, so);
+#define DDFMM_VGRP(g)                                                                                             \
+    if (nsub == 1)                                                                                                \
+        vlist_group32_kernel<g, false><<<grid, 32 * VGROUP_WARPS, 0, s>>>(o, subs, prefix, nsub, ngroups, active, so); \
+    else                                                                                                          \
+        vlist_group32_kernel<g, true><<<grid, 32 * VGROUP_WARPS, 0, s>>>(o, subs, prefix, nsub, ngroups, active, so);
     switch (G) {
         case 8: DDFMM_VGRP(8) break;
         case 12: DDFMM_VGRP(12) break;

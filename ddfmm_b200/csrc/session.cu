@@ -76,16 +76,27 @@ Session::Session(const double* pos3n, int n, const SessionParams& p, const std::
     // operator files first (Mlib3d::setup): a bad file is reported before any device work
     ld_path_ = ld_path;
     hd_path_ = hd_path;
+    auto since = [](std::chrono::steady_clock::time_point a) {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count();
+    };
     ops_.load(ld_path, hd_path);
     ops_.validate(p.accu);
+    stats_.ops_seconds = since(t0);
     CK(cudaSetDevice(p.device));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     pos_.assign(pos3n, pos3n + 3 * (size_t)n);
+    auto t1 = std::chrono::steady_clock::now();
     tree_.build(pos_.data(), n, p.tree);
+    stats_.tree_seconds = since(t1);
+    t1 = std::chrono::steady_clock::now();
     build();
+    CK(cudaStreamSynchronize(stream_));
+    stats_.plan_seconds = since(t1);
+    t1 = std::chrono::steady_clock::now();
     autotune();
     CK(cudaStreamSynchronize(stream_));
-    stats_.setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    stats_.tune_seconds = since(t1);
+    stats_.setup_seconds = since(t0);
 }
 
 Session::~Session() {
@@ -1310,7 +1321,7 @@ void Session::build() {
                 if (mixed) {
                     a.hva = VaSub{VL, a.v.grp.gptr, a.v.grp.gsrc, a.v.grp.gtrg, reinterpret_cast<const float2*>(lf_spec),
                                   reinterpret_cast<float2*>(tsp), ngroups, 0};
-                    set_multi(a, a.hva, vgroup_blocks(ngroups));
+                    set_multi(a, a.hva, ngroups);
                 }
                 push_step(a);
                 Step iv{};
@@ -1453,10 +1464,18 @@ void Session::build() {
     stats_.kernel_launches = (long long)steps_.size() + 2;
 }
 
-static const char* kernel_name(int kind) {
+static const char* kernel_name(int kind, int tpi) {
     switch (kind) {
         case 0: return "zgemm_kernel";
-        case 1: return "pt_kernel";
+        case 1:
+            switch (tpi) {  // the launch shape the autotuner chose
+                case 4: return "pt_kernel<4>";
+                case 8: return "pt_kernel<8>";
+                case 16: return "pt_kernel<16>";
+                case PT_WARP_TARGETS: return "ptw_kernel<targets>";
+                case PT_WARP_SOURCES: return "ptw_kernel<sources>";
+                default: return "pt_kernel<32>";
+            }
         case 2: return "vlist_forward_kernel";
         case 3: return "vlist_group_kernel";
         case 6: return "vlist_inverse_kernel";
@@ -1578,7 +1597,7 @@ std::vector<Session::ProfileEntry> Session::profile_read() {
         const Step& st = steps_[pe.first];
         ProfileEntry& e = prof_[st.label];
         e.label = st.label;
-        e.kernel = kernel_name(st.kind);
+        e.kernel = kernel_name(st.kind, st.tpi);
         e.launches += 1;
         e.ms += ms;
         e.flops += st.flops;

@@ -35,6 +35,7 @@ struct SessionStats {
     long long fft_spectra_bytes = 0;
     double setup_seconds = 0;
     size_t device_bytes = 0;
+    double ops_seconds = 0, tree_seconds = 0, plan_seconds = 0, tune_seconds = 0;  // parts of setup_seconds
     int tuned_steps = 0;  // steps whose launch shape the autotuner chose
 };
 

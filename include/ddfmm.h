@@ -58,6 +58,9 @@ typedef struct ddfmm_stats {
     long long fft_spectra_bytes;
     double setup_seconds;
     long long device_bytes;
+    /* setup_seconds split: operator files, octree and lists, plan and
+     * operators on the device, launch-shape tuning */
+    double ops_seconds, tree_seconds, plan_seconds, tune_seconds;
 } ddfmm_stats;
 
 /* Wave3d::setup + Mlib3d::setup.  pos3n: n points, x/y/z interleaved, in
