@@ -20,6 +20,7 @@ EXPORTS = (
     "ddfmm_batch_destroy", "ddfmm_server_create", "ddfmm_server_add_session", "ddfmm_server_session_state",
     "ddfmm_server_remove_session", "ddfmm_server_submit", "ddfmm_server_wait", "ddfmm_server_poll",
     "ddfmm_server_get_stats", "ddfmm_server_destroy", "ddfmm_operators_check", "ddfmm_session_test_gemm_stall",
+    "ddfmm_precompute_operators",
 )
 PLAIN_FP64, MIXED, MIXED_MMA_SYNC = 0, 1, 2
 
@@ -112,6 +113,8 @@ def load():
     ip = C.POINTER(C.c_int)
     lib.ddfmm_operators_check.argtypes = [C.c_char_p, C.c_char_p, C.c_int, ip, ip]
     lib.ddfmm_operators_check.restype = C.c_int
+    lib.ddfmm_precompute_operators.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_int]
+    lib.ddfmm_precompute_operators.restype = C.c_int
     lib.ddfmm_session_test_gemm_stall.argtypes = [C.c_void_p, C.c_double]
     lib.ddfmm_session_test_gemm_stall.restype = C.c_int
     vpp = C.POINTER(C.c_void_p)

@@ -1,7 +1,9 @@
 // extern "C" entry points (include/ddfmm.h).
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <new>
@@ -10,6 +12,7 @@
 
 #include "../../include/ddfmm.h"
 #include "batch.hpp"
+#include "precompute.hpp"
 #include "server.hpp"
 #include "session.hpp"
 
@@ -257,6 +260,40 @@ int ddfmm_operators_check(const char* ld_path, const char* hd_path, int accu, in
             long long n = 0;
             for (const auto& kv : ops.hd) n += (long long)kv.second.size();
             *n_hd_wedges = (int)n;
+        }
+    });
+}
+
+int ddfmm_precompute_operators(int kernel, int accu, int wmax, int threads, const char* ld_path, const char* hd_path,
+                               int verbose) {
+    if (kernel != 0 && kernel != 1) return fail(DDFMM_EINVAL, "kernel must be 0 (exp(ir)/r) or 1 (exp(ir))");
+    if (accu < 1 || accu > 3) return fail(DDFMM_EINVAL, "ACCU must be 1, 2 or 3");
+    if (wmax < 1 || wmax > 1024 || (wmax & (wmax - 1))) return fail(DDFMM_EINVAL, "wmax must be a power of two >= 1");
+    if (!ld_path && !hd_path) return fail(DDFMM_EINVAL, "no output file given");
+    // arguments are checked above: every failure below is a precompute failure
+    return guarded([&] {
+        try {
+            if (ld_path) {
+                auto t0 = std::chrono::steady_clock::now();
+                ddfmm::precompute::write_ld(ld_path, ddfmm::precompute::low_levels(accu, kernel, threads));
+                if (verbose)
+                    std::fprintf(stderr, "precompute: low frequency written in %.1f s\n",
+                                 std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+            }
+            if (hd_path) {
+                auto t0 = std::chrono::steady_clock::now();
+                auto progress = [&](double W, int done, int total) {
+                    if (verbose && done == total)
+                        std::fprintf(stderr, "precompute: width %g, %d wedges, %.1f s\n", W, total,
+                                     std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+                };
+                ddfmm::precompute::write_hd(hd_path,
+                                            ddfmm::precompute::high_levels(accu, kernel, wmax, threads, progress));
+            }
+        } catch (const std::bad_alloc&) {
+            throw;
+        } catch (const std::exception& e) {
+            throw std::runtime_error(std::string("operator precompute failed: ") + e.what());
         }
     });
 }

@@ -5,12 +5,12 @@
 // session holds that scratch.  This file holds a process-wide alternative: a
 // statically sized device array, present on every GPU that loads the library
 // until the process exits.  Host code cannot use the array's name as a device
-// address, so the first use on each device resolves it with
-// cudaGetSymbolAddress while that device is current, and later calls reuse the
-// cached address.
+// address, so every call resolves it with cudaGetSymbolAddress on the current
+// device (no allocation; the first call on a device may load the module).
+// Nothing is cached, so the address stays right after a cudaDeviceReset
+// gives the device a new primary context.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -22,28 +22,14 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = 16u << 20;  // 16 MiB
 
 static __device__ __align__(256) double2 g_vlist_scratch[NOALLOC_SCRATCH_BYTES / sizeof(double2)];
 
-namespace {
-std::mutex g_mu;
-constexpr int kMaxDevices = 64;
-void* g_addr[kMaxDevices] = {};
-}  // namespace
-
 // Device address and capacity (in double2) of the scratch on the current device.
 double2* noalloc_scratch(size_t* capacity) {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices) throw std::runtime_error("CUDA error: device ordinal beyond the scratch table");
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_vlist_scratch);
-        if (e != cudaSuccess)
-            throw std::runtime_error(std::string("CUDA error: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_addr[dev] = p;
-    }
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_vlist_scratch);
+    if (e != cudaSuccess)
+        throw std::runtime_error(std::string("CUDA error: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     *capacity = NOALLOC_SCRATCH_BYTES / sizeof(double2);
-    return static_cast<double2*>(g_addr[dev]);
+    return static_cast<double2*>(p);
 }
 
 }  // namespace ddfmm

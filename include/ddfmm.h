@@ -110,10 +110,9 @@ int ddfmm_eval_device(ddfmm_session* s, const void* den_dev, void* val_dev, void
  * nothing.  Limits and rules:
  *  - sessions whose spectra exceed 16 MiB (about 2000 low-frequency boxes at
  *    ACCU 1, 600 at ACCU 2, 250 at ACCU 3) get DDFMM_EINVAL and a message;
- *  - the first call on each device resolves the array's device address
- *    (cudaGetSymbolAddress) with that device current and keeps it for the
- *    life of the process; a cudaDeviceReset invalidates it, so do not use
- *    this call after resetting a device;
+ *  - every call resolves the array's device address (cudaGetSymbolAddress,
+ *    which allocates nothing) on the current device, so the address is
+ *    right after a cudaDeviceReset too;
  *  - every call and every session on a device share the one array: calls
  *    whose work overlaps on the GPU race.  stream == NULL means the session's
  *    own private stream, so two sessions both called with NULL overlap: with
@@ -139,6 +138,20 @@ int ddfmm_session_stats(const ddfmm_session* s, ddfmm_stats* out);
  * there); DDFMM_EINVAL for bad arguments.  Optional outputs: the number of
  * low-frequency widths and of (width, canonical wedge) entries. */
 int ddfmm_operators_check(const char* ld_path, const char* hd_path, int accu, int* n_ld_widths, int* n_hd_wedges);
+
+/* Host-only (no GPU): write the translation-operator files that
+ * Mlib3d::setup reads (src/mlib3d.cpp:70-103) for kernel (0: exp(ir)/r,
+ * 1: exp(ir)), accuracy level accu and high-frequency widths 1, 2, 4, ...
+ * up to wmax -- the FP64 precompute the reference runs offline in MATLAB
+ * (matlab/aug3d_script.m, aug3d_lowdata.m, aug3d_hghdata.m).  ld_path gets
+ * the 7 low-frequency widths 2^-7..2^-1, hd_path the high-frequency wedges;
+ * either may be NULL to skip that file.  threads <= 0 uses every host core;
+ * verbose != 0 prints one progress line per width on stderr.  The output
+ * does not depend on the thread count.  DDFMM_EINVAL for bad arguments,
+ * DDFMM_ESETUP when a factorization fails (e.g. a rank above DVMAX=400) or a
+ * file cannot be written. */
+int ddfmm_precompute_operators(int kernel, int accu, int wmax, int threads, const char* ld_path, const char* hd_path,
+                               int verbose);
 
 /* Failure-path test hook, no counterpart in the reference.  On a DDFMM_MIXED
  * session: the next eval's first tensor-core GEMM launch bounds its pipeline
