@@ -2,13 +2,21 @@
 //
 // Hot loops work on the interleaved (re, im) doubles directly: std::complex
 // products follow C99 Annex G (inf/nan recovery), which keeps them out of
-// vector registers.
+// vector registers.  The factorizations and the GEMM are compiled twice, for
+// x86-64-v3 (AVX2, FMA) and for the baseline, and the loader picks the one
+// the host supports.
 #include "dense.hpp"
 
 #include <algorithm>
 #include <cmath>
 #include <numeric>
 #include <stdexcept>
+
+#if defined(__x86_64__) && defined(__GNUC__)
+#define TUNED __attribute__((target_clones("arch=x86-64-v3", "default")))
+#else
+#define TUNED
+#endif
 
 namespace ddfmm {
 namespace dense {
@@ -19,16 +27,24 @@ constexpr double kEps = 2.220446049250313e-16;
 inline double* dp(cpx* p) { return reinterpret_cast<double*>(p); }
 inline const double* dp(const cpx* p) { return reinterpret_cast<const double*>(p); }
 
-// sum_i conj(v_i) y_i over n entries
+// sum_i conj(v_i) y_i over n entries (four partial sums, so the additions
+// of consecutive entries do not wait on one another)
 inline cpx dotc(const cpx* v, const cpx* y, int n) {
     const double* a = dp(v);
     const double* b = dp(y);
-    double re = 0, im = 0;
-    for (int i = 0; i < n; ++i) {
-        re += a[2 * i] * b[2 * i] + a[2 * i + 1] * b[2 * i + 1];
-        im += a[2 * i] * b[2 * i + 1] - a[2 * i + 1] * b[2 * i];
+    double re[4] = {0, 0, 0, 0}, im[4] = {0, 0, 0, 0};
+    int i = 0;
+    for (; i + 4 <= n; i += 4)
+        for (int u = 0; u < 4; ++u) {
+            const double ar = a[2 * (i + u)], ai = a[2 * (i + u) + 1], br = b[2 * (i + u)], bi = b[2 * (i + u) + 1];
+            re[u] += ar * br + ai * bi;
+            im[u] += ar * bi - ai * br;
+        }
+    for (; i < n; ++i) {
+        re[0] += a[2 * i] * b[2 * i] + a[2 * i + 1] * b[2 * i + 1];
+        im[0] += a[2 * i] * b[2 * i + 1] - a[2 * i + 1] * b[2 * i];
     }
-    return cpx(re, im);
+    return cpx((re[0] + re[1]) + (re[2] + re[3]), (im[0] + im[1]) + (im[2] + im[3]));
 }
 
 // y += alpha x over n entries
@@ -45,9 +61,12 @@ inline void axpy(cpx alpha, const cpx* x, cpx* y, int n) {
 
 inline double nrm2sq(const cpx* x, int n) {
     const double* a = dp(x);
-    double s = 0;
-    for (int i = 0; i < 2 * n; ++i) s += a[i] * a[i];
-    return s;
+    double s[4] = {0, 0, 0, 0};
+    int i = 0;
+    for (; i + 4 <= 2 * n; i += 4)
+        for (int u = 0; u < 4; ++u) s[u] += a[i + u] * a[i + u];
+    for (; i < 2 * n; ++i) s[0] += a[i] * a[i];
+    return (s[0] + s[1]) + (s[2] + s[3]);
 }
 
 // Elementary reflector H = I - tau v v^H with H^H (alpha; x) = (beta; 0), beta
@@ -79,7 +98,7 @@ inline void apply_reflector(const cpx* vt, cpx ctau, cpx* y, int len) {
 }
 
 // C(m x n) += A(m x k) B(k x n), all column-major with leading dimensions
-void gemm_nn(const cpx* A, int lda, const cpx* B, int ldb, cpx* C, int ldc, int m, int n, int k) {
+TUNED void gemm_nn(const cpx* A, int lda, const cpx* B, int ldb, cpx* C, int ldc, int m, int n, int k) {
     constexpr int MB = 192;
     int j0 = 0;
     for (; j0 + 4 <= n; j0 += 4) {
@@ -153,7 +172,7 @@ CMat gemm(const CMat& A, bool ah, const CMat& B, bool bh) {
     return C;
 }
 
-void qr(const CMat& A0, CMat& Q, CMat& R) {
+TUNED void qr(const CMat& A0, CMat& Q, CMat& R) {
     const int m = A0.m, n = A0.n;
     if (m < n) throw std::invalid_argument("qr: needs m >= n");
     CMat A = A0;
@@ -178,7 +197,14 @@ void qr(const CMat& A0, CMat& Q, CMat& R) {
     }
 }
 
-std::vector<int> qr_pivoted(CMat A, double reltol, std::vector<double>* rdiag) {
+// Blocked form (the BLAS-3 pivoted QR of Quintana-Orti, Sun and Bischof, as in
+// LAPACK's zlaqps): within a block of up to NB steps the trailing columns are
+// not updated; each step updates only its pivot column and pivot row from
+// F = tau A^H v (one read-only pass over the trailing matrix), and the block
+// ends with one update A -= V F^H.  A block also ends early after a step whose
+// norm downdate lost accuracy; those norms are recomputed after the update.
+TUNED std::vector<int> qr_pivoted(CMat A, double reltol, std::vector<double>* rdiag) {
+    constexpr int NB = 32;
     const int m = A.m, n = A.n, kmax = std::min(m, n);
     std::vector<int> perm(n), piv;
     std::iota(perm.begin(), perm.end(), 0);
@@ -187,44 +213,96 @@ std::vector<int> qr_pivoted(CMat A, double reltol, std::vector<double>* rdiag) {
     const double tol3z = std::sqrt(kEps);
     double r00 = 0;
     if (rdiag) rdiag->clear();
-    for (int k = 0; k < kmax; ++k) {
-        const int p = k + (int)(std::max_element(vn1.begin() + k, vn1.end()) - (vn1.begin() + k));
-        if (p != k) {
-            std::swap_ranges(&A(0, p), &A(0, p) + m, &A(0, k));
-            std::swap(perm[p], perm[k]);
-            vn1[p] = vn1[k];
-            vn2[p] = vn2[k];
-        }
-        cpx* col = &A(k, k);
-        const cpx tau = reflector(col, m - k);
-        const double rkk = std::abs(col[0]);
-        if (k == 0) {
-            r00 = rkk;
-            if (r00 == 0) break;
-        }
-        if (rkk <= reltol * r00) break;
-        piv.push_back(perm[k]);
-        if (rdiag) rdiag->push_back(rkk);
-        const cpx ct = std::conj(tau);
-        for (int j = k + 1; j < n; ++j) {
-            if (ct != cpx(0, 0)) apply_reflector(col + 1, ct, &A(k, j), m - k);
-            if (vn1[j] != 0) {
-                double t = std::abs(A(k, j)) / vn1[j];
-                t = std::max(0.0, 1.0 - t * t);
-                const double r = vn1[j] / vn2[j];
+    CMat F = zeros(n, NB);  // row c: column c of the matrix; column i: step i of the block
+    std::vector<cpx> aux(NB);
+    std::vector<int> recompute;
+    int k = 0;
+    while (k < kmax) {
+        const int nb = std::min(NB, kmax - k);
+        for (int i = 0; i < nb; ++i) std::fill(&F(0, i), &F(0, i) + n, cpx(0, 0));
+        recompute.clear();
+        int jb = 0;
+        for (int j = 0; j < nb; ++j) {
+            const int kk = k + j;
+            const int p = kk + (int)(std::max_element(vn1.begin() + kk, vn1.end()) - (vn1.begin() + kk));
+            if (p != kk) {
+                std::swap_ranges(&A(0, p), &A(0, p) + m, &A(0, kk));
+                std::swap(perm[p], perm[kk]);
+                vn1[p] = vn1[kk];
+                vn2[p] = vn2[kk];
+                for (int i = 0; i < j; ++i) std::swap(F(p, i), F(kk, i));
+            }
+            // pivot column: apply this block's earlier reflectors, A(kk:, kk) -= V(kk:, 0:j) F(kk, 0:j)^H
+            for (int i = 0; i < j; ++i) {
+                const cpx f = std::conj(F(kk, i));
+                if (f != cpx(0, 0)) axpy(-f, &A(kk, k + i), &A(kk, kk), m - kk);
+            }
+            cpx* col = &A(kk, kk);
+            const cpx tau = reflector(col, m - kk);
+            const double rkk = std::abs(col[0]);
+            if (kk == 0) {
+                r00 = rkk;
+                if (r00 == 0) return piv;
+            }
+            if (rkk <= reltol * r00) return piv;
+            piv.push_back(perm[kk]);
+            if (rdiag) rdiag->push_back(rkk);
+            jb = j + 1;
+            if (kk + 1 >= kmax) break;
+            // F(c, j) = tau (A(kk:, c)^H v) for the trailing columns, v = (1; col[1..])
+            const cpx beta = col[0];
+            col[0] = 1.0;
+            for (int c = kk + 1; c < n; ++c) F(c, j) = tau * std::conj(dotc(col, &A(kk, c), m - kk));
+            // F(:, j) -= tau F(:, 0:j) (V(kk:, 0:j)^H v)
+            if (j > 0) {
+                for (int i = 0; i < j; ++i) aux[i] = -tau * dotc(&A(kk, k + i), col, m - kk);
+                for (int i = 0; i < j; ++i)
+                    if (aux[i] != cpx(0, 0))
+                        for (int c = kk + 1; c < n; ++c) F(c, j) += F(c, i) * aux[i];
+            }
+            // pivot row: A(kk, c) -= sum_{i <= j} V(kk, i) conj(F(c, i)), V(kk, j) = 1
+            for (int c = kk + 1; c < n; ++c) {
+                cpx s(0, 0);
+                for (int i = 0; i <= j; ++i) s += A(kk, k + i) * std::conj(F(c, i));
+                A(kk, c) -= s;
+            }
+            col[0] = beta;
+            // norm downdate from the updated pivot row
+            bool lost = false;
+            for (int c = kk + 1; c < n; ++c) {
+                if (vn1[c] == 0) continue;
+                double t = std::abs(A(kk, c)) / vn1[c];
+                t = std::max(0.0, (1.0 + t) * (1.0 - t));
+                const double r = vn1[c] / vn2[c];
                 if (t * r * r <= tol3z) {
-                    vn1[j] = k + 1 < m ? std::sqrt(nrm2sq(&A(k + 1, j), m - k - 1)) : 0.0;
-                    vn2[j] = vn1[j];
+                    recompute.push_back(c);
+                    vn1[c] = 0;  // not a pivot candidate until recomputed
+                    lost = true;
                 } else {
-                    vn1[j] *= std::sqrt(t);
+                    vn1[c] *= std::sqrt(t);
                 }
             }
+            if (lost) break;
         }
+        const int kend = k + jb;
+        if (kend >= kmax) break;
+        // trailing update A(kend:, kend:) -= V(kend:, 0:jb) F(kend:, 0:jb)^H
+        if (m > kend && n > kend) {
+            CMat Fh = zeros(jb, n - kend);
+            for (int c = kend; c < n; ++c)
+                for (int i = 0; i < jb; ++i) Fh(i, c - kend) = -std::conj(F(c, i));
+            gemm_nn(&A(kend, k), m, Fh.a.data(), jb, &A(kend, kend), m, m - kend, n - kend, jb);
+        }
+        for (int c : recompute) {
+            vn1[c] = kend < m ? std::sqrt(nrm2sq(&A(kend, c), m - kend)) : 0.0;
+            vn2[c] = vn1[c];
+        }
+        k = kend;
     }
     return piv;
 }
 
-void svd(const CMat& A, CMat& U, std::vector<double>& s, CMat& V) {
+TUNED void svd(const CMat& A, CMat& U, std::vector<double>& s, CMat& V) {
     const int m = A.m, n = A.n;
     if (m < n) throw std::invalid_argument("svd: needs m >= n");
     CMat Q, X;
