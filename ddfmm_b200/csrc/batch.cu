@@ -141,6 +141,10 @@ Batch::Batch(const std::vector<Session*>& sessions) : sessions_(sessions) {
                             n.push_back(u.ngroups);
                         }
                         add(VACC, subs, n, gg.first);
+                        // one instance: the shape its session was tuned to; several: the L1
+                        // shape (the shared-memory one holds one instance's tensors)
+                        if (!launches_.empty() && launches_.back().kind == VACC)
+                            launches_.back().tpi = gg.second.size() == 1 ? gg.second[0].second->tpi : VGROUP_L1;
                     } else {
                         std::vector<ViSub> subs;
                         std::vector<int> n;
@@ -183,8 +187,10 @@ Batch::Batch(const std::vector<Session*>& sessions) : sessions_(sessions) {
 }
 
 Batch::~Batch() {
-    if (exec_) cudaGraphExecDestroy(exec_);
-    if (graph_) cudaGraphDestroy(graph_);
+    for (Graph& g : graphs_) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
     for (void* p : allocs_) cudaFree(p);
 }
 
@@ -218,7 +224,8 @@ void Batch::run(const int* active, cudaStream_t s) {
                 break;
             case VACC:
                 launch_vlist_group32(static_cast<const VaSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub,
-                                     (int)L.total, L.G, active, nullptr, s, L.nsub == 1 ? reinterpret_cast<const VaSub*>(L.one) : nullptr);
+                                     (int)L.total, L.G, active, nullptr, s, L.nsub == 1 ? reinterpret_cast<const VaSub*>(L.one) : nullptr,
+                                     L.tpi);
                 break;
             case VINV:
                 launch_vlist_inverse32(static_cast<const ViSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub,
@@ -230,25 +237,34 @@ void Batch::run(const int* active, cudaStream_t s) {
 }
 
 void Batch::run_graph(const int* active, cudaStream_t s) {
-    if (!exec_ || active != graph_active_) {
-        if (exec_) cudaGraphExecDestroy(exec_);
-        if (graph_) cudaGraphDestroy(graph_);
-        exec_ = nullptr;
-        graph_ = nullptr;
-        BCK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        try {
-            run(active, s);
-        } catch (...) {
-            cudaGraph_t g = nullptr;
-            cudaStreamEndCapture(s, &g);
-            if (g) cudaGraphDestroy(g);
-            throw;
+    for (const Graph& g : graphs_)
+        if (g.active == active) {
+            BCK(cudaGraphLaunch(g.exec, s));
+            return;
         }
-        BCK(cudaStreamEndCapture(s, &graph_));
-        BCK(cudaGraphInstantiate(&exec_, graph_, 0));
-        graph_active_ = active;
+    if (graphs_.size() >= 4) {  // keep a few: the caller's mask arrays
+        cudaGraphExecDestroy(graphs_.front().exec);
+        cudaGraphDestroy(graphs_.front().graph);
+        graphs_.erase(graphs_.begin());
     }
-    BCK(cudaGraphLaunch(exec_, s));
+    Graph g{active, nullptr, nullptr};
+    BCK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+        run(active, s);
+    } catch (...) {
+        cudaGraph_t part = nullptr;
+        cudaStreamEndCapture(s, &part);
+        if (part) cudaGraphDestroy(part);
+        throw;
+    }
+    BCK(cudaStreamEndCapture(s, &g.graph));
+    const cudaError_t e = cudaGraphInstantiate(&g.exec, g.graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g.graph);
+        BCK(e);
+    }
+    graphs_.push_back(g);
+    BCK(cudaGraphLaunch(g.exec, s));
 }
 
 void Batch::check_error(cudaStream_t s) {

@@ -32,8 +32,10 @@ public:
     // One matvec of every instance i with active[i] != 0 (device array of
     // size() ints; nullptr = all), enqueued on s.
     void run(const int* active, cudaStream_t s);
-    // The same through a CUDA graph, captured on first use and again when
-    // `active` or `s`'s device changes.
+    // The same through a CUDA graph, captured on first use for each `active`
+    // array (a few are kept: one per mask array of the caller).  Graphs of
+    // different mask arrays may run at once on different streams when their
+    // active instances are disjoint.
     void run_graph(const int* active, cudaStream_t s);
     int launches() const { return (int)launches_.size(); }
     // Throws if a tensor-core GEMM block gave up waiting (the flag is reset);
@@ -49,7 +51,7 @@ private:
         int nsub;
         long long total;
         int G;
-        int tpi = 32;  // point interactions: threads per item
+        int tpi = 32;  // launch shape: threads per item (point interactions), VGROUP_* (V-list sums)
         alignas(16) unsigned char one[256];  // host copy of the first sub-launch
     };
     template <class Sub, class Pre>
@@ -61,9 +63,12 @@ private:
     std::vector<void*> allocs_;
     int device_ = 0;
     int* d_err_ = nullptr;
-    cudaGraph_t graph_ = nullptr;
-    cudaGraphExec_t exec_ = nullptr;
-    const int* graph_active_ = nullptr;
+    struct Graph {
+        const int* active;
+        cudaGraph_t graph;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Graph> graphs_;  // captured sequences by mask array
 };
 
 }  // namespace ddfmm

@@ -14,13 +14,18 @@
 #include "session.hpp"
 
 #include <algorithm>
+#include <array>
 #include <cctype>
-#include <cstdio>
 #include <chrono>
+#include <climits>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
-#include <stdexcept>
+#include <exception>
 #include <set>
+#include <stdexcept>
+#include <thread>
 #include <unordered_map>
 #include <unordered_set>
 
@@ -61,11 +66,43 @@ void Session::dfree(const void* p) {
 
 template <class T>
 T* Session::upload(const std::vector<T>& v) {
-    T* d = dalloc<T>(v.size());
-    if (!v.empty()) CK(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream_));
-    // the host vector may die right after: make the copy complete
-    CK(cudaStreamSynchronize(stream_));
-    return d;
+    const size_t bytes = v.size() * sizeof(T);
+    if (bytes > kArenaMax) {
+        T* d = dalloc<T>(v.size());
+        CK(cudaMemcpyAsync(d, v.data(), bytes, cudaMemcpyHostToDevice, stream_));
+        // the caller's vector may die right after: make the copy complete
+        CK(cudaStreamSynchronize(stream_));
+        return d;
+    }
+    const size_t need = (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;  // 256-byte aligned slots
+    if (arena_.used + need > arena_.cap) {
+        flush_uploads();
+        // the copy out of the old host image may still be running: keep the
+        // image until the end of the plan (released after a stream sync)
+        if (!arena_.host.empty()) arena_.retired.push_back(std::move(arena_.host));
+        // chunks of 1 MiB doubling to 64 MiB: small sessions stay small
+        arena_.cap = std::max(need, std::min((size_t)64 << 20, std::max((size_t)1 << 20, 2 * arena_.cap)));
+        // not through dalloc: a chunk must never be released by dfree(), which
+        // would take an array that happens to start the chunk for its base
+        void* chunk = nullptr;
+        CK(cudaMalloc(&chunk, arena_.cap));
+        allocs_.push_back(chunk);
+        stats_.device_bytes += arena_.cap;
+        arena_.dev = static_cast<char*>(chunk);
+        arena_.host.assign(arena_.cap, 0);
+        arena_.used = arena_.sent = 0;
+    }
+    char* d = arena_.dev + arena_.used;
+    if (bytes) std::memcpy(arena_.host.data() + arena_.used, v.data(), bytes);
+    arena_.used += need;
+    return reinterpret_cast<T*>(d);
+}
+
+void Session::flush_uploads() {
+    if (arena_.used > arena_.sent)
+        CK(cudaMemcpyAsync(arena_.dev + arena_.sent, arena_.host.data() + arena_.sent, arena_.used - arena_.sent,
+                           cudaMemcpyHostToDevice, stream_));
+    arena_.sent = arena_.used;
 }
 
 Session::Session(const double* pos3n, int n, const SessionParams& p, const std::string& ld_path,
@@ -244,6 +281,7 @@ void Session::push_step(Step st) {
 }
 
 void Session::flush_packs() {
+    flush_uploads();
     if (pack_jobs_.empty()) return;
     UmmaPackJob* d = nullptr;
     CK(cudaMalloc(&d, sizeof(UmmaPackJob) * pack_jobs_.size()));
@@ -311,6 +349,33 @@ void Session::add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>&
 }
 
 namespace {
+// f(i) for i in [0, n) on the host's cores (DDFMM_HOST_THREADS when set, as for
+// the tree's lists); the first exception is rethrown after every thread joined.
+template <class F>
+void host_parallel_for(size_t n, F f) {
+    const char* e = std::getenv("DDFMM_HOST_THREADS");
+    const int v = e ? std::atoi(e) : 0;
+    const size_t hw = v > 0 ? (size_t)v : std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>(std::min<size_t>(hw, 64), n);
+    if (nt <= 1) {
+        for (size_t i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::vector<std::exception_ptr> err(nt);
+    std::vector<std::thread> th;
+    for (size_t t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            try {
+                for (size_t i = t; i < n; i += nt) f(i);
+            } catch (...) {
+                err[t] = std::current_exception();
+            }
+        });
+    for (auto& x : th) x.join();
+    for (auto& x : err)
+        if (x) std::rethrow_exception(x);
+}
+
 // Setup-time matrix products C = A * B for many small operators in one
 // launch: each product is one grouped-GEMM problem whose "columns" are the
 // columns of B (read from pool X) and of C (written to pool Y).
@@ -353,12 +418,6 @@ struct GemmBatch {
     }
 };
 
-struct NodeKey {
-    uint64_t operator()(int box, const Idx3& d) const {
-        return ((uint64_t)box << 33) | ((uint64_t)(d[0] + 1024) << 22) | ((uint64_t)(d[1] + 1024) << 11) |
-               (uint64_t)(d[2] + 1024);
-    }
-};
 // (width, wedge) as one hash key: widths are powers of two, wedge components |d| < 1024
 uint64_t wedge_key(double W, const Idx3& d) {
     const uint64_t wl = (uint64_t)(std::lround(std::log2(W)) + 32);
@@ -392,6 +451,18 @@ std::vector<double2> to_d2_transpose(const CMat& m) {  // Transpose, src/mlib3d.
 }  // namespace
 
 void Session::build() {
+    // DDFMM_SETUP_TRACE=1: time each part of the plan (with the stream drained
+    // at each mark, so device work is charged to the part that enqueued it)
+    // and print the times to stderr
+    const bool trace = std::getenv("DDFMM_SETUP_TRACE") != nullptr;
+    auto tmark = std::chrono::steady_clock::now();
+    auto phase = [&](const char* what) {
+        if (!trace) return;
+        CK(cudaStreamSynchronize(stream_));
+        const auto t = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "ddfmm setup %-16s %8.3f s\n", what, std::chrono::duration<double>(t - tmark).count());
+        tmark = t;
+    };
     const double eps = 1e-12;
     const int P = accu_to_p(prm_.accu), G = 2 * P, G3 = G * G * G;
     const int nE = P * P * P - (P - 2) * (P - 2) * (P - 2);
@@ -411,6 +482,7 @@ void Session::build() {
         auto it = op32.find(a);
         if (it != op32.end()) return it->second;
         float2* b = dalloc<float2>(n);
+        flush_uploads();
         launch_to_c64(a, b, (long long)n, stream_);
         CK(cudaGetLastError());
         return op32[a] = (const double2*)b;
@@ -454,6 +526,7 @@ void Session::build() {
     d_val_io_ = dalloc<double2>(npts_);
     zero_at_start_.push_back(Memset{d_val_sorted_, es * npts_});
 
+    phase("points");
     std::map<int, std::vector<int> > lflevels;  // level -> lf ids (key order)
     for (int l = 0; l < nLF; ++l) lflevels[T.boxes[lfbox[l]].level].push_back(l);
 
@@ -586,6 +659,7 @@ void Session::build() {
         lfops[level] = L;
     }
 
+    phase("lf_operators");
     // ---------------------------------------------------------------- HF nodes
     struct Node {
         int box;
@@ -593,6 +667,7 @@ void Session::build() {
         int canon;           // index into hfcanon
         long long off;       // upeq (up) / dnchk (down) offset
         long long toff;      // temp offset within the level
+        int did;             // dense id of (width, wedge)
     };
     struct Canon {
         double W;
@@ -640,6 +715,7 @@ void Session::build() {
     struct DirPts {
         double *ucp, *dep, *uep, *dcp;  // S*ucp, -S*ucp, S*uep, -S*uep
         int r1, r2, canon;
+        int did;  // dense id, in order of first use
     };
     std::map<std::pair<double, Idx3>, DirPts> dirpts;
     std::unordered_map<uint64_t, const DirPts*> dirfast;  // hash index into dirpts (node addresses are stable)
@@ -654,6 +730,7 @@ void Session::build() {
         int c = get_canon(W, dir, sgn, pv);
         const HighFreqOp& op = *hfcanon[c].op;
         DirPts d{};
+        d.did = (int)dirpts.size();
         d.canon = c;
         d.r1 = hfcanon[c].r1;
         d.r2 = hfcanon[c].r2;
@@ -670,8 +747,10 @@ void Session::build() {
     for (int b : T.order)
         if (T.boxes[b].has_pts() && T.width(T.boxes[b].level) > 1 - eps) hflevels[T.boxes[b].level].push_back(b);
 
+    // nodes of a box are contiguous and in its (sorted) wedge order, so a
+    // (box, wedge) node is found by binary search in the box's range
     std::vector<Node> up, dn;
-    std::unordered_map<uint64_t, int> upmap, dnmap;
+    std::vector<int> up_first(nb, 0), up_cnt(nb, 0), dn_first(nb, 0), dn_cnt(nb, 0);
     {
         size_t nu = 0, nd = 0;
         for (auto& kv : hflevels)
@@ -679,12 +758,20 @@ void Session::build() {
                 nu += T.boxes[b].outdirs.size();
                 nd += T.boxes[b].incdirs.size();
             }
-        upmap.reserve(nu);
-        dnmap.reserve(nd);
         up.reserve(nu);
         dn.reserve(nd);
     }
-    NodeKey nk;
+    auto find_node = [](const std::vector<Node>& v, int first, int cnt, const Idx3& d) -> int {
+        int lo = first, hi = first + cnt;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (v[mid].dir < d)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        return (lo < first + cnt && v[lo].dir == d) ? lo : -1;
+    };
     std::map<int, std::pair<int, int> > uprange, dnrange;  // level -> [begin, end)
     std::map<int, long long> tmp_up_level;                 // level -> temporary elements of its M2M sums
     long long upeq_total = 0, dnchk_total = 0, tmp_max = 0;
@@ -693,20 +780,22 @@ void Session::build() {
         long long tmp_up = 0, tmp_dn = 0;
         int u0 = (int)up.size(), d0 = (int)dn.size();
         for (int b : kv.second) {
+            up_first[b] = (int)up.size();
+            up_cnt[b] = (int)T.boxes[b].outdirs.size();
             for (const Idx3& d : T.boxes[b].outdirs) {
                 const DirPts& dp = get_dir(W, d);
-                Node nd{b, d, dp.canon, upeq_total, tmp_up};
+                Node nd{b, d, dp.canon, upeq_total, tmp_up, dp.did};
                 upeq_total += dp.r1;
                 tmp_up += std::max(dp.r1, dp.r2);
-                upmap[nk(b, d)] = (int)up.size();
                 up.push_back(nd);
             }
+            dn_first[b] = (int)dn.size();
+            dn_cnt[b] = (int)T.boxes[b].incdirs.size();
             for (const Idx3& d : T.boxes[b].incdirs) {
                 const DirPts& dp = get_dir(W, d);
-                Node nd{b, d, dp.canon, dnchk_total, tmp_dn};
+                Node nd{b, d, dp.canon, dnchk_total, tmp_dn, dp.did};
                 dnchk_total += dp.r1;
                 tmp_dn += std::max(dp.r1, dp.r2);
-                dnmap[nk(b, d)] = (int)dn.size();
                 dn.push_back(nd);
             }
         }
@@ -715,6 +804,7 @@ void Session::build() {
         dnrange[kv.first] = std::make_pair(d0, (int)dn.size());
         tmp_max = std::max(tmp_max, std::max(tmp_up, tmp_dn));
     }
+    phase("hf_nodes");
     stats_.hf_up_nodes = (long long)up.size();
     stats_.hf_down_nodes = (long long)dn.size();
     double2* hf_upeq = salloc((size_t)upeq_total);
@@ -814,6 +904,7 @@ void Session::build() {
             l2l_mats[key] = M;
         }
     }
+    phase("m2m_l2l_plan");
     // M2L: canonical offset o_c = S^-1 (c_t - c_s), so M(dir, o) = M(canon, o_c)
     std::unordered_map<uint64_t, int> m2l_id;  // (canon, ox, oy, oz) packed -> matrix
     struct M2LMat {
@@ -826,46 +917,97 @@ void Session::build() {
     std::vector<M2LMat> m2l_mats;
     std::map<int, std::vector<std::vector<long long> > > m2l_x, m2l_y;  // level -> per problem columns
     std::map<int, std::vector<int> > m2l_probs;                         // level -> matrix ids
-    for (auto& kv : hflevels) {
-        int level = kv.first;
-        double W = T.width(level);
-        auto dr = dnrange[level];
-        std::vector<int> local;  // matrix id -> local problem index (-1: none yet)
-        auto& X = m2l_x[level];
-        auto& Y = m2l_y[level];
-        auto& Pids = m2l_probs[level];
-        for (int i = dr.first; i < dr.second; ++i) {
-            const Node& t = dn[i];
-            const Box& tb = T.boxes[t.box];
-            auto fit = tb.far.find(t.dir);
-            if (fit == tb.far.end()) continue;
-            Idx3 sgn, pv, srt;
-            index3_sort(t.dir, srt, sgn, pv);
-            for (int sb_i : fit->second) {
-                auto uit = upmap.find(nk(sb_i, t.dir));
-                if (uit == upmap.end()) throw std::runtime_error("M2L source has no outgoing equivalent density");
-                const Box& sb = T.boxes[sb_i];
-                int o[3], oc[3];
-                for (int d = 0; d < 3; ++d) o[d] = tb.idx[d] - sb.idx[d];
-                for (int d = 0; d < 3; ++d) oc[d] = sgn[pv[d]] * o[pv[d]];
-                const uint64_t key = ((uint64_t)t.canon << 33) | ((uint64_t)(oc[0] + 1024) << 22) |
-                                     ((uint64_t)(oc[1] + 1024) << 11) | (uint64_t)(oc[2] + 1024);
-                auto mit = m2l_id.find(key);
+    {
+        // The far pairs of chunks of target nodes (a chunk never spans two levels)
+        // are listed on all host cores, then merged in chunk order, so matrix ids,
+        // problem order and column order are those of one pass in node order.
+        struct Chunk {
+            int level, i0, i1;
+            std::vector<uint64_t> keys;  // (canon, canonical offset), first-seen order
+            std::vector<int> kcanon;
+            std::vector<std::array<int, 3> > koc;
+            std::vector<std::vector<long long> > X, Y;  // per key
+            long long pairs = 0;
+        };
+        std::vector<Chunk> chunks;
+        for (auto& kv : hflevels) {
+            const auto dr = dnrange[kv.first];
+            for (int i0 = dr.first; i0 < dr.second; i0 += 2048) {
+                Chunk c;
+                c.level = kv.first;
+                c.i0 = i0;
+                c.i1 = std::min(dr.second, i0 + 2048);
+                chunks.push_back(std::move(c));
+            }
+        }
+        host_parallel_for(chunks.size(), [&](size_t ci) {
+            Chunk& C = chunks[ci];
+            std::unordered_map<uint64_t, int> loc;
+            for (int i = C.i0; i < C.i1; ++i) {
+                const Node& t = dn[i];
+                const Box& tb = T.boxes[t.box];
+                auto fit = tb.far.find(t.dir);
+                if (fit == tb.far.end()) continue;
+                Idx3 sgn, pv, srt;
+                index3_sort(t.dir, srt, sgn, pv);
+                for (int sb_i : fit->second) {
+                    const int uit = find_node(up, up_first[sb_i], up_cnt[sb_i], t.dir);
+                    if (uit < 0) throw std::runtime_error("M2L source has no outgoing equivalent density");
+                    const Box& sb = T.boxes[sb_i];
+                    int o[3];
+                    std::array<int, 3> oc;
+                    for (int d = 0; d < 3; ++d) o[d] = tb.idx[d] - sb.idx[d];
+                    for (int d = 0; d < 3; ++d) oc[d] = sgn[pv[d]] * o[pv[d]];
+                    const uint64_t key = ((uint64_t)t.canon << 33) | ((uint64_t)(oc[0] + 1024) << 22) |
+                                         ((uint64_t)(oc[1] + 1024) << 11) | (uint64_t)(oc[2] + 1024);
+                    auto it = loc.find(key);
+                    int li;
+                    if (it == loc.end()) {
+                        li = (int)C.keys.size();
+                        loc.emplace(key, li);
+                        C.keys.push_back(key);
+                        C.kcanon.push_back(t.canon);
+                        C.koc.push_back(oc);
+                        C.X.emplace_back();
+                        C.Y.emplace_back();
+                    } else {
+                        li = it->second;
+                    }
+                    C.X[li].push_back(up[uit].off);
+                    C.Y[li].push_back(t.off);
+                    C.pairs++;
+                }
+            }
+        });
+        std::vector<int> local;  // matrix id -> problem index within its level (-1: none yet)
+        int cur_level = INT_MIN;
+        for (Chunk& C : chunks) {
+            if (C.level != cur_level) {
+                cur_level = C.level;
+                local.assign(m2l_mats.size(), -1);
+            }
+            const double W = T.width(C.level);
+            auto& X = m2l_x[C.level];
+            auto& Y = m2l_y[C.level];
+            auto& Pids = m2l_probs[C.level];
+            for (size_t k = 0; k < C.keys.size(); ++k) {
+                auto mit = m2l_id.find(C.keys[k]);
                 int gid;
                 if (mit == m2l_id.end()) {
-                    const Canon& c = hfcanon[t.canon];
+                    const Canon& c = hfcanon[C.kcanon[k]];
+                    const std::array<int, 3>& oc = C.koc[k];
                     gid = (int)m2l_mats.size();
                     size_t n = (size_t)c.r1 * c.r1;
-                    const std::string k = opk("m2l", W, c.srt, oc[0], oc[1], oc[2]);
-                    const float* pk = cached_op(k);
-                    M2LMat M{0, 0, 0, t.canon, c.r1, Pt3{{oc[0] * W, oc[1] * W, oc[2] * W}}, pk, k};
+                    const std::string key = opk("m2l", W, c.srt, oc[0], oc[1], oc[2]);
+                    const float* pk = cached_op(key);
+                    M2LMat M{0, 0, 0, C.kcanon[k], c.r1, Pt3{{oc[0] * W, oc[1] * W, oc[2] * W}}, pk, key};
                     if (!pk) {
                         M.raw = take(scr, n);
                         M.tmp = take(scr, n);
                         M.fin = take(keep, n);
                     }
                     m2l_mats.push_back(M);
-                    m2l_id[key] = gid;
+                    m2l_id[C.keys[k]] = gid;
                 } else {
                     gid = mit->second;
                 }
@@ -878,12 +1020,15 @@ void Session::build() {
                     X.emplace_back();
                     Y.emplace_back();
                 }
-                X[li].push_back(up[uit->second].off);
-                Y[li].push_back(t.off);
-                stats_.hf_far_pairs++;
+                X[li].insert(X[li].end(), C.X[k].begin(), C.X[k].end());
+                Y[li].insert(Y[li].end(), C.Y[k].begin(), C.Y[k].end());
             }
+            stats_.hf_far_pairs += C.pairs;
+            std::vector<std::vector<long long> >().swap(C.X);
+            std::vector<std::vector<long long> >().swap(C.Y);
         }
     }
+    phase("m2l_plan");
     stats_.m2l_matrices = (long long)m2l_mats.size();
     // right factors E1 and E3^T as gatherable columns in the scratch pool
     std::vector<size_t> scr_E1(hfcanon.size()), scr_E3t(hfcanon.size());
@@ -894,6 +1039,7 @@ void Session::build() {
     double2* dkeep = dalloc<double2>(keep);
     double2* dscr = nullptr;
     if (scr) CK(cudaMalloc(&dscr, sizeof(double2) * scr));
+    flush_uploads();
     for (size_t c = 0; c < hfcanon.size(); ++c) {
         CK(cudaMemcpyAsync(dscr + scr_E1[c], hfcanon[c].E1, sizeof(double2) * hfcanon[c].r1 * hfcanon[c].r1,
                            cudaMemcpyDeviceToDevice, stream_));
@@ -921,14 +1067,17 @@ void Session::build() {
     for (const M2LMat& M : m2l_mats)
         if (!M.pk) add_job(hfcanon[M.canon].neg_uep, M.shift, hfcanon[M.canon].uep, zero3, M.r1, M.r1, dscr + M.raw);
 
+    phase("job_list");
     // generate every kernel matrix now
     if (!jobs.empty()) {
         KmatJob* d_jobs = upload(jobs);
+        flush_uploads();
         launch_kmat(d_jobs, (int)jobs.size(), job_elems, kern, stream_);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(stream_));
     }
 
+    phase("kmat");
     // fold: right products (raw * E1 or raw * E3^T), then left products (E3 * . or E1^T * .)
     if (scr) {
         GemmBatch right_s, right_k, left;
@@ -965,6 +1114,7 @@ void Session::build() {
         CK(cudaStreamSynchronize(stream_));
         CK(cudaFree(dscr));
     }
+    phase("fold");
     const double2* dkeepm = opm(dkeep, keep);
     auto KP = [&](size_t off) { return E((double2*)dkeepm, off); };
 
@@ -1030,6 +1180,22 @@ void Session::build() {
                "lf_uc2ue");
     }
 
+    phase("steps_lf_up");
+    // children with points of every high-frequency box (-1: none), and dense
+    // (wedge, child) -> problem tables for the per-level step building
+    std::vector<int> kids((size_t)nb * 8, -1);
+    for (auto& kv : hflevels)
+        for (int b : kv.second)
+            for (int ind = 0; ind < 8; ++ind) {
+                const int c = T.child(b, ind);
+                if (c >= 0 && T.boxes[c].has_pts()) kids[(size_t)b * 8 + ind] = c;
+            }
+    std::vector<int> ptab(dirpts.size() * 8, -1), ctab(hfcanon.size(), -1);
+    std::vector<size_t> touched;
+    auto reset_tab = [&](std::vector<int>& tab) {
+        for (size_t t : touched) tab[t] = -1;
+        touched.clear();
+    };
     // ---------------------------------------------------------------- steps: HF upward
     // widths ascending = levels descending; hf_upeq holds w (upeqnden = E1 w)
     for (auto hit = hflevels.rbegin(); hit != hflevels.rend(); ++hit) {
@@ -1047,29 +1213,28 @@ void Session::build() {
         // one launch for the 8 child positions: a problem per (wedge, child), all adding into
         // the parents' sums
         {
-            std::unordered_map<uint64_t, int> pid;  // (wedge, child) -> problem
             std::vector<GemmProblem> probs;
             std::vector<std::vector<long long> > xo, yo;
             for (int ind = 0; ind < 8; ++ind)
             for (int i = ur.first; i < ur.second; ++i) {
                 const Node& u = up[i];
-                int c = T.child(u.box, ind);
-                if (c < 0 || !T.boxes[c].has_pts()) continue;
+                const int c = kids[(size_t)u.box * 8 + ind];
+                if (c < 0) continue;
                 long long xoff;
                 if (W == 1.0) {
                     xoff = (long long)lfidx[c] * nE;
                 } else {
-                    auto cit = upmap.find(nk(c, predir(u.dir)));
-                    if (cit == upmap.end()) throw std::runtime_error("child has no directional equivalent density");
-                    xoff = up[cit->second].off;
+                    const int cit = find_node(up, up_first[c], up_cnt[c], predir(u.dir));
+                    if (cit < 0) throw std::runtime_error("child has no directional equivalent density");
+                    xoff = up[cit].off;
                 }
-                const uint64_t pk = (wedge_key(W, u.dir) << 3) | (uint64_t)ind;
-                auto pit = pid.find(pk);
-                int p;
-                if (pit == pid.end()) {
+                const size_t pk = (size_t)u.did * 8 + ind;  // (wedge, child) -> problem
+                int p = ptab[pk];
+                if (p < 0) {
                     const DirMats& M = m2m_mats.at(std::make_pair(W, u.dir));
                     p = (int)probs.size();
-                    pid[pk] = p;
+                    ptab[pk] = p;
+                    touched.push_back(pk);
                     if (M.cached) {
                         probs.push_back(GemmProblem{nullptr, M.mrows, M.mcols, M.mrows, 0, 0, M.pk[ind]});
                     } else {
@@ -1078,26 +1243,24 @@ void Session::build() {
                     }
                     xo.emplace_back();
                     yo.emplace_back();
-                } else {
-                    p = pit->second;
                 }
                 xo[p].push_back(xoff);
                 yo[p].push_back(u.toff);
             }
+            reset_tab(ptab);
             add_gemm(probs, xo, yo, W == 1.0 ? lf_upeq : hf_upeq, T0, GEMM_ATOMIC, width_label("hf_m2m", W));
         }
         // w = E2 * (E3 upchkval)   (src/wave3d_eval.cpp:837-849)
-        std::map<int, int> cp;
         std::vector<GemmProblem> p2;
         std::vector<std::vector<long long> > xa, ya;
         for (int i = ur.first; i < ur.second; ++i) {
             const Node& u = up[i];
-            auto it2 = cp.find(u.canon);
-            int p;
-            if (it2 == cp.end()) {
+            int p = ctab[u.canon];
+            if (p < 0) {
                 const Canon& c = hfcanon[u.canon];
                 p = (int)p2.size();
-                cp[u.canon] = p;
+                ctab[u.canon] = p;
+                touched.push_back(u.canon);
                 const std::string k = opk("e2", c.W, c.srt, 0);
                 if (const float* pk = cached_op(k)) {
                     p2.push_back(GemmProblem{nullptr, c.r1, c.r2, c.r1, 0, 0, pk});
@@ -1108,15 +1271,15 @@ void Session::build() {
                 }
                 xa.emplace_back();
                 ya.emplace_back();
-            } else {
-                p = it2->second;
             }
             xa[p].push_back(u.toff);
             ya[p].push_back(u.off);
         }
+        reset_tab(ctab);
         add_gemm(p2, xa, ya, T0, hf_upeq, GEMM_SET, width_label("hf_uc2ue", W));
     }
 
+    phase("steps_hf_up");
     // ---------------------------------------------------------------- steps: HF downward
     // widths descending = levels ascending; hf_dnchk holds u = E1^T dnchkval
     for (auto it = hflevels.begin(); it != hflevels.end(); ++it) {
@@ -1140,17 +1303,16 @@ void Session::build() {
             add_gemm(probs, m2l_x[level], m2l_y[level], hf_upeq, hf_dnchk, GEMM_ATOMIC, width_label("hf_m2l", W));
         }
         // t = E2^T u   (dneqnden = E3^T t, src/wave3d_eval.cpp:938-948, src/mlib3d.cpp:246-250)
-        std::map<int, int> cp;
         std::vector<GemmProblem> p2;
         std::vector<std::vector<long long> > xa, xt;
         for (int i = dr.first; i < dr.second; ++i) {
             const Node& d = dn[i];
-            auto it2 = cp.find(d.canon);
-            int p;
-            if (it2 == cp.end()) {
+            int p = ctab[d.canon];
+            if (p < 0) {
                 const Canon& c = hfcanon[d.canon];
                 p = (int)p2.size();
-                cp[d.canon] = p;
+                ctab[d.canon] = p;
+                touched.push_back(d.canon);
                 const std::string k = opk("e2t", c.W, c.srt, 0);
                 if (const float* pk = cached_op(k)) {
                     p2.push_back(GemmProblem{nullptr, c.r2, c.r1, c.r2, 0, 0, pk});
@@ -1161,39 +1323,37 @@ void Session::build() {
                 }
                 xa.emplace_back();
                 xt.emplace_back();
-            } else {
-                p = it2->second;
             }
             xa[p].push_back(d.off);
             xt[p].push_back(d.toff);
         }
+        reset_tab(ctab);
         add_gemm(p2, xa, xt, hf_dnchk, T1, GEMM_SET, width_label("hf_dc2de", W));
         // L2L into the children's (pdir) u, or LF dnchkval at W=1 (src/wave3d_eval.cpp:950-991),
         // one launch for the 8 child positions: a problem per (wedge, child)
         {
-            std::unordered_map<uint64_t, int> pid;  // (wedge, child) -> problem
             std::vector<GemmProblem> probs;
             std::vector<std::vector<long long> > xo, yo;
             for (int ind = 0; ind < 8; ++ind)
             for (int i = dr.first; i < dr.second; ++i) {
                 const Node& d = dn[i];
-                int c = T.child(d.box, ind);
-                if (c < 0 || !T.boxes[c].has_pts()) continue;
+                const int c = kids[(size_t)d.box * 8 + ind];
+                if (c < 0) continue;
                 long long yoff;
                 if (W == 1.0) {
                     yoff = (long long)lfidx[c] * nE;
                 } else {
-                    auto cit = dnmap.find(nk(c, predir(d.dir)));
-                    if (cit == dnmap.end()) throw std::runtime_error("child has no directional check value");
-                    yoff = dn[cit->second].off;
+                    const int cit = find_node(dn, dn_first[c], dn_cnt[c], predir(d.dir));
+                    if (cit < 0) throw std::runtime_error("child has no directional check value");
+                    yoff = dn[cit].off;
                 }
-                const uint64_t pk = (wedge_key(W, d.dir) << 3) | (uint64_t)ind;
-                auto pit = pid.find(pk);
-                int p;
-                if (pit == pid.end()) {
+                const size_t pk = (size_t)d.did * 8 + ind;  // (wedge, child) -> problem
+                int p = ptab[pk];
+                if (p < 0) {
                     const DirMats& M = l2l_mats.at(std::make_pair(W, d.dir));
                     p = (int)probs.size();
-                    pid[pk] = p;
+                    ptab[pk] = p;
+                    touched.push_back(pk);
                     if (M.cached) {
                         probs.push_back(GemmProblem{nullptr, M.mrows, M.mcols, M.mrows, 0, 0, M.pk[ind]});
                     } else {
@@ -1202,16 +1362,16 @@ void Session::build() {
                     }
                     xo.emplace_back();
                     yo.emplace_back();
-                } else {
-                    p = pit->second;
                 }
                 xo[p].push_back(d.toff);
                 yo[p].push_back(yoff);
             }
+            reset_tab(ptab);
             add_gemm(probs, xo, yo, T1, W == 1.0 ? lf_dnchk : hf_dnchk, GEMM_ATOMIC, width_label("hf_l2l", W));
         }
     }
 
+    phase("steps_hf_down");
     // ---------------------------------------------------------------- steps: LF downward
     for (auto& kv : lflevels) {  // levels ascending = widths descending
         int level = kv.first;
@@ -1300,11 +1460,15 @@ void Session::build() {
                     set_multi(f, f.hvf, f.v.nsrc);
                 }
                 push_step(f);
-                // summed target spectra: the high-frequency temporary T0 when it is large
-                // enough (every high-frequency pass has run before this low-frequency
-                // downward step, so T0 is free), else a buffer of their own
+                // summed target spectra: a high-frequency buffer when one is large enough
+                // (every high-frequency pass has run before this low-frequency downward
+                // step, so the outgoing densities, the incoming check values and both
+                // temporaries are all free by then), else a buffer of their own
                 const size_t tsp_elems = trg.size() * (size_t)G3;
-                double2* tsp = tsp_elems <= (size_t)tmp_max ? T0 : salloc(tsp_elems);
+                double2* tsp = tsp_elems <= (size_t)upeq_total    ? hf_upeq
+                               : tsp_elems <= (size_t)dnchk_total ? hf_dnchk
+                               : tsp_elems <= (size_t)tmp_max     ? T0
+                                                                  : salloc(tsp_elems);
                 const int ngroups = (int)gptr.size() - 1;
                 long long npairs = 0;
                 for (const int2& e2 : gsrc) npairs += __builtin_popcount(e2.y & 255);
@@ -1449,6 +1613,7 @@ void Session::build() {
                        "lf_l2l");
             }
     }
+    phase("steps_lf_down");
     flush_packs();
     if (mixed) {
         // the mixed eval reads only the FP32 copies (and, on tcgen05, only the packed
@@ -1461,6 +1626,12 @@ void Session::build() {
             if (umma() && !vlist32.count(kv.second)) dfree(kv.second);
         }
     }
+    flush_uploads();
+    CK(cudaStreamSynchronize(stream_));
+    std::vector<char>().swap(arena_.host);  // every chunk is on the device now
+    arena_.retired.clear();
+    arena_.used = arena_.sent = arena_.cap;
+    phase("packs_release");
     stats_.kernel_launches = (long long)steps_.size() + 2;
 }
 
@@ -1477,7 +1648,7 @@ static const char* kernel_name(int kind, int tpi) {
                 default: return "pt_kernel<32>";
             }
         case 2: return "vlist_forward_kernel";
-        case 3: return "vlist_group_kernel";
+        case 3: return tpi == VGROUP_L1 ? "vlist_group_kernel<l1>" : "vlist_group_kernel<smem>";
         case 6: return "vlist_inverse_kernel";
         case 5: return "umma_cgemm_kernel";
         default: return "memset";
@@ -1509,9 +1680,9 @@ void Session::launch_step(const Step& st, cudaStream_t s, double2* spec) {
         case 3:
             if (m)
                 launch_vlist_group32(static_cast<const VaSub*>(st.msubs), st.mpre, 1, st.mtotal, st.v.L.G, nullptr,
-                                     spec != st.v.spec ? spec : nullptr, s, &st.hva);
+                                     spec != st.v.spec ? spec : nullptr, s, &st.hva, st.tpi);
             else
-                launch_vlist_group(st.v.L, st.v.grp, spec, st.v.tsp, s);
+                launch_vlist_group(st.v.L, st.v.grp, spec, st.v.tsp, s, st.tpi);
             break;
         case 6:
             if (m)
@@ -1540,10 +1711,13 @@ void Session::autotune() {
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
     for (Step& st : steps_) {
-        if (st.kind != 1) continue;
+        if (st.kind != 1 && st.kind != 3) continue;
+        static const std::vector<int> pt_shapes{32, 16, 8, 4, PT_WARP_TARGETS, PT_WARP_SOURCES};
+        static const std::vector<int> vg_shapes{VGROUP_SMEM, VGROUP_L1};
+        const std::vector<int>& shapes = st.kind == 1 ? pt_shapes : vg_shapes;
         float best = 0.f;
-        int best_tpi = 32;
-        for (int tpi : {32, 16, 8, 4, PT_WARP_TARGETS, PT_WARP_SOURCES}) {
+        int best_tpi = shapes[0];
+        for (int tpi : shapes) {
             st.tpi = tpi;
             launch_step(st, stream_, st.v.spec);  // warm-up
             CK(cudaEventRecord(a, stream_));
@@ -1552,7 +1726,7 @@ void Session::autotune() {
             CK(cudaEventSynchronize(b));
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, a, b));
-            if (tpi == 32 || ms < best) {
+            if (tpi == shapes[0] || ms < best) {
                 best = ms;
                 best_tpi = tpi;
             }

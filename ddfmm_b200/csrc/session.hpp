@@ -136,7 +136,9 @@ private:
         // that play the same part (phase, width, step type, occurrence): a Batch
         // merges the steps of its sessions that share a key into one launch.
         long long key;
-        int tpi;  // point interactions: launch shape (launch_pt; 0 = 32 threads per item), set by autotune()
+        // launch shape, set by autotune(): point interactions: threads per item
+        // (launch_pt; 0 = 32); V-list sums: VGROUP_L1 or VGROUP_SMEM
+        int tpi;
         // mixed form: the step as a one-instance launch (device sub-launch array and
         // prefix sums) and the host copy of its sub-launch
         void* msubs;
@@ -152,9 +154,18 @@ private:
 
     template <class T>
     T* dalloc(size_t count);
+    // Copies a host array to the device and returns its device address.
+    // Arrays above kArenaMax bytes get their own allocation and a completed
+    // copy (the caller's vector may die right after).  Arrays up to kArenaMax
+    // bytes -- most of the plan's many small tables -- are copied into the
+    // host image of a device chunk (1 MiB doubling to 64 MiB); flush_uploads()
+    // sends what is new in the image with one copy, and must run before any
+    // device work reads those arrays.  Images stay alive until the plan's
+    // last stream sync, as an asynchronous copy may still be reading them.
     template <class T>
     T* upload(const std::vector<T>& v);
-    void dfree(const void* p);  // release one allocation made by dalloc / upload
+    void flush_uploads();
+    void dfree(const void* p);  // release one allocation made by dalloc / a large upload
     void add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<long long> >& xo,
                   std::vector<std::vector<long long> >& yo, const double2* X, double2* Y, int mode,
                   const char* label);
@@ -182,6 +193,13 @@ private:
     OperatorLib ops_;
     std::vector<void*> allocs_;
     std::map<const void*, size_t> alloc_bytes_;
+    static constexpr size_t kArenaMax = 64 << 10;
+    struct UploadArena {
+        char* dev = nullptr;     // current device chunk
+        std::vector<char> host;  // its host image
+        std::vector<std::vector<char> > retired;  // images of earlier chunks, kept until the plan's last sync
+        size_t cap = 0, used = 0, sent = 0;
+    } arena_;
     std::vector<Step> steps_;
     cudaStream_t stream_ = nullptr;
     SessionStats stats_;
