@@ -141,10 +141,6 @@ Batch::Batch(const std::vector<Session*>& sessions) : sessions_(sessions) {
                             n.push_back(u.ngroups);
                         }
                         add(VACC, subs, n, gg.first);
-                        // one instance: the shape its session was tuned to; several: the L1
-                        // shape (the shared-memory one holds one instance's tensors)
-                        if (!launches_.empty() && launches_.back().kind == VACC)
-                            launches_.back().tpi = gg.second.size() == 1 ? gg.second[0].second->tpi : VGROUP_L1;
                     } else {
                         std::vector<ViSub> subs;
                         std::vector<int> n;
@@ -224,8 +220,7 @@ void Batch::run(const int* active, cudaStream_t s) {
                 break;
             case VACC:
                 launch_vlist_group32(static_cast<const VaSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub,
-                                     (int)L.total, L.G, active, nullptr, s, L.nsub == 1 ? reinterpret_cast<const VaSub*>(L.one) : nullptr,
-                                     L.tpi);
+                                     (int)L.total, L.G, active, nullptr, s, L.nsub == 1 ? reinterpret_cast<const VaSub*>(L.one) : nullptr);
                 break;
             case VINV:
                 launch_vlist_inverse32(static_cast<const ViSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub,

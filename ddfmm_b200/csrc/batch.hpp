@@ -51,7 +51,7 @@ private:
         int nsub;
         long long total;
         int G;
-        int tpi = 32;  // launch shape: threads per item (point interactions), VGROUP_* (V-list sums)
+        int tpi = 32;  // point interactions: threads per item
         alignas(16) unsigned char one[256];  // host copy of the first sub-launch
     };
     template <class Sub, class Pre>

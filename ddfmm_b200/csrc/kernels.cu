@@ -533,67 +533,6 @@ __global__ void __launch_bounds__(256) vlist_group_kernel(const int* __restrict_
     }
 }
 
-// The same sums with the level's translation tensors in shared memory: a
-// block owns one 32-frequency chunk (blockIdx.y), copies that chunk of all 343
-// offset tensors (176 KB) into shared memory once, then its 16 warps walk
-// groups blockIdx.x * 16 + warp, + gridDim.x * 16, ...  Per (source, child)
-// pair the tensor value comes from shared memory; only the source spectrum
-// value is a global load, one per source entry, four entries in flight per
-// warp.
-constexpr int VGS_WARPS = 16, VG_TENSORS64 = 343;
-template <int G>
-__global__ void __launch_bounds__(32 * VGS_WARPS, 1) vlist_groups_kernel(const int* __restrict__ gptr,
-                                                                         const int2* __restrict__ gsrc,
-                                                                         const int* __restrict__ gtrg, int ngroups,
-                                                                         const double2* __restrict__ spec,
-                                                                         const double2* __restrict__ tns,
-                                                                         double2* __restrict__ tsp) {
-    constexpr int G3 = G * G * G;
-    extern __shared__ double2 vts64[];  // [offset][lane]
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int f0 = blockIdx.y * 32, f = f0 + lane;
-    for (int e = threadIdx.x; e < VG_TENSORS64 * 32; e += blockDim.x)
-        vts64[e] = __ldg(tns + (size_t)(e >> 5) * G3 + f0 + (e & 31));
-    __syncthreads();
-    for (int grp = blockIdx.x * VGS_WARPS + warp; grp < ngroups; grp += gridDim.x * VGS_WARPS) {
-        double2 acc[8];
-#pragma unroll
-        for (int c = 0; c < 8; ++c) acc[c] = make_double2(0.0, 0.0);
-        const int e0 = __ldg(gptr + grp), e1 = __ldg(gptr + grp + 1);
-        int e = e0;
-        for (; e + 4 <= e1; e += 4) {
-            int2 ent[4];
-            double2 sv[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) ent[u] = __ldg(gsrc + e + u);
-#pragma unroll
-            for (int u = 0; u < 4; ++u) sv[u] = __ldg(spec + (size_t)ent[u].x * G3 + f);
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int mask = ent[u].y & 255;
-                const double2* tb = vts64 + (ent[u].y >> 8) * 32 + lane;
-#pragma unroll
-                for (int c = 0; c < 8; ++c)
-                    if (mask & (1 << c)) cfma(acc[c], tb[child_voff(c) * 32], sv[u]);
-            }
-        }
-        for (; e < e1; ++e) {
-            const int2 ent = __ldg(gsrc + e);
-            const double2 sv = __ldg(spec + (size_t)ent.x * G3 + f);
-            const int mask = ent.y & 255;
-            const double2* tb = vts64 + (ent.y >> 8) * 32 + lane;
-#pragma unroll
-            for (int c = 0; c < 8; ++c)
-                if (mask & (1 << c)) cfma(acc[c], tb[child_voff(c) * 32], sv);
-        }
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int t = __ldg(gtrg + 8 * grp + c);
-            if (t >= 0) tsp[(size_t)t * G3 + f] = acc[c];
-        }
-    }
-}
-
 // Pruned inverse DFT of one target's summed spectrum per block: P outputs
 // of G-term sums along z (each thread one (ka, kb) line, its G inputs read
 // straight from the summed spectrum), then y, then x; the corner-cube nodes
@@ -677,10 +616,6 @@ void vlist_init(int) {
     cudaFuncSetAttribute(vlist_inverse_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(8, 16));
     cudaFuncSetAttribute(vlist_inverse_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(12, 16));
     cudaFuncSetAttribute(vlist_inverse_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vt_smem(16, 16));
-    const int vg = VG_TENSORS64 * 32 * (int)sizeof(double2);
-    cudaFuncSetAttribute(vlist_groups_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, vg);
-    cudaFuncSetAttribute(vlist_groups_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, vg);
-    cudaFuncSetAttribute(vlist_groups_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, vg);
 }
 
 void launch_vlist_forward(const VlistLevel& L, const int* boxes, int nbox, const double2* upeq, double2* spec,
@@ -696,27 +631,13 @@ void launch_vlist_forward(const VlistLevel& L, const int* boxes, int nbox, const
 }
 
 void launch_vlist_group(const VlistLevel& L, const VlistGroups& V, const double2* spec, double2* tsp,
-                        cudaStream_t s, int shape) {
+                        cudaStream_t s) {
     if (V.ngroups == 0) return;
-    if (shape == VGROUP_L1) {
-        const dim3 grid((V.ngroups + VGROUP_WARPS - 1) / VGROUP_WARPS, L.G * L.G * L.G / 32);
-        switch (L.G) {
-            case 8: vlist_group_kernel<8><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
-            case 12: vlist_group_kernel<12><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
-            case 16: vlist_group_kernel<16><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
-            default: break;
-        }
-        return;
-    }
-    // tensors in shared memory (one block per SM): about four waves of blocks
-    const int chunks = L.G * L.G * L.G / 32;
-    const int gx = std::max(1, std::min((V.ngroups + VGS_WARPS - 1) / VGS_WARPS, (4 * 148 + chunks - 1) / chunks));
-    const dim3 grid(gx, chunks);
-    const size_t sm = (size_t)VG_TENSORS64 * 32 * sizeof(double2);
+    const dim3 grid((V.ngroups + VGROUP_WARPS - 1) / VGROUP_WARPS, L.G * L.G * L.G / 32);
     switch (L.G) {
-        case 8: vlist_groups_kernel<8><<<grid, 32 * VGS_WARPS, sm, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
-        case 12: vlist_groups_kernel<12><<<grid, 32 * VGS_WARPS, sm, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
-        case 16: vlist_groups_kernel<16><<<grid, 32 * VGS_WARPS, sm, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
+        case 8: vlist_group_kernel<8><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
+        case 12: vlist_group_kernel<12><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
+        case 16: vlist_group_kernel<16><<<grid, 32 * VGROUP_WARPS, 0, s>>>(V.gptr, V.gsrc, V.gtrg, V.ngroups, spec, L.tns, tsp); break;
         default: break;
     }
 }

@@ -104,13 +104,8 @@ struct VlistGroups {
     const int* gtrg;   // ngroups x 8: row of tsp of each child position, -1 where none
     int ngroups;
 };
-// Launch shapes of the sums, chosen per step by the session's autotuner:
-// VGROUP_L1 reads the translation tensors through L1 / L2 (one pass per
-// group block); VGROUP_SMEM keeps a 32-frequency chunk of all tensors in
-// shared memory and loops its warps over the groups (single instance only).
-constexpr int VGROUP_L1 = 0, VGROUP_SMEM = 1;
 void launch_vlist_group(const VlistLevel& L, const VlistGroups& V, const double2* spec, double2* tsp,
-                        cudaStream_t s, int shape = VGROUP_SMEM);
+                        cudaStream_t s);
 // dnchk[trg[t]] += pruned inverse DFT of tsp[t] / G^3 at the corner-cube nodes
 void launch_vlist_inverse(const VlistLevel& L, const int* trg, int ntrg, const double2* tsp, double2* dnchk,
                           cudaStream_t s);
@@ -185,7 +180,7 @@ void launch_vlist_forward32(const VfSub* subs, const int* prefix, int nsub, int 
                             void* spec_override, cudaStream_t s, const VfSub* one);
 // work items: groups (launch_vlist_group32) or targets (launch_vlist_inverse32)
 void launch_vlist_group32(const VaSub* subs, const int* prefix, int nsub, int ngroups, int G, const int* active,
-                          const void* spec_override, cudaStream_t s, const VaSub* one, int shape = VGROUP_SMEM);
+                          const void* spec_override, cudaStream_t s, const VaSub* one);
 void launch_vlist_inverse32(const ViSub* subs, const int* prefix, int nsub, int ntrg, int G, const int* active,
                             cudaStream_t s, const ViSub* one);
 void launch_move32(const MoveSub* subs, const int* prefix, int nsub, int n, const int* active, int scatter,

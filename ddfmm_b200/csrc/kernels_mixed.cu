@@ -570,67 +570,6 @@ __global__ void __launch_bounds__(256) vlist_group32_kernel(const VaSub one, con
     }
 }
 
-// Single-instance form of vlist_group32_kernel with the level's translation
-// tensors in shared memory: a block owns one 32-frequency chunk (blockIdx.y),
-// copies that chunk of all 343 offset tensors (88 KB) into shared memory once,
-// then its warps walk groups blockIdx.x * 8 + warp, + gridDim.x * 8, ...  Per
-// (source, child) pair the tensor value comes from shared memory instead of a
-// global load that misses L1 (a level's tensors are ~9.5 MB); only the source
-// spectrum value stays a global load, one per source entry, four entries in
-// flight per warp.
-constexpr int VG_TENSORS = 343;
-template <int G>
-__global__ void __launch_bounds__(256, 2) vlist_group32s_kernel(const VaSub S, const int* __restrict__ active,
-                                                               const float2* spec_override) {
-    constexpr int G3 = G * G * G;
-    extern __shared__ float2 vts[];  // [offset][lane]
-    if (active && !active[S.inst]) return;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int f0 = blockIdx.y * 32, f = f0 + lane;
-    const float2* __restrict__ tns = reinterpret_cast<const float2*>(S.L.tns);
-    for (int e = threadIdx.x; e < VG_TENSORS * 32; e += blockDim.x)
-        vts[e] = __ldg(tns + (size_t)(e >> 5) * G3 + f0 + (e & 31));
-    __syncthreads();
-    const float2* __restrict__ spec = spec_override ? spec_override : S.spec;
-    for (int grp = blockIdx.x * VGROUP_WARPS + warp; grp < S.ngroups; grp += gridDim.x * VGROUP_WARPS) {
-        float2 acc[8];
-#pragma unroll
-        for (int c = 0; c < 8; ++c) acc[c] = make_float2(0.f, 0.f);
-        const int e0 = __ldg(S.gptr + grp), e1 = __ldg(S.gptr + grp + 1);
-        int e = e0;
-        for (; e + 4 <= e1; e += 4) {
-            int2 ent[4];
-            float2 sv[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) ent[u] = __ldg(S.gsrc + e + u);
-#pragma unroll
-            for (int u = 0; u < 4; ++u) sv[u] = __ldg(spec + (size_t)ent[u].x * G3 + f);
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int mask = ent[u].y & 255;
-                const float2* tb = vts + (ent[u].y >> 8) * 32 + lane;
-#pragma unroll
-                for (int c = 0; c < 8; ++c)
-                    if (mask & (1 << c)) cfma32(acc[c], tb[child_voff32(c) * 32], sv[u]);
-            }
-        }
-        for (; e < e1; ++e) {
-            const int2 ent = __ldg(S.gsrc + e);
-            const float2 sv = __ldg(spec + (size_t)ent.x * G3 + f);
-            const int mask = ent.y & 255;
-            const float2* tb = vts + (ent.y >> 8) * 32 + lane;
-#pragma unroll
-            for (int c = 0; c < 8; ++c)
-                if (mask & (1 << c)) cfma32(acc[c], tb[child_voff32(c) * 32], sv);
-        }
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int t = __ldg(S.gtrg + 8 * grp + c);
-            if (t >= 0) S.tsp[(size_t)t * G3 + f] = acc[c];
-        }
-    }
-}
-
 // The inverse transform of kernels.cu (vlist_inverse_kernel) in complex FP32,
 // one block per target.
 template <int G>
@@ -729,10 +668,6 @@ void vlist32_init(int) {
     DDFMM_VT_ATTR(vlist_inverse32_kernel, 12)
     DDFMM_VT_ATTR(vlist_inverse32_kernel, 16)
 #undef DDFMM_VT_ATTR
-    const int vg_smem = VG_TENSORS * 32 * (int)sizeof(float2);
-    cudaFuncSetAttribute(vlist_group32s_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, vg_smem);
-    cudaFuncSetAttribute(vlist_group32s_kernel<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, vg_smem);
-    cudaFuncSetAttribute(vlist_group32s_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, vg_smem);
 }
 
 // L.tns, L.twf, L.twb hold float2 data in this form.
@@ -761,7 +696,7 @@ void launch_vlist_forward32(const VfSub* subs, const int* prefix, int nsub, int 
 }
 
 void launch_vlist_group32(const VaSub* subs, const int* prefix, int nsub, int ngroups, int G, const int* active,
-                          const void* spec_override, cudaStream_t s, const VaSub* one, int shape) {
+                          const void* spec_override, cudaStream_t s, const VaSub* one) {
     if (ngroups == 0) return;
     VaSub o{};
     if (nsub == 1) {
@@ -769,20 +704,6 @@ void launch_vlist_group32(const VaSub* subs, const int* prefix, int nsub, int ng
         o = *one;
     }
     const float2* so = static_cast<const float2*>(spec_override);
-    if (nsub == 1 && shape == VGROUP_SMEM) {
-        // tensors in shared memory: about four resident waves of blocks (two per SM)
-        const int chunks = G * G * G / 32;
-        const int gx = std::max(1, std::min((ngroups + VGROUP_WARPS - 1) / VGROUP_WARPS, (4 * 2 * 148 + chunks - 1) / chunks));
-        const dim3 sgrid(gx, chunks);
-        const size_t sm = (size_t)VG_TENSORS * 32 * sizeof(float2);
-        switch (G) {
-            case 8: vlist_group32s_kernel<8><<<sgrid, 32 * VGROUP_WARPS, sm, s>>>(o, active, so); break;
-            case 12: vlist_group32s_kernel<12><<<sgrid, 32 * VGROUP_WARPS, sm, s>>>(o, active, so); break;
-            case 16: vlist_group32s_kernel<16><<<sgrid, 32 * VGROUP_WARPS, sm, s>>>(o, active, so); break;
-            default: break;
-        }
-        return;
-    }
     const dim3 grid((ngroups + VGROUP_WARPS - 1) / VGROUP_WARPS, G * G * G / 32);
 #define DDFMM_VGRP(g)                                                                                             \
     if (nsub == 1)                                                                                                \

@@ -3,8 +3,12 @@
 
 #include <cstring>
 #include <fstream>
+#include <iterator>
+#include <mutex>
 #include <sstream>
 #include <stdexcept>
+
+#include <sys/stat.h>
 
 namespace ddfmm {
 
@@ -122,6 +126,33 @@ void OperatorLib::load(const std::string& ld_path, const std::string& hd_path) {
         }
     }
     if (b.o != b.buf.size()) throw std::runtime_error("hd file has trailing bytes");
+}
+
+std::shared_ptr<const OperatorLib> OperatorLib::shared(const std::string& ld_path, const std::string& hd_path) {
+    auto stamp = [](const std::string& path) {
+        struct stat st;
+        if (stat(path.c_str(), &st) != 0) throw std::runtime_error("cannot open operator file " + path);
+        return std::to_string((long long)st.st_size) + ":" + std::to_string((long long)st.st_mtim.tv_sec) + "." +
+               std::to_string((long long)st.st_mtim.tv_nsec);
+    };
+    const std::string key = ld_path + "|" + stamp(ld_path) + "|" + hd_path + "|" + stamp(hd_path);
+    static std::mutex mu;
+    static std::map<std::string, std::weak_ptr<const OperatorLib> > cache;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end())
+            if (auto p = it->second.lock()) return p;
+    }
+    auto lib = std::make_shared<OperatorLib>();
+    lib->load(ld_path, hd_path);  // outside the lock: seconds for large files
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto it = cache.begin(); it != cache.end();)
+        it = it->second.expired() ? cache.erase(it) : std::next(it);
+    auto& slot = cache[key];
+    if (auto p = slot.lock()) return p;  // another thread loaded the same files meanwhile
+    slot = lib;
+    return lib;
 }
 
 void OperatorLib::validate(int accu) const {

@@ -10,6 +10,7 @@
 #pragma once
 #include <complex>
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -48,6 +49,10 @@ struct OperatorLib {
     std::map<double, LowFreqOp> ld;
     std::map<double, std::map<Idx3, HighFreqOp> > hd;
     void load(const std::string& ld_path, const std::string& hd_path);
+    // The files as loaded once per process: sessions of the same files share one
+    // read-only copy while any of them holds it (keyed by path, size and
+    // modification time of both files, so a rewritten file is read again).
+    static std::shared_ptr<const OperatorLib> shared(const std::string& ld_path, const std::string& hd_path);
     // Shapes every entry must have for accuracy level `accu` (P = 4/6/8): LF
     // surfaces of P^3 - (P-2)^3 points, uc2ue factors v (n x r), 1/sigma (r x 1),
     // U^H (r x n), ue2dc tensors of edge 2P (or empty); HF factors E1 (r1 x r1),

@@ -116,8 +116,8 @@ Session::Session(const double* pos3n, int n, const SessionParams& p, const std::
     auto since = [](std::chrono::steady_clock::time_point a) {
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count();
     };
-    ops_.load(ld_path, hd_path);
-    ops_.validate(p.accu);
+    ops_ = OperatorLib::shared(ld_path, hd_path);
+    ops_->validate(p.accu);
     stats_.ops_seconds = since(t0);
     CK(cudaSetDevice(p.device));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
@@ -595,7 +595,7 @@ void Session::build() {
     for (auto& kv : lflevels) {
         int level = kv.first;
         double W = T.width(level);
-        const LowFreqOp& op = ops_.low(W);
+        const LowFreqOp& op = ops_->low(W);
         if (op.uep.n != nE || op.ucp.n != nE)
             throw std::runtime_error("low-frequency operator size does not match ACCU");
         LfLevelOps L{};
@@ -647,7 +647,7 @@ void Session::build() {
         for (int l : kv.second)
             if (!T.boxes[lfbox[l]].terminal()) L.has_children = true;
         if (L.has_children) {
-            const LowFreqOp& ch = ops_.low(W / 2);  // UpwardLowFetch / DownwardLowFetch
+            const LowFreqOp& ch = ops_->low(W / 2);  // UpwardLowFetch / DownwardLowFetch
             const double* chuep = upload(ch.uep.x);
             for (int ind = 0; ind < 8; ++ind) {
                 L.ue2uc[ind] = dalloc<double2>((size_t)nE * nE);
@@ -688,7 +688,7 @@ void Session::build() {
         Canon c{};
         c.W = W;
         c.srt = srt;
-        c.op = &ops_.high(W, srt);
+        c.op = &ops_->high(W, srt);
         c.r1 = c.op->uep.n;
         c.r2 = c.op->ucp.n;
         if (c.op->E1.m != c.r1 || c.op->E1.n != c.r1 || c.op->E2.m != c.r1 || c.op->E2.n != c.r2 ||
@@ -846,7 +846,7 @@ void Session::build() {
     std::map<std::pair<double, Idx3>, DirMats> m2m_mats, l2l_mats;
     const double* lf_half_uep = nullptr;
     if (!hflevels.empty()) {
-        const LowFreqOp& lf_half = ops_.low(0.5);
+        const LowFreqOp& lf_half = ops_->low(0.5);
         if (lf_half.uep.n != nE) throw std::runtime_error("width-1/2 operators do not match ACCU");
         lf_half_uep = upload(lf_half.uep.x);
     }
@@ -1181,8 +1181,7 @@ void Session::build() {
     }
 
     phase("steps_lf_up");
-    // children with points of every high-frequency box (-1: none), and dense
-    // (wedge, child) -> problem tables for the per-level step building
+    // children with points of every high-frequency box (-1: none)
     std::vector<int> kids((size_t)nb * 8, -1);
     for (auto& kv : hflevels)
         for (int b : kv.second)
@@ -1190,12 +1189,84 @@ void Session::build() {
                 const int c = T.child(b, ind);
                 if (c >= 0 && T.boxes[c].has_pts()) kids[(size_t)b * 8 + ind] = c;
             }
-    std::vector<int> ptab(dirpts.size() * 8, -1), ctab(hfcanon.size(), -1);
-    std::vector<size_t> touched;
-    auto reset_tab = [&](std::vector<int>& tab) {
-        for (size_t t : touched) tab[t] = -1;
-        touched.clear();
+    // The column lists of every high-frequency level's M2M, E2, E2^T and L2L
+    // launches, built on all host cores (one job per level and pass): each
+    // holds its problems in first-seen order -- keyed by (wedge, child) or by
+    // canonical wedge -- and their input / output columns in node order, as
+    // one sequential pass over the nodes would list them.
+    struct ColLists {
+        std::vector<int> key;
+        std::vector<std::vector<long long> > x, y;
+        void add(std::vector<int>& tab, int k, long long xv, long long yv) {
+            int p = tab[k];
+            if (p < 0) {
+                p = tab[k] = (int)key.size();
+                key.push_back(k);
+                x.emplace_back();
+                y.emplace_back();
+            }
+            x[p].push_back(xv);
+            y[p].push_back(yv);
+        }
     };
+    std::vector<std::pair<double, Idx3> > did_wedge(dirpts.size());
+    for (auto& kv : dirpts) did_wedge[kv.second.did] = kv.first;
+    std::map<int, ColLists> cl_m2m, cl_e2, cl_e2t, cl_l2l;
+    {
+        std::vector<std::pair<int, int> > jobs;  // (level, pass)
+        for (auto& kv : hflevels)
+            for (int pass = 0; pass < 4; ++pass) {
+                jobs.push_back(std::make_pair(kv.first, pass));
+                (pass == 0 ? cl_m2m : pass == 1 ? cl_e2 : pass == 2 ? cl_e2t : cl_l2l)[kv.first];
+            }
+        host_parallel_for(jobs.size(), [&](size_t j) {
+            const int level = jobs[j].first, pass = jobs[j].second;
+            const double W = T.width(level);
+            if (pass == 0 || pass == 3) {
+                const bool upward = pass == 0;
+                const auto r = upward ? uprange[level] : dnrange[level];
+                const std::vector<Node>& nodes = upward ? up : dn;
+                const std::vector<int>& first = upward ? up_first : dn_first;
+                const std::vector<int>& cnt = upward ? up_cnt : dn_cnt;
+                ColLists& L = (upward ? cl_m2m : cl_l2l).at(level);
+                std::vector<int> tab(dirpts.size() * 8, -1);
+                for (int ind = 0; ind < 8; ++ind)
+                    for (int i = r.first; i < r.second; ++i) {
+                        const Node& u = nodes[i];
+                        const int c = kids[(size_t)u.box * 8 + ind];
+                        if (c < 0) continue;
+                        long long coff;
+                        if (W == 1.0) {
+                            coff = (long long)lfidx[c] * nE;
+                        } else {
+                            const int ci = find_node(nodes, first[c], cnt[c], predir(u.dir));
+                            if (ci < 0)
+                                throw std::runtime_error(upward ? "child has no directional equivalent density"
+                                                                : "child has no directional check value");
+                            coff = nodes[ci].off;
+                        }
+                        // M2M: child w -> parent sum; L2L: parent t -> child u
+                        if (upward)
+                            L.add(tab, u.did * 8 + ind, coff, u.toff);
+                        else
+                            L.add(tab, u.did * 8 + ind, u.toff, coff);
+                    }
+            } else {
+                const bool upward = pass == 1;
+                const auto r = upward ? uprange[level] : dnrange[level];
+                const std::vector<Node>& nodes = upward ? up : dn;
+                ColLists& L = (upward ? cl_e2 : cl_e2t).at(level);
+                std::vector<int> tab(hfcanon.size(), -1);
+                for (int i = r.first; i < r.second; ++i) {
+                    const Node& u = nodes[i];
+                    if (upward)
+                        L.add(tab, u.canon, u.toff, u.off);
+                    else
+                        L.add(tab, u.canon, u.off, u.toff);
+                }
+            }
+        });
+    }
     // ---------------------------------------------------------------- steps: HF upward
     // widths ascending = levels descending; hf_upeq holds w (upeqnden = E1 w)
     for (auto hit = hflevels.rbegin(); hit != hflevels.rend(); ++hit) {
@@ -1213,70 +1284,38 @@ void Session::build() {
         // one launch for the 8 child positions: a problem per (wedge, child), all adding into
         // the parents' sums
         {
+            ColLists& L = cl_m2m.at(level);
             std::vector<GemmProblem> probs;
-            std::vector<std::vector<long long> > xo, yo;
-            for (int ind = 0; ind < 8; ++ind)
-            for (int i = ur.first; i < ur.second; ++i) {
-                const Node& u = up[i];
-                const int c = kids[(size_t)u.box * 8 + ind];
-                if (c < 0) continue;
-                long long xoff;
-                if (W == 1.0) {
-                    xoff = (long long)lfidx[c] * nE;
+            for (int k : L.key) {
+                const Idx3& dir = did_wedge[k / 8].second;
+                const int ind = k % 8;
+                const DirMats& M = m2m_mats.at(std::make_pair(W, dir));
+                if (M.cached) {
+                    probs.push_back(GemmProblem{nullptr, M.mrows, M.mcols, M.mrows, 0, 0, M.pk[ind]});
                 } else {
-                    const int cit = find_node(up, up_first[c], up_cnt[c], predir(u.dir));
-                    if (cit < 0) throw std::runtime_error("child has no directional equivalent density");
-                    xoff = up[cit].off;
+                    probs.push_back(GemmProblem{KP(M.fin[ind]), M.mrows, M.mcols, M.mrows, 0, 0});
+                    if (!opctx_.empty()) opkey_[KP(M.fin[ind])] = opk("m2m", W, dir, ind);
                 }
-                const size_t pk = (size_t)u.did * 8 + ind;  // (wedge, child) -> problem
-                int p = ptab[pk];
-                if (p < 0) {
-                    const DirMats& M = m2m_mats.at(std::make_pair(W, u.dir));
-                    p = (int)probs.size();
-                    ptab[pk] = p;
-                    touched.push_back(pk);
-                    if (M.cached) {
-                        probs.push_back(GemmProblem{nullptr, M.mrows, M.mcols, M.mrows, 0, 0, M.pk[ind]});
-                    } else {
-                        probs.push_back(GemmProblem{KP(M.fin[ind]), M.mrows, M.mcols, M.mrows, 0, 0});
-                        if (!opctx_.empty()) opkey_[KP(M.fin[ind])] = opk("m2m", W, u.dir, ind);
-                    }
-                    xo.emplace_back();
-                    yo.emplace_back();
-                }
-                xo[p].push_back(xoff);
-                yo[p].push_back(u.toff);
             }
-            reset_tab(ptab);
-            add_gemm(probs, xo, yo, W == 1.0 ? lf_upeq : hf_upeq, T0, GEMM_ATOMIC, width_label("hf_m2m", W));
+            add_gemm(probs, L.x, L.y, W == 1.0 ? lf_upeq : hf_upeq, T0, GEMM_ATOMIC, width_label("hf_m2m", W));
         }
         // w = E2 * (E3 upchkval)   (src/wave3d_eval.cpp:837-849)
-        std::vector<GemmProblem> p2;
-        std::vector<std::vector<long long> > xa, ya;
-        for (int i = ur.first; i < ur.second; ++i) {
-            const Node& u = up[i];
-            int p = ctab[u.canon];
-            if (p < 0) {
-                const Canon& c = hfcanon[u.canon];
-                p = (int)p2.size();
-                ctab[u.canon] = p;
-                touched.push_back(u.canon);
-                const std::string k = opk("e2", c.W, c.srt, 0);
-                if (const float* pk = cached_op(k)) {
+        {
+            ColLists& L = cl_e2.at(level);
+            std::vector<GemmProblem> p2;
+            for (int k : L.key) {
+                const Canon& c = hfcanon[k];
+                const std::string key = opk("e2", c.W, c.srt, 0);
+                if (const float* pk = cached_op(key)) {
                     p2.push_back(GemmProblem{nullptr, c.r1, c.r2, c.r1, 0, 0, pk});
                 } else {
                     const double2* a = opm(c.E2, (size_t)c.r1 * c.r2);
                     p2.push_back(GemmProblem{a, c.r1, c.r2, c.r1, 0, 0});
-                    if (!opctx_.empty()) opkey_[a] = k;
+                    if (!opctx_.empty()) opkey_[a] = key;
                 }
-                xa.emplace_back();
-                ya.emplace_back();
             }
-            xa[p].push_back(u.toff);
-            ya[p].push_back(u.off);
+            add_gemm(p2, L.x, L.y, T0, hf_upeq, GEMM_SET, width_label("hf_uc2ue", W));
         }
-        reset_tab(ctab);
-        add_gemm(p2, xa, ya, T0, hf_upeq, GEMM_SET, width_label("hf_uc2ue", W));
     }
 
     phase("steps_hf_up");
@@ -1303,71 +1342,39 @@ void Session::build() {
             add_gemm(probs, m2l_x[level], m2l_y[level], hf_upeq, hf_dnchk, GEMM_ATOMIC, width_label("hf_m2l", W));
         }
         // t = E2^T u   (dneqnden = E3^T t, src/wave3d_eval.cpp:938-948, src/mlib3d.cpp:246-250)
-        std::vector<GemmProblem> p2;
-        std::vector<std::vector<long long> > xa, xt;
-        for (int i = dr.first; i < dr.second; ++i) {
-            const Node& d = dn[i];
-            int p = ctab[d.canon];
-            if (p < 0) {
-                const Canon& c = hfcanon[d.canon];
-                p = (int)p2.size();
-                ctab[d.canon] = p;
-                touched.push_back(d.canon);
-                const std::string k = opk("e2t", c.W, c.srt, 0);
-                if (const float* pk = cached_op(k)) {
+        {
+            ColLists& L = cl_e2t.at(level);
+            std::vector<GemmProblem> p2;
+            for (int k : L.key) {
+                const Canon& c = hfcanon[k];
+                const std::string key = opk("e2t", c.W, c.srt, 0);
+                if (const float* pk = cached_op(key)) {
                     p2.push_back(GemmProblem{nullptr, c.r2, c.r1, c.r2, 0, 0, pk});
                 } else {
                     const double2* a = opm(c.E2t, (size_t)c.r1 * c.r2);
                     p2.push_back(GemmProblem{a, c.r2, c.r1, c.r2, 0, 0});
-                    if (!opctx_.empty()) opkey_[a] = k;
+                    if (!opctx_.empty()) opkey_[a] = key;
                 }
-                xa.emplace_back();
-                xt.emplace_back();
             }
-            xa[p].push_back(d.off);
-            xt[p].push_back(d.toff);
+            add_gemm(p2, L.x, L.y, hf_dnchk, T1, GEMM_SET, width_label("hf_dc2de", W));
         }
-        reset_tab(ctab);
-        add_gemm(p2, xa, xt, hf_dnchk, T1, GEMM_SET, width_label("hf_dc2de", W));
         // L2L into the children's (pdir) u, or LF dnchkval at W=1 (src/wave3d_eval.cpp:950-991),
         // one launch for the 8 child positions: a problem per (wedge, child)
         {
+            ColLists& L = cl_l2l.at(level);
             std::vector<GemmProblem> probs;
-            std::vector<std::vector<long long> > xo, yo;
-            for (int ind = 0; ind < 8; ++ind)
-            for (int i = dr.first; i < dr.second; ++i) {
-                const Node& d = dn[i];
-                const int c = kids[(size_t)d.box * 8 + ind];
-                if (c < 0) continue;
-                long long yoff;
-                if (W == 1.0) {
-                    yoff = (long long)lfidx[c] * nE;
+            for (int k : L.key) {
+                const Idx3& dir = did_wedge[k / 8].second;
+                const int ind = k % 8;
+                const DirMats& M = l2l_mats.at(std::make_pair(W, dir));
+                if (M.cached) {
+                    probs.push_back(GemmProblem{nullptr, M.mrows, M.mcols, M.mrows, 0, 0, M.pk[ind]});
                 } else {
-                    const int cit = find_node(dn, dn_first[c], dn_cnt[c], predir(d.dir));
-                    if (cit < 0) throw std::runtime_error("child has no directional check value");
-                    yoff = dn[cit].off;
+                    probs.push_back(GemmProblem{KP(M.fin[ind]), M.mrows, M.mcols, M.mrows, 0, 0});
+                    if (!opctx_.empty()) opkey_[KP(M.fin[ind])] = opk("l2l", W, dir, ind);
                 }
-                const size_t pk = (size_t)d.did * 8 + ind;  // (wedge, child) -> problem
-                int p = ptab[pk];
-                if (p < 0) {
-                    const DirMats& M = l2l_mats.at(std::make_pair(W, d.dir));
-                    p = (int)probs.size();
-                    ptab[pk] = p;
-                    touched.push_back(pk);
-                    if (M.cached) {
-                        probs.push_back(GemmProblem{nullptr, M.mrows, M.mcols, M.mrows, 0, 0, M.pk[ind]});
-                    } else {
-                        probs.push_back(GemmProblem{KP(M.fin[ind]), M.mrows, M.mcols, M.mrows, 0, 0});
-                        if (!opctx_.empty()) opkey_[KP(M.fin[ind])] = opk("l2l", W, d.dir, ind);
-                    }
-                    xo.emplace_back();
-                    yo.emplace_back();
-                }
-                xo[p].push_back(d.toff);
-                yo[p].push_back(yoff);
             }
-            reset_tab(ptab);
-            add_gemm(probs, xo, yo, T1, W == 1.0 ? lf_dnchk : hf_dnchk, GEMM_ATOMIC, width_label("hf_l2l", W));
+            add_gemm(probs, L.x, L.y, T1, W == 1.0 ? lf_dnchk : hf_dnchk, GEMM_ATOMIC, width_label("hf_l2l", W));
         }
     }
 
@@ -1648,7 +1655,7 @@ static const char* kernel_name(int kind, int tpi) {
                 default: return "pt_kernel<32>";
             }
         case 2: return "vlist_forward_kernel";
-        case 3: return tpi == VGROUP_L1 ? "vlist_group_kernel<l1>" : "vlist_group_kernel<smem>";
+        case 3: return "vlist_group_kernel";
         case 6: return "vlist_inverse_kernel";
         case 5: return "umma_cgemm_kernel";
         default: return "memset";
@@ -1680,9 +1687,9 @@ void Session::launch_step(const Step& st, cudaStream_t s, double2* spec) {
         case 3:
             if (m)
                 launch_vlist_group32(static_cast<const VaSub*>(st.msubs), st.mpre, 1, st.mtotal, st.v.L.G, nullptr,
-                                     spec != st.v.spec ? spec : nullptr, s, &st.hva, st.tpi);
+                                     spec != st.v.spec ? spec : nullptr, s, &st.hva);
             else
-                launch_vlist_group(st.v.L, st.v.grp, spec, st.v.tsp, s, st.tpi);
+                launch_vlist_group(st.v.L, st.v.grp, spec, st.v.tsp, s);
             break;
         case 6:
             if (m)
@@ -1711,10 +1718,8 @@ void Session::autotune() {
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
     for (Step& st : steps_) {
-        if (st.kind != 1 && st.kind != 3) continue;
-        static const std::vector<int> pt_shapes{32, 16, 8, 4, PT_WARP_TARGETS, PT_WARP_SOURCES};
-        static const std::vector<int> vg_shapes{VGROUP_SMEM, VGROUP_L1};
-        const std::vector<int>& shapes = st.kind == 1 ? pt_shapes : vg_shapes;
+        if (st.kind != 1) continue;
+        static const std::vector<int> shapes{32, 16, 8, 4, PT_WARP_TARGETS, PT_WARP_SOURCES};
         float best = 0.f;
         int best_tpi = shapes[0];
         for (int tpi : shapes) {
@@ -1778,8 +1783,13 @@ std::vector<Session::ProfileEntry> Session::profile_read() {
         e.bytes += st.bytes;
     }
     ev_pending_.clear();
+    // in launch order: by the first step of each label
     std::vector<ProfileEntry> out;
-    for (auto& kv : prof_) out.push_back(kv.second);
+    std::set<std::string> seen;
+    for (const Step& st : steps_) {
+        auto it = prof_.find(st.label);
+        if (it != prof_.end() && seen.insert(st.label).second) out.push_back(it->second);
+    }
     return out;
 }
 

@@ -136,9 +136,7 @@ private:
         // that play the same part (phase, width, step type, occurrence): a Batch
         // merges the steps of its sessions that share a key into one launch.
         long long key;
-        // launch shape, set by autotune(): point interactions: threads per item
-        // (launch_pt; 0 = 32); V-list sums: VGROUP_L1 or VGROUP_SMEM
-        int tpi;
+        int tpi;  // point interactions: launch shape (launch_pt; 0 = 32 threads per item), set by autotune()
         // mixed form: the step as a one-instance launch (device sub-launch array and
         // prefix sums) and the host copy of its sub-launch
         void* msubs;
@@ -190,7 +188,7 @@ private:
     int npts_ = 0;
     std::vector<double> pos_;
     Tree tree_;
-    OperatorLib ops_;
+    std::shared_ptr<const OperatorLib> ops_;  // shared with sessions of the same files
     std::vector<void*> allocs_;
     std::map<const void*, size_t> alloc_bytes_;
     static constexpr size_t kArenaMax = 64 << 10;

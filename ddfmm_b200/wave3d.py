@@ -169,7 +169,8 @@ class Wave3d:
         _lib.check(_lib.load().ddfmm_profile_enable(self._s, 1 if on else 0))
 
     def profile_read(self, reset=True):
-        """Per-pass totals since the last reset: {label: dict(kernel, launches, ms, flops, bytes)}."""
+        """Per-pass totals since the last reset: {label: dict(kernel, launches, ms, flops, bytes)}, in the
+        order the eval first launches each label."""
         self._need()
         arr = (_lib.ddfmm_profile_entry * 64)()
         n = C.c_int()

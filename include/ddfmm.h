@@ -183,8 +183,9 @@ int ddfmm_tree_stats(const double* pos3n, int n, double K, const double* ctr3, i
                      ddfmm_tree_level* levels);
 /* Per-pass profile: while enabled, every launch of ddfmm_eval* is bracketed
  * by CUDA events on its stream.  ddfmm_profile_read returns the totals
- * accumulated since the last reset (one entry per pass label), with the
- * algorithmic flops and DRAM bytes of those launches.  The reference's
+ * accumulated since the last reset (one entry per pass label, in the order
+ * the eval first launches each label), with the algorithmic flops and DRAM
+ * bytes of those launches.  The reference's
  * counterpart is the per-pass wall time it prints (src/wave3d_eval.cpp:59-66). */
 typedef struct ddfmm_profile_entry {
     char label[32];
