@@ -254,18 +254,19 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def gemm_traffic(kernel, workload_name):
-    """DRAM bytes (read + write) per launch of the GEMM kernel over one matvec of
-    the bench workload, from the one-pass ncu capture committed under profiles/,
-    or None for other workloads or kernels."""
-    from ddfmm_b200 import workloads as wl
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "gemm_dram_traffic_sphere_K64_P6.txt")
-    if workload_name != wl.LARGE.name or not os.path.exists(path):
+def gemm_traffic(kernel, algorithmic_bytes):
+    """DRAM bytes (read + write) per launch of the GEMM kernel, scaled from the
+    small-case ncu capture committed under profiles/: the width-1 M2M launch of
+    a K=16 sphere, whose DRAM bytes over its algorithmic bytes give the ratio
+    applied to this workload's algorithmic bytes per launch.  None without the
+    capture."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "gemm_dram_traffic_sphere_K16_P6.txt")
+    if not os.path.exists(path):
         return None
     for line in open(path):
         f = line.split()
         if f and not line.startswith("#") and f[0] == kernel:
-            return (float(f[2]) + float(f[3])) / float(f[1])
+            return (float(f[3]) + float(f[4])) / float(f[2]) * algorithmic_bytes
     return None
 
 
@@ -342,10 +343,11 @@ def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws, profile_json=None, 
         kname = "umma_cgemm_kernel" if precision == _lib.MIXED else "cgemm_kernel"
         roof = {"bound": "tensor", "kernel": kname,
                 "achieved": executed, "peak": peak, "unit": "TFLOP/s", "frac": executed / peak,
-                "traffic": gemm_traffic(kname, w.name),
-                "traffic_note": "DRAM read + write bytes per launch, averaged over one matvec's GEMM launches "
-                                "(one-pass ncu capture); algorithmic bytes per launch with complex64 columns "
-                                "and operators: algorithmic_bytes",
+                "traffic": gemm_traffic(kname, 0.5 * gk["bytes"] / max(1, gk["launches"])),
+                "traffic_note": "DRAM read + write bytes per launch: this workload's algorithmic bytes per launch "
+                                "(complex64 columns and operators: algorithmic_bytes) times the DRAM / algorithmic "
+                                "ratio of an ncu capture of the width-1 M2M launch on a K=16 sphere "
+                                "(profiles/gemm_dram_traffic_sphere_K16_P6.txt)",
                 "algorithmic_bytes": 0.5 * gk["bytes"] / max(1, gk["launches"]),
                 "algorithmic_complex_tflops": algo, "launches": gk["launches"] // 3,
                 "peak_source": src + " (dense TF32 runs at half the BF16 rate on B200's tensor cores)",
@@ -704,9 +706,10 @@ def run_ours(args):
         achieved = dk["flops"] / (dk["ms"] * 1e-3) / 1e12
         roof = {"bound": "tensor", "pipe": "FP64 DMMA (mma.sync.m8n8k4.f64)", "kernel": dom, "achieved": achieved,
                 "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": gemm_traffic(dom, w.name),
-                "traffic_note": "DRAM read + write bytes per launch, averaged over one matvec's GEMM launches "
-                                "(one-pass ncu capture); algorithmic bytes per launch: algorithmic_bytes",
+                "traffic": gemm_traffic(dom, dk["bytes"] / max(1, dk["launches"])),
+                "traffic_note": "DRAM read + write bytes per launch: this workload's algorithmic bytes per launch "
+                                "(algorithmic_bytes) times the DRAM / algorithmic ratio of an ncu capture of the "
+                                "width-1 M2M launch on a K=16 sphere (profiles/gemm_dram_traffic_sphere_K16_P6.txt)",
                 "algorithmic_bytes": dk["bytes"] / max(1, dk["launches"]),
                 "peak_source": "measured cuBLAS DGEMM 4096^3 on this GPU (FP64 has no entry in MEASURED_PEAKS.json)",
                 "launches": dk["launches"]}

@@ -15,6 +15,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libddfmm_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# extra -D options for measuring build-time kernel variants against each other
+# (e.g. DDFMM_NVCC_DEFINES="-DDDFMM_ZGEMM_BK=32 -DDDFMM_ZGEMM_MINB=1"; build(force=True))
+DEFINES = os.environ.get("DDFMM_NVCC_DEFINES", "").split()
 
 
 def sources():
@@ -43,7 +46,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     procs = []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
-        cmd = [NVCC, "-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "-Xptxas", "-v" if verbose else "-O3",
+        cmd = [NVCC, "-std=c++17", "-O3", "-lineinfo", *ARCH, *DEFINES, "-Xcompiler", "-fPIC", "-Xptxas", "-v" if verbose else "-O3",
                "-I", CSRC, "-x", "cu" if src.endswith(".cu") else "c++", "-c", src, "-o", obj]
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
         objs.append(obj)

@@ -5,8 +5,6 @@
 // with r taken as 1 when r^2 < (1e-8)^2, which makes a coincident pair
 // contribute exp(2 pi i) = 1 times the density (src/kernel3d.cpp:21,47-49).
 // The phase is evaluated with sincospi(2r), i.e. without rounding 2*pi*r.
-#include <algorithm>
-
 #include "kernels.cuh"
 
 #include <cstdio>
@@ -71,14 +69,26 @@ void launch_kmat(const KmatJob* jobs, int njobs, long long total, int kernel, cu
 // four-product form at the same FP64 accuracy (outputs agree to ~3e-15).
 // Slabs beyond the operator's rows are skipped (a tile carries
 // ceil(rows / 16) active slabs), so an 80-150-row translation operator
-// wastes at most 15 rows.  K is consumed in slices of 16 through a 3-stage
-// cp.async pipeline; rows, columns and k beyond the problem are zero-filled
+// wastes at most 15 rows.  K is consumed in slices of BK (16) through a
+// GSTAGES-deep (3) cp.async pipeline; rows, columns and k beyond the problem are zero-filled
 // by the copy (src-size 0).  128-bit shared loads are served in 8-lane
 // phases (lanes with g in {2p, 2p+1}, tig 0..3); both fragment layouts put
 // those 8 granules in 8 different bank groups: the operator slice is stored
-// [k][row ^ 2*(k & 3)] and the column slice [col][k] with a 20-granule stride
+// [k][row ^ 2*(k & 3)] and the column slice [col][k] with a BK + 4 granule stride
 // (k = tig and tig + 4 of a fragment share k & 3, hence the same swizzle).
-constexpr int BM = 64, BN = 64, BK = 16, BKP = 20, GSTAGES = 3;
+// Build-time variants (measured against each other): K slice DDFMM_ZGEMM_BK
+// (16 or 32), ring depth DDFMM_ZGEMM_STAGES, blocks per SM DDFMM_ZGEMM_MINB.
+#ifndef DDFMM_ZGEMM_BK
+#define DDFMM_ZGEMM_BK 16
+#endif
+#ifndef DDFMM_ZGEMM_STAGES
+#define DDFMM_ZGEMM_STAGES 3
+#endif
+#ifndef DDFMM_ZGEMM_MINB
+#define DDFMM_ZGEMM_MINB 2
+#endif
+constexpr int BM = 64, BN = 64, BK = DDFMM_ZGEMM_BK, BKP = BK + 4, GSTAGES = DDFMM_ZGEMM_STAGES;
+static_assert(BK == 16 || BK == 32, "K slice of 16 or 32");
 constexpr int GSTAGE = BK * BM + BN * BKP;  // double2 per stage
 constexpr int GEMM_SMEM = GSTAGES * GSTAGE * (int)sizeof(double2);
 
@@ -99,7 +109,7 @@ __device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[4], con
         : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-__global__ void __launch_bounds__(256, 2) zgemm_kernel(const GemmProblem* __restrict__ probs,
+__global__ void __launch_bounds__(256, DDFMM_ZGEMM_MINB) zgemm_kernel(const GemmProblem* __restrict__ probs,
                                                        const GemmTile* __restrict__ tiles,
                                                        const long long* __restrict__ xoff,
                                                        const long long* __restrict__ yoff,
@@ -130,8 +140,8 @@ __global__ void __launch_bounds__(256, 2) zgemm_kernel(const GemmProblem* __rest
                        ok ? (const void*)(p.A + (size_t)gk * p.lda + t.row0 + row) : (const void*)p.A, ok ? 16 : 0);
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            int e = tid + 256 * q, kk = e & 15, col = e >> 4;
+        for (int q = 0; q < BN * BK / 256; ++q) {
+            int e = tid + 256 * q, kk = e % BK, col = e / BK;
             int gk = k0 + kk;
             bool ok = col < ncol && gk < p.k;
             cp_async16(&Xs[col * BKP + kk], ok ? (const void*)(X + xo[col] + gk) : (const void*)X, ok ? 16 : 0);

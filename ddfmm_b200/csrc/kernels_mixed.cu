@@ -8,8 +8,6 @@
 // in FP32 on coordinate differences formed in FP64 (|p_t - p_s| is then
 // exact to FP32 and the phase 2 pi r stays accurate however far from the
 // origin the leaf sits).
-#include <algorithm>
-
 #include "kernels.cuh"
 
 namespace ddfmm {
