@@ -1408,19 +1408,27 @@ void Session::build() {
                 tlist.push_back(std::make_pair(morton(par), std::make_pair(ct, l)));
             }
             std::sort(tlist.begin(), tlist.end());
-            std::vector<int> trg, gptr(1, 0), gtrg;
-            std::vector<int2> gsrc;
-            std::vector<std::pair<int, int> > ent;  // (source lf id, (tbase << 8) | mask) of the current group
+            // per target parent: its children's tsp rows and, by local source position
+            // (the tensor index of the pair for child 0, tbase), the source and the mask
+            // of the children that list it
+            struct Parent {
+                Idx3 idx;
+                int trow[8];
+                std::map<int, std::pair<int, int> > by_tbase;  // tbase -> (source lf id, child mask)
+            };
+            std::vector<Parent> parents;
+            std::vector<int> trg;
+            std::map<Idx3, int> parent_at;
             for (size_t i = 0; i < tlist.size();) {
                 size_t j = i;
                 while (j < tlist.size() && tlist[j].first == tlist[i].first) ++j;  // one parent: [i, j)
-                const size_t g0 = gtrg.size();
-                gtrg.resize(g0 + 8, -1);
-                std::map<int, int> srcs;  // source lf id -> (tbase << 8) | mask
+                Parent pa;
+                for (int c = 0; c < 8; ++c) pa.trow[c] = -1;
                 for (size_t k = i; k < j; ++k) {
                     const int ct = tlist[k].second.first, l = tlist[k].second.second;
                     const Box& B = T.boxes[lfbox[l]];
-                    gtrg[g0 + ct] = (int)trg.size();
+                    pa.idx = Idx3{{B.idx[0] >> 1, B.idx[1] >> 1, B.idx[2] >> 1}};
+                    pa.trow[ct] = (int)trg.size();
                     trg.push_back(l);
                     for (int s : B.vlist) {
                         const Box& SB = T.boxes[s];
@@ -1436,15 +1444,50 @@ void Session::build() {
                         const int voff = (o[0] + 3) + 7 * ((o[1] + 3) + 7 * (o[2] + 3));
                         if (tbase + ((ct >> 2) & 1) + 7 * ((ct >> 1) & 1) + 49 * (ct & 1) != voff)
                             throw std::logic_error("V-list offset bookkeeping");
-                        int& e = srcs[lfidx[s]];
-                        e = (tbase << 8) | (e & 255) | (1 << ct);
+                        auto& e = pa.by_tbase[tbase];
+                        if (e.second == 0) e.first = lfidx[s];
+                        if (e.first != lfidx[s]) throw std::logic_error("V-list source position bookkeeping");
+                        e.second |= 1 << ct;
                         is_src[lfidx[s]] = 1;
                         stats_.v_pairs++;
                     }
                 }
-                for (auto& kv : srcs) gsrc.push_back(make_int2(kv.first, kv.second));
-                gptr.push_back((int)gsrc.size());
+                parent_at[pa.idx] = (int)parents.size();
+                parents.push_back(std::move(pa));
                 i = j;
+            }
+            // groups: a parent with its +x neighbour when that one has targets too (each
+            // source position's tensor values then serve both), else alone; in the
+            // parents' Morton order
+            std::vector<int> gptr(1, 0), gtrg;
+            std::vector<int4> gsrc;
+            std::vector<char> taken(parents.size(), 0);
+            for (size_t pi = 0; pi < parents.size(); ++pi) {
+                if (taken[pi]) continue;
+                taken[pi] = 1;
+                const Parent& A = parents[pi];
+                const Parent* B = nullptr;
+                auto it = parent_at.find(Idx3{{A.idx[0] + 1, A.idx[1], A.idx[2]}});
+                if (it != parent_at.end() && !taken[it->second]) {
+                    taken[it->second] = 1;
+                    B = &parents[it->second];
+                }
+                for (int c = 0; c < 8; ++c) gtrg.push_back(A.trow[c]);
+                for (int c = 0; c < 8; ++c) gtrg.push_back(B ? B->trow[c] : -1);
+                std::map<int, int4> ents;  // tbase -> (row A, row B, tbase, mask A | mask B << 8)
+                for (auto& kv : A.by_tbase) ents[kv.first] = make_int4(kv.second.first, -1, kv.first, kv.second.second);
+                if (B)
+                    for (auto& kv : B->by_tbase) {
+                        auto e = ents.find(kv.first);
+                        if (e == ents.end())
+                            ents[kv.first] = make_int4(-1, kv.second.first, kv.first, kv.second.second << 8);
+                        else {
+                            e->second.y = kv.second.first;
+                            e->second.w |= kv.second.second << 8;
+                        }
+                    }
+                for (auto& kv : ents) gsrc.push_back(kv.second);
+                gptr.push_back((int)gsrc.size());
             }
             if (!trg.empty()) {
                 std::vector<int> srcb;
@@ -1478,7 +1521,7 @@ void Session::build() {
                                                                   : salloc(tsp_elems);
                 const int ngroups = (int)gptr.size() - 1;
                 long long npairs = 0;
-                for (const int2& e2 : gsrc) npairs += __builtin_popcount(e2.y & 255);
+                for (const int4& e4 : gsrc) npairs += __builtin_popcount(e4.w & 0xffff);
                 Step a{};
                 a.kind = 3;
                 a.label = "lf_vlist_m2l";
