@@ -283,12 +283,12 @@ __global__ void pt_kernel(const PtItem* __restrict__ items, int nitems, const Pt
 // one warp per item, its source points staged PTW_TILE at a time in shared
 // memory (scaled and shifted once, not once per target), segment descriptors
 // 32 at a time with their point counts prefix-summed across the warp.  MODE 0:
-// lane = target (up to PTW_TPL per lane), sources read by broadcast; MODE 1:
-// PTW_TT targets per pass, lane = every 32nd source, per-target sums reduced
+// lane = target (up to NT per lane), sources read by broadcast; MODE 1:
+// NT targets per pass, lane = every 32nd source, per-target sums reduced
 // with warp shuffles.
-constexpr int PTW_WARPS = 8, PTW_TILE = 64, PTW_TPL = 4, PTW_TT = 8;
+constexpr int PTW_WARPS = 8, PTW_TILE = 64;
 
-template <int MODE>
+template <int MODE, int NT>
 __global__ void __launch_bounds__(32 * PTW_WARPS) ptw_kernel(const PtItem* __restrict__ items, int nitems,
                                                              const PtSrc* __restrict__ srcs, int kernel) {
     __shared__ double sx[PTW_WARPS][PTW_TILE], sy[PTW_WARPS][PTW_TILE], sz[PTW_WARPS][PTW_TILE];
@@ -300,8 +300,7 @@ __global__ void __launch_bounds__(32 * PTW_WARPS) ptw_kernel(const PtItem* __res
     if (w >= nitems) return;  // whole warps only: the kernel syncs nothing wider than a warp
     const PtItem it = items[w];
     const PtSet& T = it.trg;
-    constexpr int NT = MODE == 0 ? PTW_TPL : PTW_TT;
-    constexpr int TCH = MODE == 0 ? 32 * PTW_TPL : PTW_TT;  // targets per pass
+    constexpr int TCH = MODE == 0 ? 32 * NT : NT;  // targets per pass
     for (int t0 = 0; t0 < T.n; t0 += TCH) {
         double tx[NT], ty[NT], tz[NT];
         double2 acc[NT];
@@ -408,12 +407,14 @@ __global__ void __launch_bounds__(32 * PTW_WARPS) ptw_kernel(const PtItem* __res
 
 void launch_pt(const PtItem* items, int nitems, const PtSrc* srcs, int kernel, cudaStream_t s, int tpi) {
     if (nitems == 0) return;
-    if (tpi == PT_WARP_TARGETS || tpi == PT_WARP_SOURCES) {
+    if (pt_warp_shape(tpi)) {
         const int blocks = (nitems + PTW_WARPS - 1) / PTW_WARPS;
-        if (tpi == PT_WARP_TARGETS)
-            ptw_kernel<0><<<blocks, 32 * PTW_WARPS, 0, s>>>(items, nitems, srcs, kernel);
-        else
-            ptw_kernel<1><<<blocks, 32 * PTW_WARPS, 0, s>>>(items, nitems, srcs, kernel);
+        switch (tpi) {
+            case PT_WARP_TARGETS: ptw_kernel<0, 4><<<blocks, 32 * PTW_WARPS, 0, s>>>(items, nitems, srcs, kernel); break;
+            case PT_WARP_TARGETS2: ptw_kernel<0, 2><<<blocks, 32 * PTW_WARPS, 0, s>>>(items, nitems, srcs, kernel); break;
+            case PT_WARP_SOURCES: ptw_kernel<1, 8><<<blocks, 32 * PTW_WARPS, 0, s>>>(items, nitems, srcs, kernel); break;
+            default: ptw_kernel<1, 4><<<blocks, 32 * PTW_WARPS, 0, s>>>(items, nitems, srcs, kernel); break;
+        }
         return;
     }
     const int blocks = (int)(((long long)nitems * tpi + 255) / 256);

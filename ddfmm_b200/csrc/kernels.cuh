@@ -65,9 +65,11 @@ void launch_gemm(const GemmProblem* probs_dev, const GemmTile* tiles_dev, int nt
 // tpi: the launch shape, chosen per step by the session's autotuner: 4, 8, 16 or
 // 32 threads per item, each thread taking targets and walking the sources in
 // global memory; or one warp per item with the item's sources staged in
-// shared memory, lanes over targets (PT_WARP_TARGETS) or over sources with a
-// warp-shuffle reduction per target (PT_WARP_SOURCES)
-constexpr int PT_WARP_TARGETS = 1001, PT_WARP_SOURCES = 1002;
+// shared memory, lanes over targets (PT_WARP_TARGETS: 4 targets a lane;
+// PT_WARP_TARGETS2: 2, fewer registers) or over sources with a warp-shuffle
+// reduction per target (PT_WARP_SOURCES: 8 targets a pass; PT_WARP_SOURCES4: 4)
+constexpr int PT_WARP_TARGETS = 1001, PT_WARP_SOURCES = 1002, PT_WARP_TARGETS2 = 1003, PT_WARP_SOURCES4 = 1004;
+__host__ __device__ constexpr bool pt_warp_shape(int tpi) { return tpi >= PT_WARP_TARGETS && tpi <= PT_WARP_SOURCES4; }
 void launch_pt(const PtItem* items_dev, int nitems, const PtSrc* srcs_dev, int kernel, cudaStream_t s, int tpi = 32);
 
 // FFT-based low-frequency M2L on a G^3 grid (G = 2P), see kernels.cu.

@@ -280,15 +280,15 @@ __global__ void pt32_kernel(const PtSub* __restrict__ subs, const int* __restric
 // FP64, not once per target); every difference is taken in FP64 and rounded
 // to FP32 before the kernel is evaluated, as in pt32_kernel, so |p_t - p_s|
 // is accurate to FP32 however close the pair (a coincident pair gives exactly
-// zero).  MODE 0: each lane owns up to PTW_TPL targets (lane + 32 i) and walks
-// the staged sources (broadcast reads); MODE 1: the targets go PTW_TT at a
+// zero).  MODE 0: each lane owns up to NT targets (lane + 32 i) and walks
+// the staged sources (broadcast reads); MODE 1: the targets go NT at a
 // time, each lane takes every 32nd staged source and the per-target sums are
 // reduced across the warp with shuffles.  Segment descriptors are read 32 at
 // a time into shared memory; their point counts, prefix-summed across the
 // warp, map a staged point to its segment.
-constexpr int PTW_WARPS = 8, PTW_TILE = 64, PTW_TPL = 4, PTW_TT = 8;
+constexpr int PTW_WARPS = 8, PTW_TILE = 64;
 
-template <int MODE>
+template <int MODE, int NT>
 __global__ void __launch_bounds__(32 * PTW_WARPS) pt32w_kernel(const PtSub* __restrict__ subs,
                                                                const int* __restrict__ prefix, int nsub, int nitems,
                                                                const int* __restrict__ active) {
@@ -305,8 +305,7 @@ __global__ void __launch_bounds__(32 * PTW_WARPS) pt32w_kernel(const PtSub* __re
     const PtItem it = S.items[w - prefix[j]];
     float2* out = reinterpret_cast<float2*>(it.out);
     const PtSet& T = it.trg;
-    constexpr int NT = MODE == 0 ? PTW_TPL : PTW_TT;
-    constexpr int TCH = MODE == 0 ? 32 * PTW_TPL : PTW_TT;  // targets per pass
+    constexpr int TCH = MODE == 0 ? 32 * NT : NT;  // targets per pass
     for (int t0 = 0; t0 < T.n; t0 += TCH) {
         double tx[NT], ty[NT], tz[NT];
         float2 acc[NT];
@@ -411,12 +410,14 @@ __global__ void __launch_bounds__(32 * PTW_WARPS) pt32w_kernel(const PtSub* __re
 void launch_pt32(const PtSub* subs, const int* prefix, int nsub, int nitems, const int* active, cudaStream_t s,
                  int tpi) {
     if (nitems == 0) return;
-    if (tpi == PT_WARP_TARGETS || tpi == PT_WARP_SOURCES) {
+    if (pt_warp_shape(tpi)) {
         const int blocks = (nitems + PTW_WARPS - 1) / PTW_WARPS;
-        if (tpi == PT_WARP_TARGETS)
-            pt32w_kernel<0><<<blocks, 32 * PTW_WARPS, 0, s>>>(subs, prefix, nsub, nitems, active);
-        else
-            pt32w_kernel<1><<<blocks, 32 * PTW_WARPS, 0, s>>>(subs, prefix, nsub, nitems, active);
+        switch (tpi) {
+            case PT_WARP_TARGETS: pt32w_kernel<0, 4><<<blocks, 32 * PTW_WARPS, 0, s>>>(subs, prefix, nsub, nitems, active); break;
+            case PT_WARP_TARGETS2: pt32w_kernel<0, 2><<<blocks, 32 * PTW_WARPS, 0, s>>>(subs, prefix, nsub, nitems, active); break;
+            case PT_WARP_SOURCES: pt32w_kernel<1, 8><<<blocks, 32 * PTW_WARPS, 0, s>>>(subs, prefix, nsub, nitems, active); break;
+            default: pt32w_kernel<1, 4><<<blocks, 32 * PTW_WARPS, 0, s>>>(subs, prefix, nsub, nitems, active); break;
+        }
         return;
     }
     const int blocks = (int)(((long long)nitems * tpi + 255) / 256);

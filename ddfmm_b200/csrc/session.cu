@@ -1693,8 +1693,10 @@ static const char* kernel_name(int kind, int tpi) {
                 case 4: return "pt_kernel<4>";
                 case 8: return "pt_kernel<8>";
                 case 16: return "pt_kernel<16>";
-                case PT_WARP_TARGETS: return "ptw_kernel<targets>";
-                case PT_WARP_SOURCES: return "ptw_kernel<sources>";
+                case PT_WARP_TARGETS: return "ptw_kernel<targets,4>";
+                case PT_WARP_TARGETS2: return "ptw_kernel<targets,2>";
+                case PT_WARP_SOURCES: return "ptw_kernel<sources,8>";
+                case PT_WARP_SOURCES4: return "ptw_kernel<sources,4>";
                 default: return "pt_kernel<32>";
             }
         case 2: return "vlist_forward_kernel";
@@ -1762,7 +1764,8 @@ void Session::autotune() {
     CK(cudaEventCreate(&b));
     for (Step& st : steps_) {
         if (st.kind != 1) continue;
-        static const std::vector<int> shapes{32, 16, 8, 4, PT_WARP_TARGETS, PT_WARP_SOURCES};
+        static const std::vector<int> shapes{32, 16, 8, 4, PT_WARP_TARGETS, PT_WARP_TARGETS2, PT_WARP_SOURCES,
+                                             PT_WARP_SOURCES4};
         float best = 0.f;
         int best_tpi = shapes[0];
         for (int tpi : shapes) {
