@@ -1,0 +1,34 @@
+"""Host-only pieces of the launch plan (ddfmm_b200/csrc/plan.hpp), checked
+without a GPU by a C++ driver linked against the library."""
+import os
+import subprocess
+
+import pytest
+
+from ddfmm_b200 import geometry
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.join(ROOT, "ddfmm_b200")
+
+
+@pytest.fixture(scope="module")
+def plan_test(tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("plan") / "plan_test")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(LIBDIR, "csrc"), "-o", out,
+                    os.path.join(ROOT, "tests", "cpp", "plan_test.cpp"), os.path.join(LIBDIR, "libddfmm_b200.so"),
+                    "-Wl,-rpath," + LIBDIR], check=True)
+    return out
+
+
+@pytest.mark.parametrize("geom,K,N,ptsmax", [("sphere", 8.0, 5027, 100), ("sphere", 16.0, 20106, 100),
+                                             ("ellipsoid", 8.0, 3000, 100), ("cluster", 4.0, 1500, 8)])
+def test_vlist_groups_cover_every_pair_once(plan_test, tmp_path, geom, K, N, ptsmax):
+    pos = {"sphere": geometry.sphere_points, "ellipsoid": geometry.ellipsoid_points,
+           "cluster": geometry.cluster_points}[geom](N, K)
+    path = tmp_path / "pos.bin"
+    pos.astype("<f8").tofile(path)
+    r = subprocess.run([plan_test, str(path), str(len(pos)), repr(K), str(geometry.cells_for(K)),
+                        str(geometry.maxlevel_for(K)), str(ptsmax)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    words = r.stdout.split()
+    assert words[0] == "ok" and int(words[2]) > 0, r.stdout
