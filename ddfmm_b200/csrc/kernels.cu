@@ -504,20 +504,19 @@ __global__ void __launch_bounds__(vt_threads(G)) vlist_forward_kernel(VlistLevel
 }
 
 // The pointwise products of the V list, by target parent: warp w of a block
-// takes group blockIdx.x * VGROUP_WARPS + w (one parent or a pair, see
-// VlistGroups) and lane l frequency 32 blockIdx.y + l of the G^3 grid, with
-// one accumulator per child position of each parent.  The loop over the
-// group's source entries is the same for the 32 lanes, so the mask branches
-// are warp-uniform; a source's spectrum value is loaded once and used by every
-// child of its parent that lists it, and a tensor value once for both
-// parents.  Blocks of one frequency chunk run together (blockIdx.x varies
-// fastest), so the translation tensors' 32-frequency slices of that chunk
-// (316 x 512 bytes) mostly stay in the SM's L1 while the chunk lasts, and the
-// source spectra's slices in L2.
+// takes target parent blockIdx.x * VGROUP_WARPS + w and lane l frequency
+// 32 blockIdx.y + l of the G^3 grid, with one accumulator per child position.
+// The loop over the parent's source entries is the same for the 32 lanes, so
+// the child mask branches are warp-uniform; a source's spectrum value is
+// loaded once and used by every child that has it in its V list.  Blocks of
+// one frequency chunk run together (blockIdx.x varies fastest), so the
+// translation tensors' 32-frequency slices of that chunk (316 x 512 bytes)
+// stay in the SM's L1 while the chunk lasts, and the source spectra's slices
+// (32 MB over all boxes at the bench workload) in L2.
 __host__ __device__ constexpr int child_voff(int c) { return ((c >> 2) & 1) + 7 * ((c >> 1) & 1) + 49 * (c & 1); }
 
 template <int G>
-__global__ void __launch_bounds__(256) vlist_group_kernel(const int* __restrict__ gptr, const int4* __restrict__ gsrc,
+__global__ void __launch_bounds__(256) vlist_group_kernel(const int* __restrict__ gptr, const int2* __restrict__ gsrc,
                                                           const int* __restrict__ gtrg, int ngroups,
                                                           const double2* __restrict__ spec,
                                                           const double2* __restrict__ tns, double2* __restrict__ tsp) {
@@ -525,29 +524,23 @@ __global__ void __launch_bounds__(256) vlist_group_kernel(const int* __restrict_
     const int grp = blockIdx.x * VGROUP_WARPS + (threadIdx.x >> 5);
     if (grp >= ngroups) return;
     const int f = blockIdx.y * 32 + (threadIdx.x & 31);
-    double2 acc[8], bcc[8];
+    double2 acc[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) acc[c] = bcc[c] = make_double2(0.0, 0.0);
+    for (int c = 0; c < 8; ++c) acc[c] = make_double2(0.0, 0.0);
     const int e1 = __ldg(gptr + grp + 1);
     for (int e = __ldg(gptr + grp); e < e1; ++e) {
-        const int4 ent = __ldg(gsrc + e);
-        const int ma = ent.w & 255, mb = (ent.w >> 8) & 255;
-        const double2 Sa = ent.x >= 0 ? __ldg(spec + (size_t)ent.x * G3 + f) : make_double2(0.0, 0.0);
-        const double2 Sb = ent.y >= 0 ? __ldg(spec + (size_t)ent.y * G3 + f) : make_double2(0.0, 0.0);
-        const double2* tb = tns + (size_t)ent.z * G3 + f;
+        const int2 ent = __ldg(gsrc + e);
+        const double2 S = __ldg(spec + (size_t)ent.x * G3 + f);
+        const int mask = ent.y & 255;
+        const double2* tb = tns + (size_t)(ent.y >> 8) * G3 + f;
 #pragma unroll
         for (int c = 0; c < 8; ++c)
-            if ((ma | mb) & (1 << c)) {
-                const double2 t = __ldg(tb + (size_t)child_voff(c) * G3);
-                if (ma & (1 << c)) cfma(acc[c], t, Sa);
-                if (mb & (1 << c)) cfma(bcc[c], t, Sb);
-            }
+            if (mask & (1 << c)) cfma(acc[c], __ldg(tb + (size_t)child_voff(c) * G3), S);
     }
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-        const int ta = __ldg(gtrg + 16 * grp + c), tb2 = __ldg(gtrg + 16 * grp + 8 + c);
-        if (ta >= 0) tsp[(size_t)ta * G3 + f] = acc[c];
-        if (tb2 >= 0) tsp[(size_t)tb2 * G3 + f] = bcc[c];
+        const int t = __ldg(gtrg + 8 * grp + c);
+        if (t >= 0) tsp[(size_t)t * G3 + f] = acc[c];
     }
 }
 

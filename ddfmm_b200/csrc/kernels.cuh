@@ -90,24 +90,20 @@ size_t vt_smem(int G, size_t es);
 void launch_vlist_forward(const VlistLevel& L, const int* boxes, int nbox, const double2* upeq,
                           double2* spec, cudaStream_t s);
 // The V-list sums in Fourier space, by target parent: the target boxes of a
-// level are grouped by their parent, and a parent is paired with its +x
-// neighbour when that one has targets too (groups in Morton order of the
-// first parent).  A group lists the source positions around its parents: a
-// source at position r in [-2, 3]^3 relative to twice a parent's index has
-// the translation-tensor index tbase = (3 - r0) + 7 (3 - r1) + 49 (3 - r2) for
-// child position 0 of that parent, and child position c = 4a + 2b + c' adds
-// a + 7b + 49c' -- the same for both parents of a group, so one tensor value
-// serves both.  An entry is
-//   {spectrum row of parent A's source at r (or -1), the same for parent B,
-//    tbase, mask A | mask B << 8}
-// where bit c of a mask says that the child at position c of that parent has
-// the source in its V list.  tsp[t] (G^3 per target) receives the summed
-// spectrum of target t, overwritten each eval.
-constexpr int VGROUP_WARPS = 8;  // groups per block of the sums
+// level are grouped by their parent (the groups in Morton order of the
+// parents); a group lists the union of its targets' V-list sources, each as
+//   {spectrum row of the source, (tbase << 8) | mask}
+// where bit c of mask says that the child at position c = 4a + 2b + c' of
+// the parent (offset (a, b, c') from twice the parent's index) has the
+// source in its V list, and tbase is the translation-tensor index of that
+// pair for child position 0; child position c adds a + 7b + 49c'.
+// tsp[t] (G^3 per target, rows in group order) receives the summed spectrum
+// of target t, overwritten each eval.
+constexpr int VGROUP_WARPS = 8;  // target parents per block of the sums
 struct VlistGroups {
     const int* gptr;   // ngroups + 1: the source entries of each group
-    const int4* gsrc;  // the source entries
-    const int* gtrg;   // ngroups x 16: row of tsp of each child position of parent A, then B; -1 where none
+    const int2* gsrc;  // the source entries
+    const int* gtrg;   // ngroups x 8: row of tsp of each child position, -1 where none
     int ngroups;
 };
 void launch_vlist_group(const VlistLevel& L, const VlistGroups& V, const double2* spec, double2* tsp,
@@ -149,7 +145,7 @@ struct VfSub {  // V-list source spectra, one work item per source box
 struct VaSub {  // V-list sums by target parent (VlistGroups), one work item per group
     VlistLevel L;
     const int* gptr;
-    const int4* gsrc;
+    const int2* gsrc;
     const int* gtrg;
     const float2* spec;
     float2* tsp;

@@ -524,7 +524,7 @@ __device__ __forceinline__ void vlist_forward32_body(const VfSub& S, int local, 
 }
 
 // V-list sums by target parent (see vlist_group_kernel in kernels.cu): warp =
-// one group (a target parent or a pair), lane = one frequency of a 32-frequency chunk
+// one group (target parent), lane = one frequency of a 32-frequency chunk
 // (blockIdx.y).  MULTI: each warp finds its own sub-launch from the prefix
 // sums of the groups; spec_override replaces the source spectra (single
 // instance).
@@ -548,30 +548,24 @@ __global__ void __launch_bounds__(256) vlist_group32_kernel(const VaSub one, con
     const float2* __restrict__ spec = spec_override ? spec_override : S.spec;
     const float2* __restrict__ tns = reinterpret_cast<const float2*>(S.L.tns);
     const int f = blockIdx.y * 32 + (threadIdx.x & 31);
-    float2 acc[8], bcc[8];
+    float2 acc[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) acc[c] = bcc[c] = make_float2(0.f, 0.f);
+    for (int c = 0; c < 8; ++c) acc[c] = make_float2(0.f, 0.f);
     const int e1 = __ldg(S.gptr + grp + 1);
     for (int e = __ldg(S.gptr + grp); e < e1; ++e) {
-        const int4 ent = __ldg(S.gsrc + e);
-        const int ma = ent.w & 255, mb = (ent.w >> 8) & 255;
-        const float2 sa = ent.x >= 0 ? __ldg(spec + (size_t)ent.x * G3 + f) : make_float2(0.f, 0.f);
-        const float2 sb = ent.y >= 0 ? __ldg(spec + (size_t)ent.y * G3 + f) : make_float2(0.f, 0.f);
-        const float2* tb = tns + (size_t)ent.z * G3 + f;
+        const int2 ent = __ldg(S.gsrc + e);
+        const float2 sv = __ldg(spec + (size_t)ent.x * G3 + f);
+        const int mask = ent.y & 255;
+        const float2* tb = tns + (size_t)(ent.y >> 8) * G3 + f;
 #pragma unroll
         for (int c = 0; c < 8; ++c)
-            if ((ma | mb) & (1 << c)) {
-                const float2 t = __ldg(tb + (size_t)child_voff32(c) * G3);
-                if (ma & (1 << c)) cfma32(acc[c], t, sa);
-                if (mb & (1 << c)) cfma32(bcc[c], t, sb);
-            }
+            if (mask & (1 << c)) cfma32(acc[c], __ldg(tb + (size_t)child_voff32(c) * G3), sv);
     }
     float2* tsp = S.tsp;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-        const int ta = __ldg(S.gtrg + 16 * grp + c), tb2 = __ldg(S.gtrg + 16 * grp + 8 + c);
-        if (ta >= 0) tsp[(size_t)ta * G3 + f] = acc[c];
-        if (tb2 >= 0) tsp[(size_t)tb2 * G3 + f] = bcc[c];
+        const int t = __ldg(S.gtrg + 8 * grp + c);
+        if (t >= 0) tsp[(size_t)t * G3 + f] = acc[c];
     }
 }
 

@@ -1433,7 +1433,7 @@ void Session::build() {
                 // compulsory: each source spectrum, the 316 tensors, each target's summed spectrum
                 a.bytes = 16.0 * ((double)G3 * srcb.size() + 316.0 * G3 + (double)G3 * trg.size());
                 a.v.L = VL;
-                a.v.grp = VlistGroups{upload(vg.gptr), reinterpret_cast<const int4*>(upload(vg.gsrc)), upload(vg.gtrg),
+                a.v.grp = VlistGroups{upload(vg.gptr), reinterpret_cast<const int2*>(upload(vg.gsrc)), upload(vg.gtrg),
                                       ngroups};
                 a.v.spec = lf_spec;
                 a.v.tsp = tsp;

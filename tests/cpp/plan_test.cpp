@@ -38,7 +38,7 @@ int main(int argc, char** argv) {
         }
     std::map<int, std::vector<int> > levels;
     for (int l = 0; l < (int)lfbox.size(); ++l) levels[T.boxes[lfbox[l]].level].push_back(l);
-    long long pairs = 0, groups = 0, paired = 0;
+    long long pairs = 0, groups = 0;
     for (auto& kv : levels) {
         const VlistGroupPlan g = vlist_groups(T, lfbox, lfidx, kv.second);
         std::set<std::pair<int, int> > want, got;  // (target lf id, source lf id)
@@ -47,35 +47,29 @@ int main(int argc, char** argv) {
         std::set<int> rows;
         for (size_t k = 0; k + 1 < g.gptr.size(); ++k) {
             groups++;
-            bool has_b = false;
             for (int e = g.gptr[k]; e < g.gptr[k + 1]; ++e) {
                 const VgEntry& E = g.gsrc[e];
-                for (int side = 0; side < 2; ++side) {
-                    const int mask = (E.masks >> (8 * side)) & 255, row = side ? E.row_b : E.row_a;
-                    if (mask && row < 0) { std::printf("mask without a source\n"); return 1; }
-                    for (int c = 0; c < 8; ++c) {
-                        if (!(mask & (1 << c))) continue;
-                        const int tr = g.gtrg[16 * k + 8 * side + c];
-                        if (tr < 0) { std::printf("pair for a missing child\n"); return 1; }
-                        has_b |= side == 1;
-                        const int t = g.trg[tr];
-                        const Box& TB = T.boxes[lfbox[t]];
-                        const Box& SB = T.boxes[lfbox[row]];
-                        int o[3];
-                        for (int d = 0; d < 3; ++d) o[d] = TB.idx[d] - SB.idx[d];
-                        const int voff = (o[0] + 3) + 7 * ((o[1] + 3) + 7 * (o[2] + 3));
-                        if (E.tbase + vlist_child_voff(c) != voff) { std::printf("tensor index\n"); return 1; }
-                        if ((TB.idx[0] & 1) * 4 + (TB.idx[1] & 1) * 2 + (TB.idx[2] & 1) != c) {
-                            std::printf("child position\n");
-                            return 1;
-                        }
-                        if (!got.insert(std::make_pair(t, row)).second) { std::printf("pair twice\n"); return 1; }
+                const int mask = E.tbase_mask & 255, tbase = E.tbase_mask >> 8;
+                for (int c = 0; c < 8; ++c) {
+                    if (!(mask & (1 << c))) continue;
+                    const int tr = g.gtrg[8 * k + c];
+                    if (tr < 0) { std::printf("pair for a missing child\n"); return 1; }
+                    const int t = g.trg[tr];
+                    const Box& TB = T.boxes[lfbox[t]];
+                    const Box& SB = T.boxes[lfbox[E.row]];
+                    int o[3];
+                    for (int d = 0; d < 3; ++d) o[d] = TB.idx[d] - SB.idx[d];
+                    const int voff = (o[0] + 3) + 7 * ((o[1] + 3) + 7 * (o[2] + 3));
+                    if (tbase + vlist_child_voff(c) != voff) { std::printf("tensor index\n"); return 1; }
+                    if ((TB.idx[0] & 1) * 4 + (TB.idx[1] & 1) * 2 + (TB.idx[2] & 1) != c) {
+                        std::printf("child position\n");
+                        return 1;
                     }
+                    if (!got.insert(std::make_pair(t, E.row)).second) { std::printf("pair twice\n"); return 1; }
                 }
             }
-            paired += has_b;
-            for (int c = 0; c < 16; ++c)
-                if (g.gtrg[16 * k + c] >= 0 && !rows.insert(g.gtrg[16 * k + c]).second) {
+            for (int c = 0; c < 8; ++c)
+                if (g.gtrg[8 * k + c] >= 0 && !rows.insert(g.gtrg[8 * k + c]).second) {
                     std::printf("row twice\n");
                     return 1;
                 }
@@ -85,6 +79,6 @@ int main(int argc, char** argv) {
         if (rows.size() != g.trg.size()) { std::printf("rows\n"); return 1; }
         pairs += g.pairs;
     }
-    std::printf("ok pairs %lld groups %lld paired %lld\n", pairs, groups, paired);
+    std::printf("ok pairs %lld groups %lld\n", pairs, groups);
     return 0;
 }
