@@ -354,10 +354,13 @@ def measure_mixed(w, wave_args, steps, warmup, dev, chk, ws, profile_json=None, 
                 "note": "executed = 3 x algorithmic (hi*hi + lo*hi + hi*lo TF32 products)"}
     m.close()
     gemm = "tcgen05" if precision == _lib.MIXED else "mma.sync"
+    passes = {lab: {"ms_per_step": e["ms"] / 3, "launches_per_step": e["launches"] / 3, "kernel": e["kernel"]}
+              for lab, e in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])}
     return {"value": whole_job_rate(ms, ws), "unit": "matvec/s", "ms_per_step": ms,
             "dtype": "c64 (3xTF32 translations on %s)" % gemm,
             "relerr_vs_fp64_direct": relerr, "setup_s": setup_s, "roofline": roof,
-            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))}}
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "passes": passes}
 
 
 def instance_mix(Ks, seed0):

@@ -351,33 +351,6 @@ void Session::add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>&
 }
 
 namespace {
-// f(i) for i in [0, n) on the host's cores (DDFMM_HOST_THREADS when set, as for
-// the tree's lists); the first exception is rethrown after every thread joined.
-template <class F>
-void host_parallel_for(size_t n, F f) {
-    const char* e = std::getenv("DDFMM_HOST_THREADS");
-    const int v = e ? std::atoi(e) : 0;
-    const size_t hw = v > 0 ? (size_t)v : std::max(1u, std::thread::hardware_concurrency());
-    const size_t nt = std::min<size_t>(std::min<size_t>(hw, 64), n);
-    if (nt <= 1) {
-        for (size_t i = 0; i < n; ++i) f(i);
-        return;
-    }
-    std::vector<std::exception_ptr> err(nt);
-    std::vector<std::thread> th;
-    for (size_t t = 0; t < nt; ++t)
-        th.emplace_back([&, t] {
-            try {
-                for (size_t i = t; i < n; i += nt) f(i);
-            } catch (...) {
-                err[t] = std::current_exception();
-            }
-        });
-    for (auto& x : th) x.join();
-    for (auto& x : err)
-        if (x) std::rethrow_exception(x);
-}
-
 // Setup-time matrix products C = A * B for many small operators in one
 // launch: each product is one grouped-GEMM problem whose "columns" are the
 // columns of B (read from pool X) and of C (written to pool Y).
@@ -663,14 +636,6 @@ void Session::build() {
 
     phase("lf_operators");
     // ---------------------------------------------------------------- HF nodes
-    struct Node {
-        int box;
-        Idx3 dir;
-        int canon;           // index into hfcanon
-        long long off;       // upeq (up) / dnchk (down) offset
-        long long toff;      // temp offset within the level
-        int did;             // dense id of (width, wedge)
-    };
     struct Canon {
         double W;
         Idx3 srt;
@@ -750,9 +715,12 @@ void Session::build() {
         if (T.boxes[b].has_pts() && T.width(T.boxes[b].level) > 1 - eps) hflevels[T.boxes[b].level].push_back(b);
 
     // nodes of a box are contiguous and in its (sorted) wedge order, so a
-    // (box, wedge) node is found by binary search in the box's range
-    std::vector<Node> up, dn;
-    std::vector<int> up_first(nb, 0), up_cnt(nb, 0), dn_first(nb, 0), dn_cnt(nb, 0);
+    // (box, wedge) node is found by binary search in the box's range (HfNodes::find)
+    HfNodes up, dn;
+    up.first.assign(nb, 0);
+    up.cnt.assign(nb, 0);
+    dn.first.assign(nb, 0);
+    dn.cnt.assign(nb, 0);
     {
         size_t nu = 0, nd = 0;
         for (auto& kv : hflevels)
@@ -760,55 +728,41 @@ void Session::build() {
                 nu += T.boxes[b].outdirs.size();
                 nd += T.boxes[b].incdirs.size();
             }
-        up.reserve(nu);
-        dn.reserve(nd);
+        up.v.reserve(nu);
+        dn.v.reserve(nd);
     }
-    auto find_node = [](const std::vector<Node>& v, int first, int cnt, const Idx3& d) -> int {
-        int lo = first, hi = first + cnt;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (v[mid].dir < d)
-                lo = mid + 1;
-            else
-                hi = mid;
-        }
-        return (lo < first + cnt && v[lo].dir == d) ? lo : -1;
-    };
-    std::map<int, std::pair<int, int> > uprange, dnrange;  // level -> [begin, end)
-    std::map<int, long long> tmp_up_level;                 // level -> temporary elements of its M2M sums
+    std::map<int, long long> tmp_up_level;  // level -> temporary elements of its M2M sums
     long long upeq_total = 0, dnchk_total = 0, tmp_max = 0;
     for (auto& kv : hflevels) {
         double W = T.width(kv.first);
         long long tmp_up = 0, tmp_dn = 0;
-        int u0 = (int)up.size(), d0 = (int)dn.size();
+        int u0 = (int)up.v.size(), d0 = (int)dn.v.size();
         for (int b : kv.second) {
-            up_first[b] = (int)up.size();
-            up_cnt[b] = (int)T.boxes[b].outdirs.size();
+            up.first[b] = (int)up.v.size();
+            up.cnt[b] = (int)T.boxes[b].outdirs.size();
             for (const Idx3& d : T.boxes[b].outdirs) {
                 const DirPts& dp = get_dir(W, d);
-                Node nd{b, d, dp.canon, upeq_total, tmp_up, dp.did};
+                up.v.push_back(HfNode{b, d, dp.canon, upeq_total, tmp_up, dp.did});
                 upeq_total += dp.r1;
                 tmp_up += std::max(dp.r1, dp.r2);
-                up.push_back(nd);
             }
-            dn_first[b] = (int)dn.size();
-            dn_cnt[b] = (int)T.boxes[b].incdirs.size();
+            dn.first[b] = (int)dn.v.size();
+            dn.cnt[b] = (int)T.boxes[b].incdirs.size();
             for (const Idx3& d : T.boxes[b].incdirs) {
                 const DirPts& dp = get_dir(W, d);
-                Node nd{b, d, dp.canon, dnchk_total, tmp_dn, dp.did};
+                dn.v.push_back(HfNode{b, d, dp.canon, dnchk_total, tmp_dn, dp.did});
                 dnchk_total += dp.r1;
                 tmp_dn += std::max(dp.r1, dp.r2);
-                dn.push_back(nd);
             }
         }
-        uprange[kv.first] = std::make_pair(u0, (int)up.size());
+        up.range[kv.first] = std::make_pair(u0, (int)up.v.size());
         tmp_up_level[kv.first] = tmp_up;
-        dnrange[kv.first] = std::make_pair(d0, (int)dn.size());
+        dn.range[kv.first] = std::make_pair(d0, (int)dn.v.size());
         tmp_max = std::max(tmp_max, std::max(tmp_up, tmp_dn));
     }
     phase("hf_nodes");
-    stats_.hf_up_nodes = (long long)up.size();
-    stats_.hf_down_nodes = (long long)dn.size();
+    stats_.hf_up_nodes = (long long)up.v.size();
+    stats_.hf_down_nodes = (long long)dn.v.size();
     double2* hf_upeq = salloc((size_t)upeq_total);
     double2* hf_dnchk = salloc((size_t)dnchk_total);
     double2* T0 = salloc((size_t)tmp_max);
@@ -866,18 +820,18 @@ void Session::build() {
     std::unordered_set<uint64_t> m2m_seen, l2l_seen;  // wedges already in m2m_mats / l2l_mats
     for (auto& kv : hflevels) {
         double W = T.width(kv.first);
-        auto ur = uprange[kv.first], dr = dnrange[kv.first];
+        auto ur = up.range[kv.first], dr = dn.range[kv.first];
         for (int i = ur.first; i < ur.second; ++i) {
-            if (!m2m_seen.insert(wedge_key(W, up[i].dir)).second) continue;
-            auto key = std::make_pair(W, up[i].dir);
-            const DirPts& dp = get_dir(W, up[i].dir);
+            if (!m2m_seen.insert(wedge_key(W, up.v[i].dir)).second) continue;
+            auto key = std::make_pair(W, up.v[i].dir);
+            const DirPts& dp = get_dir(W, up.v[i].dir);
             DirMats M{};
-            child_pts(W, up[i].dir, true, M.mcols, M.ccanon);
+            child_pts(W, up.v[i].dir, true, M.mcols, M.ccanon);
             M.mrows = dp.r2;
             M.canon = dp.canon;
             M.cached = !opctx_.empty();
             for (int ind = 0; ind < 8 && M.cached; ++ind)
-                M.cached = (M.pk[ind] = cached_op(opk("m2m", W, up[i].dir, ind))) != nullptr;
+                M.cached = (M.pk[ind] = cached_op(opk("m2m", W, up.v[i].dir, ind))) != nullptr;
             for (int ind = 0; ind < 8 && !M.cached; ++ind) {
                 size_t n = (size_t)M.mrows * M.mcols;
                 M.raw[ind] = take(scr, n);
@@ -887,16 +841,16 @@ void Session::build() {
             m2m_mats[key] = M;
         }
         for (int i = dr.first; i < dr.second; ++i) {
-            if (!l2l_seen.insert(wedge_key(W, dn[i].dir)).second) continue;
-            auto key = std::make_pair(W, dn[i].dir);
-            const DirPts& dp = get_dir(W, dn[i].dir);
+            if (!l2l_seen.insert(wedge_key(W, dn.v[i].dir)).second) continue;
+            auto key = std::make_pair(W, dn.v[i].dir);
+            const DirPts& dp = get_dir(W, dn.v[i].dir);
             DirMats M{};
-            child_pts(W, dn[i].dir, false, M.mrows, M.ccanon);
+            child_pts(W, dn.v[i].dir, false, M.mrows, M.ccanon);
             M.mcols = dp.r2;
             M.canon = dp.canon;
             M.cached = !opctx_.empty();
             for (int ind = 0; ind < 8 && M.cached; ++ind)
-                M.cached = (M.pk[ind] = cached_op(opk("l2l", W, dn[i].dir, ind))) != nullptr;
+                M.cached = (M.pk[ind] = cached_op(opk("l2l", W, dn.v[i].dir, ind))) != nullptr;
             for (int ind = 0; ind < 8 && !M.cached; ++ind) {
                 size_t n = (size_t)M.mrows * M.mcols;
                 M.raw[ind] = take(scr, n);
@@ -920,70 +874,12 @@ void Session::build() {
     std::map<int, std::vector<std::vector<long long> > > m2l_x, m2l_y;  // level -> per problem columns
     std::map<int, std::vector<int> > m2l_probs;                         // level -> matrix ids
     {
-        // The far pairs of chunks of target nodes (a chunk never spans two levels)
-        // are listed on all host cores, then merged in chunk order, so matrix ids,
-        // problem order and column order are those of one pass in node order.
-        struct Chunk {
-            int level, i0, i1;
-            std::vector<uint64_t> keys;  // (canon, canonical offset), first-seen order
-            std::vector<int> kcanon;
-            std::vector<std::array<int, 3> > koc;
-            std::vector<std::vector<long long> > X, Y;  // per key
-            long long pairs = 0;
-        };
-        std::vector<Chunk> chunks;
-        for (auto& kv : hflevels) {
-            const auto dr = dnrange[kv.first];
-            for (int i0 = dr.first; i0 < dr.second; i0 += 2048) {
-                Chunk c;
-                c.level = kv.first;
-                c.i0 = i0;
-                c.i1 = std::min(dr.second, i0 + 2048);
-                chunks.push_back(std::move(c));
-            }
-        }
-        host_parallel_for(chunks.size(), [&](size_t ci) {
-            Chunk& C = chunks[ci];
-            std::unordered_map<uint64_t, int> loc;
-            for (int i = C.i0; i < C.i1; ++i) {
-                const Node& t = dn[i];
-                const Box& tb = T.boxes[t.box];
-                auto fit = tb.far.find(t.dir);
-                if (fit == tb.far.end()) continue;
-                Idx3 sgn, pv, srt;
-                index3_sort(t.dir, srt, sgn, pv);
-                for (int sb_i : fit->second) {
-                    const int uit = find_node(up, up_first[sb_i], up_cnt[sb_i], t.dir);
-                    if (uit < 0) throw std::runtime_error("M2L source has no outgoing equivalent density");
-                    const Box& sb = T.boxes[sb_i];
-                    int o[3];
-                    std::array<int, 3> oc;
-                    for (int d = 0; d < 3; ++d) o[d] = tb.idx[d] - sb.idx[d];
-                    for (int d = 0; d < 3; ++d) oc[d] = sgn[pv[d]] * o[pv[d]];
-                    const uint64_t key = ((uint64_t)t.canon << 33) | ((uint64_t)(oc[0] + 1024) << 22) |
-                                         ((uint64_t)(oc[1] + 1024) << 11) | (uint64_t)(oc[2] + 1024);
-                    auto it = loc.find(key);
-                    int li;
-                    if (it == loc.end()) {
-                        li = (int)C.keys.size();
-                        loc.emplace(key, li);
-                        C.keys.push_back(key);
-                        C.kcanon.push_back(t.canon);
-                        C.koc.push_back(oc);
-                        C.X.emplace_back();
-                        C.Y.emplace_back();
-                    } else {
-                        li = it->second;
-                    }
-                    C.X[li].push_back(up[uit].off);
-                    C.Y[li].push_back(t.off);
-                    C.pairs++;
-                }
-            }
-        });
+        // far pairs listed on all host cores (plan.cpp), merged here in chunk order:
+        // matrix ids, problem order and column order as one pass in node order
+        std::vector<M2LChunk> chunks = m2l_pairs(T, up, dn);
         std::vector<int> local;  // matrix id -> problem index within its level (-1: none yet)
         int cur_level = INT_MIN;
-        for (Chunk& C : chunks) {
+        for (M2LChunk& C : chunks) {
             if (C.level != cur_level) {
                 cur_level = C.level;
                 local.assign(m2l_mats.size(), -1);
@@ -1191,90 +1087,19 @@ void Session::build() {
                 const int c = T.child(b, ind);
                 if (c >= 0 && T.boxes[c].has_pts()) kids[(size_t)b * 8 + ind] = c;
             }
-    // The column lists of every high-frequency level's M2M, E2, E2^T and L2L
-    // launches, built on all host cores (one job per level and pass): each
-    // holds its problems in first-seen order -- keyed by (wedge, child) or by
-    // canonical wedge -- and their input / output columns in node order, as
-    // one sequential pass over the nodes would list them.
-    struct ColLists {
-        std::vector<int> key;
-        std::vector<std::vector<long long> > x, y;
-        void add(std::vector<int>& tab, int k, long long xv, long long yv) {
-            int p = tab[k];
-            if (p < 0) {
-                p = tab[k] = (int)key.size();
-                key.push_back(k);
-                x.emplace_back();
-                y.emplace_back();
-            }
-            x[p].push_back(xv);
-            y[p].push_back(yv);
-        }
-    };
+    // the column lists of every level's M2M, E2, E2^T and L2L launches, built on
+    // all host cores (plan.cpp)
     std::vector<std::pair<double, Idx3> > did_wedge(dirpts.size());
     for (auto& kv : dirpts) did_wedge[kv.second.did] = kv.first;
-    std::map<int, ColLists> cl_m2m, cl_e2, cl_e2t, cl_l2l;
-    {
-        std::vector<std::pair<int, int> > jobs;  // (level, pass)
-        for (auto& kv : hflevels)
-            for (int pass = 0; pass < 4; ++pass) {
-                jobs.push_back(std::make_pair(kv.first, pass));
-                (pass == 0 ? cl_m2m : pass == 1 ? cl_e2 : pass == 2 ? cl_e2t : cl_l2l)[kv.first];
-            }
-        host_parallel_for(jobs.size(), [&](size_t j) {
-            const int level = jobs[j].first, pass = jobs[j].second;
-            const double W = T.width(level);
-            if (pass == 0 || pass == 3) {
-                const bool upward = pass == 0;
-                const auto r = upward ? uprange[level] : dnrange[level];
-                const std::vector<Node>& nodes = upward ? up : dn;
-                const std::vector<int>& first = upward ? up_first : dn_first;
-                const std::vector<int>& cnt = upward ? up_cnt : dn_cnt;
-                ColLists& L = (upward ? cl_m2m : cl_l2l).at(level);
-                std::vector<int> tab(dirpts.size() * 8, -1);
-                for (int ind = 0; ind < 8; ++ind)
-                    for (int i = r.first; i < r.second; ++i) {
-                        const Node& u = nodes[i];
-                        const int c = kids[(size_t)u.box * 8 + ind];
-                        if (c < 0) continue;
-                        long long coff;
-                        if (W == 1.0) {
-                            coff = (long long)lfidx[c] * nE;
-                        } else {
-                            const int ci = find_node(nodes, first[c], cnt[c], predir(u.dir));
-                            if (ci < 0)
-                                throw std::runtime_error(upward ? "child has no directional equivalent density"
-                                                                : "child has no directional check value");
-                            coff = nodes[ci].off;
-                        }
-                        // M2M: child w -> parent sum; L2L: parent t -> child u
-                        if (upward)
-                            L.add(tab, u.did * 8 + ind, coff, u.toff);
-                        else
-                            L.add(tab, u.did * 8 + ind, u.toff, coff);
-                    }
-            } else {
-                const bool upward = pass == 1;
-                const auto r = upward ? uprange[level] : dnrange[level];
-                const std::vector<Node>& nodes = upward ? up : dn;
-                ColLists& L = (upward ? cl_e2 : cl_e2t).at(level);
-                std::vector<int> tab(hfcanon.size(), -1);
-                for (int i = r.first; i < r.second; ++i) {
-                    const Node& u = nodes[i];
-                    if (upward)
-                        L.add(tab, u.canon, u.toff, u.off);
-                    else
-                        L.add(tab, u.canon, u.off, u.toff);
-                }
-            }
-        });
-    }
+    std::vector<long long> lf_off(nb, -1);
+    for (int l = 0; l < nLF; ++l) lf_off[lfbox[l]] = (long long)l * nE;
+    HfColumns cols = hf_columns(T, up, dn, kids, lf_off, dirpts.size(), hfcanon.size());
     // ---------------------------------------------------------------- steps: HF upward
     // widths ascending = levels descending; hf_upeq holds w (upeqnden = E1 w)
     for (auto hit = hflevels.rbegin(); hit != hflevels.rend(); ++hit) {
         int level = hit->first;
         double W = T.width(level);
-        auto ur = uprange[level];
+        auto ur = up.range[level];
         if (ur.first == ur.second) continue;
         begin_block(1, W);
         Step ms{};
@@ -1286,7 +1111,7 @@ void Session::build() {
         // one launch for the 8 child positions: a problem per (wedge, child), all adding into
         // the parents' sums
         {
-            ColLists& L = cl_m2m.at(level);
+            ColLists& L = cols.m2m.at(level);
             std::vector<GemmProblem> probs;
             for (int k : L.key) {
                 const Idx3& dir = did_wedge[k / 8].second;
@@ -1303,7 +1128,7 @@ void Session::build() {
         }
         // w = E2 * (E3 upchkval)   (src/wave3d_eval.cpp:837-849)
         {
-            ColLists& L = cl_e2.at(level);
+            ColLists& L = cols.e2.at(level);
             std::vector<GemmProblem> p2;
             for (int k : L.key) {
                 const Canon& c = hfcanon[k];
@@ -1326,7 +1151,7 @@ void Session::build() {
     for (auto it = hflevels.begin(); it != hflevels.end(); ++it) {
         int level = it->first;
         double W = T.width(level);
-        auto dr = dnrange[level];
+        auto dr = dn.range[level];
         if (dr.first == dr.second) continue;
         begin_block(2, W);
         // M2L (src/wave3d_eval.cpp:876-928)
@@ -1345,7 +1170,7 @@ void Session::build() {
         }
         // t = E2^T u   (dneqnden = E3^T t, src/wave3d_eval.cpp:938-948, src/mlib3d.cpp:246-250)
         {
-            ColLists& L = cl_e2t.at(level);
+            ColLists& L = cols.e2t.at(level);
             std::vector<GemmProblem> p2;
             for (int k : L.key) {
                 const Canon& c = hfcanon[k];
@@ -1363,7 +1188,7 @@ void Session::build() {
         // L2L into the children's (pdir) u, or LF dnchkval at W=1 (src/wave3d_eval.cpp:950-991),
         // one launch for the 8 child positions: a problem per (wedge, child)
         {
-            ColLists& L = cl_l2l.at(level);
+            ColLists& L = cols.l2l.at(level);
             std::vector<GemmProblem> probs;
             for (int k : L.key) {
                 const Idx3& dir = did_wedge[k / 8].second;
@@ -1673,15 +1498,22 @@ void Session::autotune() {
                                              PT_WARP_SOURCES4};
         float best = 0.f;
         int best_tpi = shapes[0];
-        for (int tpi : shapes) {
-            st.tpi = tpi;
-            launch_step(st, stream_, st.v.spec);  // warm-up
+        // per-launch time of one shape over `reps` launches after a warm-up
+        auto time_shape = [&](int reps) {
+            launch_step(st, stream_, st.v.spec);
             CK(cudaEventRecord(a, stream_));
-            for (int r = 0; r < 3; ++r) launch_step(st, stream_, st.v.spec);
+            for (int r = 0; r < reps; ++r) launch_step(st, stream_, st.v.spec);
             CK(cudaEventRecord(b, stream_));
             CK(cudaEventSynchronize(b));
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, a, b));
+            return ms / reps;
+        };
+        for (int tpi : shapes) {
+            st.tpi = tpi;
+            float ms = time_shape(3);
+            // short steps: time over ~0.5 ms of launches, or three launches read mostly noise
+            if (ms * 3 < 0.5f) ms = time_shape(std::min(50, (int)(0.5f / std::max(ms, 1e-3f)) + 1));
             if (tpi == shapes[0] || ms < best) {
                 best = ms;
                 best_tpi = tpi;

@@ -1,13 +1,20 @@
-// Host-only check of the V-list sum groups (ddfmm_b200/csrc/plan.hpp) on a
-// tree built from points read from a file: every (target, source) pair of
-// every target's V list (src/wave3d_setup.cpp:302-390 builds those lists) is
-// covered exactly once, by an entry whose tensor index is the pair's offset
-// index, and nothing else is covered.
+// Host-only checks of the launch plan's pieces (ddfmm_b200/csrc/plan.hpp) on a
+// tree built from points read from a file:
+//  * V-list sum groups: every (target, source) pair of every target's V list
+//    (src/wave3d_setup.cpp:302-390 builds those lists) is covered exactly
+//    once, by an entry whose tensor index is the pair's offset index;
+//  * M2L far pairs: every (incoming node, far source box) pair of every level
+//    (src/wave3d_setup.cpp:393-443) appears once, with the source's outgoing
+//    node and the canonical offset of the pair;
+//  * M2M / E2 / E2^T / L2L column lists: every (node, child position with a
+//    child) pair and every node appears once, in the problem of its wedge and
+//    child position or of its canonical wedge, with the right columns.
 //   plan_test <points.bin (3n doubles)> <n> <K> <ncell> <maxlevel> <ptsmax>
 #include <cstdio>
 #include <cstdlib>
 #include <map>
 #include <set>
+#include <tuple>
 #include <vector>
 
 #include "plan.hpp"
@@ -79,6 +86,126 @@ int main(int argc, char** argv) {
         if (rows.size() != g.trg.size()) { std::printf("rows\n"); return 1; }
         pairs += g.pairs;
     }
-    std::printf("ok pairs %lld groups %lld\n", pairs, groups);
+    // ---------------------------------------------------------------- high frequency
+    std::map<std::pair<double, Idx3>, int> dids, canons;
+    auto did_of = [&](double W, const Idx3& d) { return dids.emplace(std::make_pair(W, d), (int)dids.size()).first->second; };
+    auto canon_of = [&](double W, const Idx3& d) {
+        Idx3 srt, sgn, prm;
+        index3_sort(d, srt, sgn, prm);
+        return canons.emplace(std::make_pair(W, srt), (int)canons.size()).first->second;
+    };
+    HfNodes up, dn;
+    up.first.assign(T.boxes.size(), 0);
+    up.cnt.assign(T.boxes.size(), 0);
+    dn.first.assign(T.boxes.size(), 0);
+    dn.cnt.assign(T.boxes.size(), 0);
+    std::map<int, std::vector<int> > hf;
+    for (int b : T.order)
+        if (T.boxes[b].has_pts() && T.width(T.boxes[b].level) > 1 - 1e-12) hf[T.boxes[b].level].push_back(b);
+    long long off = 0;
+    for (auto& kv : hf) {
+        const double W = T.width(kv.first);
+        const int u0 = (int)up.v.size(), d0 = (int)dn.v.size();
+        for (int b : kv.second) {
+            up.first[b] = (int)up.v.size();
+            up.cnt[b] = (int)T.boxes[b].outdirs.size();
+            for (const Idx3& d : T.boxes[b].outdirs) {
+                up.v.push_back(HfNode{b, d, canon_of(W, d), off, off + 1, did_of(W, d)});
+                off += 10;
+            }
+            dn.first[b] = (int)dn.v.size();
+            dn.cnt[b] = (int)T.boxes[b].incdirs.size();
+            for (const Idx3& d : T.boxes[b].incdirs) {
+                dn.v.push_back(HfNode{b, d, canon_of(W, d), off, off + 1, did_of(W, d)});
+                off += 10;
+            }
+        }
+        up.range[kv.first] = std::make_pair(u0, (int)up.v.size());
+        dn.range[kv.first] = std::make_pair(d0, (int)dn.v.size());
+    }
+    // M2L pairs
+    long long far = 0;
+    std::set<std::pair<long long, long long> > seen;  // (target off, source off)
+    for (const M2LChunk& C : m2l_pairs(T, up, dn, 97)) {
+        for (size_t k = 0; k < C.keys.size(); ++k)
+            for (size_t q = 0; q < C.X[k].size(); ++q) {
+                if (!seen.insert(std::make_pair(C.Y[k][q], C.X[k][q])).second) { std::printf("far pair twice\n"); return 1; }
+            }
+        far += C.pairs;
+    }
+    long long want_far = 0;
+    std::map<long long, int> dn_by_off, up_by_off;
+    for (size_t i = 0; i < dn.v.size(); ++i) dn_by_off[dn.v[i].off] = (int)i;
+    for (size_t i = 0; i < up.v.size(); ++i) up_by_off[up.v[i].off] = (int)i;
+    for (const HfNode& t : dn.v) {
+        auto fit = T.boxes[t.box].far.find(t.dir);
+        if (fit == T.boxes[t.box].far.end()) continue;
+        for (int sb : fit->second) {
+            want_far++;
+            const int ui = up.find(sb, t.dir);
+            if (ui < 0 || !seen.count(std::make_pair(t.off, up.v[ui].off))) { std::printf("far pair missing\n"); return 1; }
+        }
+    }
+    if (far != want_far || (long long)seen.size() != want_far) { std::printf("far pair count\n"); return 1; }
+    // canonical offsets: recomputed for every listed pair
+    for (const M2LChunk& C : m2l_pairs(T, up, dn))
+        for (size_t k = 0; k < C.keys.size(); ++k)
+            for (size_t q = 0; q < C.X[k].size(); ++q) {
+                const HfNode& t = dn.v[dn_by_off.at(C.Y[k][q])];
+                const HfNode& s = up.v[up_by_off.at(C.X[k][q])];
+                Idx3 srt, sgn, prm;
+                index3_sort(t.dir, srt, sgn, prm);
+                int oc[3];
+                for (int d = 0; d < 3; ++d) oc[d] = sgn[prm[d]] * (T.boxes[t.box].idx[prm[d]] - T.boxes[s.box].idx[prm[d]]);
+                if (C.kcanon[k] != t.canon || oc[0] != C.koc[k][0] || oc[1] != C.koc[k][1] || oc[2] != C.koc[k][2]) {
+                    std::printf("canonical offset\n");
+                    return 1;
+                }
+            }
+    // column lists
+    std::vector<int> kids(T.boxes.size() * 8, -1);
+    for (auto& kv : hf)
+        for (int b : kv.second)
+            for (int ind = 0; ind < 8; ++ind) {
+                const int c = T.child(b, ind);
+                if (c >= 0 && T.boxes[c].has_pts()) kids[(size_t)b * 8 + ind] = c;
+            }
+    std::vector<long long> lf_off(T.boxes.size(), -1);
+    for (int l = 0; l < (int)lfbox.size(); ++l) lf_off[lfbox[l]] = 1000000000LL + l;
+    const HfColumns cols = hf_columns(T, up, dn, kids, lf_off, dids.size(), canons.size());
+    long long ncols = 0;
+    for (auto& kv : hf) {
+        const int level = kv.first;
+        const bool lfc = T.width(level) == 1.0;
+        for (int pass = 0; pass < 4; ++pass) {
+            const bool upward = pass < 2;
+            const HfNodes& N = upward ? up : dn;
+            const ColLists& L = (pass == 0 ? cols.m2m : pass == 1 ? cols.e2 : pass == 2 ? cols.e2t : cols.l2l).at(level);
+            std::set<std::tuple<int, long long, long long> > got2, want2;  // (key, x, y)
+            for (size_t k = 0; k < L.key.size(); ++k)
+                for (size_t q = 0; q < L.x[k].size(); ++q)
+                    if (!got2.insert(std::make_tuple(L.key[k], L.x[k][q], L.y[k][q])).second) {
+                        std::printf("column twice\n");
+                        return 1;
+                    }
+            const auto r = N.range.at(level);
+            for (int i = r.first; i < r.second; ++i) {
+                const HfNode& u = N.v[i];
+                if (pass == 1) want2.insert(std::make_tuple(u.canon, u.toff, u.off));
+                if (pass == 2) want2.insert(std::make_tuple(u.canon, u.off, u.toff));
+                if (pass == 0 || pass == 3)
+                    for (int ind = 0; ind < 8; ++ind) {
+                        const int c = kids[(size_t)u.box * 8 + ind];
+                        if (c < 0) continue;
+                        const long long co = lfc ? lf_off[c] : N.v[N.find(c, predir(u.dir))].off;
+                        if (pass == 0) want2.insert(std::make_tuple(u.did * 8 + ind, co, u.toff));
+                        else want2.insert(std::make_tuple(u.did * 8 + ind, u.toff, co));
+                    }
+            }
+            if (got2 != want2) { std::printf("columns differ (level %d pass %d)\n", level, pass); return 1; }
+            ncols += (long long)got2.size();
+        }
+    }
+    std::printf("ok pairs %lld groups %lld far %lld columns %lld\n", pairs, groups, far, ncols);
     return 0;
 }

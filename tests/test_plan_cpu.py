@@ -1,5 +1,6 @@
-"""Host-only pieces of the launch plan (ddfmm_b200/csrc/plan.hpp), checked
-without a GPU by a C++ driver linked against the library."""
+"""Host-only pieces of the launch plan (ddfmm_b200/csrc/plan.hpp: V-list sum
+groups, M2L far pairs, M2M / E2 / E2^T / L2L column lists), checked without a
+GPU by a C++ driver linked against the library."""
 import os
 import subprocess
 
@@ -22,7 +23,7 @@ def plan_test(tmp_path_factory):
 
 @pytest.mark.parametrize("geom,K,N,ptsmax", [("sphere", 8.0, 5027, 100), ("sphere", 16.0, 20106, 100),
                                              ("ellipsoid", 8.0, 3000, 100), ("cluster", 4.0, 1500, 8)])
-def test_vlist_groups_cover_every_pair_once(plan_test, tmp_path, geom, K, N, ptsmax):
+def test_plan_pieces_cover_every_pair_once(plan_test, tmp_path, geom, K, N, ptsmax):
     pos = {"sphere": geometry.sphere_points, "ellipsoid": geometry.ellipsoid_points,
            "cluster": geometry.cluster_points}[geom](N, K)
     path = tmp_path / "pos.bin"
@@ -32,3 +33,5 @@ def test_vlist_groups_cover_every_pair_once(plan_test, tmp_path, geom, K, N, pts
     assert r.returncode == 0, r.stdout + r.stderr
     words = r.stdout.split()
     assert words[0] == "ok" and int(words[2]) > 0, r.stdout
+    if K >= 8:  # trees with high-frequency levels
+        assert int(words[6]) > 0 and int(words[8]) > 0, r.stdout
