@@ -698,7 +698,8 @@ def run_ours(args):
     # roofline of the dominant kernel -------------------------------------------
     by_kernel = {}
     for lab, e in prof.items():
-        k = by_kernel.setdefault(e["kernel"], dict(ms=0.0, launches=0, flops=0.0, bytes=0.0))
+        # one kernel, whatever launch shape the autotuner chose for the pass
+        k = by_kernel.setdefault(e["kernel"].split("<")[0], dict(ms=0.0, launches=0, flops=0.0, bytes=0.0))
         for f in ("ms", "launches", "flops", "bytes"):
             k[f] += e[f]
     dom = max(by_kernel, key=lambda k: by_kernel[k]["ms"])
