@@ -87,15 +87,10 @@ void launch_kmat(const KmatJob* jobs, int njobs, long long total, int kernel, cu
 #ifndef DDFMM_ZGEMM_MINB
 #define DDFMM_ZGEMM_MINB 2
 #endif
-constexpr int BN = 64, BK = DDFMM_ZGEMM_BK, BKP = BK + 4, GSTAGES = DDFMM_ZGEMM_STAGES;
+constexpr int BM = 64, BN = 64, BK = DDFMM_ZGEMM_BK, BKP = BK + 4, GSTAGES = DDFMM_ZGEMM_STAGES;
 static_assert(BK == 16 || BK == 32, "K slice of 16 or 32");
-// tile rows BM = 16 SL (SL 16-row slabs, two warps each); SL = 4 (64 rows, two
-// blocks per SM) or 8 (128 rows, one block per SM: an operator of 65-128 rows
-// gathers its columns once instead of twice)
-template <int SL>
-__host__ __device__ constexpr int gstage() { return BK * 16 * SL + BN * BKP; }  // double2 per stage
-template <int SL>
-__host__ __device__ constexpr int gemm_smem() { return GSTAGES * gstage<SL>() * (int)sizeof(double2); }
+constexpr int GSTAGE = BK * BM + BN * BKP;  // double2 per stage
+constexpr int GEMM_SMEM = GSTAGES * GSTAGE * (int)sizeof(double2);
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
     unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -114,13 +109,11 @@ __device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[4], con
         : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-template <int SL>
-__global__ void __launch_bounds__(64 * SL, SL == 4 ? DDFMM_ZGEMM_MINB : 1) zgemm_kernel(const GemmProblem* __restrict__ probs,
+__global__ void __launch_bounds__(256, DDFMM_ZGEMM_MINB) zgemm_kernel(const GemmProblem* __restrict__ probs,
                                                        const GemmTile* __restrict__ tiles,
                                                        const long long* __restrict__ xoff,
                                                        const long long* __restrict__ yoff,
                                                        const double2* __restrict__ X, double2* Y, int mode) {
-    constexpr int BM = 16 * SL, NT = 64 * SL, GSTAGE = gstage<SL>();
     extern __shared__ double2 gsm[];
     __shared__ long long xo[BN], yo[BN];
     const GemmTile t = tiles[blockIdx.x];
@@ -139,7 +132,7 @@ __global__ void __launch_bounds__(64 * SL, SL == 4 ? DDFMM_ZGEMM_MINB : 1) zgemm
     auto load = [&](int stage, int k0) {
         double2* As = gsm + stage * GSTAGE;
         double2* Xs = As + BK * BM;
-        for (int e = tid; e < BK * nrow; e += NT) {
+        for (int e = tid; e < BK * nrow; e += 256) {
             int kk = e / nrow, row = e - kk * nrow;
             int gk = k0 + kk;
             bool ok = row < rows && gk < p.k;
@@ -147,8 +140,8 @@ __global__ void __launch_bounds__(64 * SL, SL == 4 ? DDFMM_ZGEMM_MINB : 1) zgemm
                        ok ? (const void*)(p.A + (size_t)gk * p.lda + t.row0 + row) : (const void*)p.A, ok ? 16 : 0);
         }
 #pragma unroll
-        for (int q = 0; q < BN * BK / NT; ++q) {
-            int e = tid + NT * q, kk = e % BK, col = e / BK;
+        for (int q = 0; q < BN * BK / 256; ++q) {
+            int e = tid + 256 * q, kk = e % BK, col = e / BK;
             int gk = k0 + kk;
             bool ok = col < ncol && gk < p.k;
             cp_async16(&Xs[col * BKP + kk], ok ? (const void*)(X + xo[col] + gk) : (const void*)X, ok ? 16 : 0);
@@ -244,17 +237,13 @@ __global__ void __launch_bounds__(64 * SL, SL == 4 ? DDFMM_ZGEMM_MINB : 1) zgemm
 }
 
 void gemm_init() {
-    cudaFuncSetAttribute(zgemm_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem<4>());
-    cudaFuncSetAttribute(zgemm_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem<8>());
+    cudaFuncSetAttribute(zgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
 }
 
 void launch_gemm(const GemmProblem* probs, const GemmTile* tiles, int ntiles, const long long* xoff,
-                 const long long* yoff, const double2* X, double2* Y, int mode, cudaStream_t s, int tile_rows) {
+                 const long long* yoff, const double2* X, double2* Y, int mode, cudaStream_t s) {
     if (ntiles == 0) return;
-    if (tile_rows == 128)
-        zgemm_kernel<8><<<ntiles, 512, gemm_smem<8>(), s>>>(probs, tiles, xoff, yoff, X, Y, mode);
-    else
-        zgemm_kernel<4><<<ntiles, 256, gemm_smem<4>(), s>>>(probs, tiles, xoff, yoff, X, Y, mode);
+    zgemm_kernel<<<ntiles, 256, GEMM_SMEM, s>>>(probs, tiles, xoff, yoff, X, Y, mode);
 }
 
 // ---------------------------------------------------------------- points

@@ -59,10 +59,9 @@ struct PtSrc {
 };
 
 void launch_kmat(const KmatJob* jobs_dev, int njobs, long long total, int kernel, cudaStream_t s);
-// tile_rows: 64 (tiles listed in 64-row steps) or 128 (128-row steps)
 void launch_gemm(const GemmProblem* probs_dev, const GemmTile* tiles_dev, int ntiles,
                  const long long* xoff, const long long* yoff, const double2* X, double2* Y, int mode,
-                 cudaStream_t s, int tile_rows = 64);
+                 cudaStream_t s);
 // tpi: the launch shape, chosen per step by the session's autotuner: 4, 8, 16 or
 // 32 threads per item, each thread taking targets and walking the sources in
 // global memory; or one warp per item with the item's sources staged in

@@ -185,20 +185,6 @@ void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<
     st.g.xoff = upload(xs);
     st.g.yoff = upload(ys);
     st.g.ntiles = (int)tiles.size();
-    if (!mixed()) {
-        // the same tiles in 128-row steps, for the autotuner to weigh against 64
-        std::vector<GemmTile> t128;
-        bool taller = false;
-        for (size_t i = 0; i < P.size(); ++i) {
-            taller |= P[i].m > GEMM_TILE_M;
-            for (int r0 = 0; r0 < P[i].m; r0 += 128)
-                for (int c0 = 0; c0 < P[i].ncol; c0 += GEMM_TILE_N) t128.push_back(GemmTile{(int)i, r0, c0, 0});
-        }
-        if (taller) {
-            st.g.tiles128 = upload(t128);
-            st.g.ntiles128 = (int)t128.size();
-        }
-    }
     st.g.X = X;
     st.g.Y = Y;
     st.g.mode = mode;
@@ -1431,7 +1417,7 @@ void Session::build() {
 
 static const char* kernel_name(int kind, int tpi) {
     switch (kind) {
-        case 0: return tpi == 128 ? "zgemm_kernel<128>" : "zgemm_kernel";
+        case 0: return "zgemm_kernel";
         case 1:
             switch (tpi) {  // the launch shape the autotuner chose
                 case 4: return "pt_kernel<4>";
@@ -1457,9 +1443,6 @@ void Session::launch_step(const Step& st, cudaStream_t s, double2* spec) {
         case 0:
             if (m)
                 launch_cgemm(st.g.probs, st.g.tiles, st.g.ntiles, st.g.xoff, st.g.yoff, st.g.X, st.g.Y, st.g.mode, s);
-            else if (st.tpi == 128)
-                launch_gemm(st.g.probs, st.g.tiles128, st.g.ntiles128, st.g.xoff, st.g.yoff, st.g.X, st.g.Y, st.g.mode, s,
-                            128);
             else
                 launch_gemm(st.g.probs, st.g.tiles, st.g.ntiles, st.g.xoff, st.g.yoff, st.g.X, st.g.Y, st.g.mode, s);
             break;
@@ -1510,12 +1493,9 @@ void Session::autotune() {
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
     for (Step& st : steps_) {
-        const bool gemm = st.kind == 0 && st.g.ntiles128 > 0;  // plain-form GEMM with operators over 64 rows
-        if (st.kind != 1 && !gemm) continue;
-        static const std::vector<int> pt_shapes{32, 16, 8, 4, PT_WARP_TARGETS, PT_WARP_TARGETS2, PT_WARP_SOURCES,
-                                                PT_WARP_SOURCES4};
-        static const std::vector<int> gemm_shapes{0, 128};
-        const std::vector<int>& shapes = gemm ? gemm_shapes : pt_shapes;
+        if (st.kind != 1) continue;
+        static const std::vector<int> shapes{32, 16, 8, 4, PT_WARP_TARGETS, PT_WARP_TARGETS2, PT_WARP_SOURCES,
+                                             PT_WARP_SOURCES4};
         float best = 0.f;
         int best_tpi = shapes[0];
         // per-launch time of one shape over `reps` launches after a warm-up
@@ -1531,7 +1511,7 @@ void Session::autotune() {
         };
         for (int tpi : shapes) {
             st.tpi = tpi;
-            float ms = time_shape(gemm ? 1 : 3);
+            float ms = time_shape(3);
             // short steps: time over ~0.5 ms of launches, or three launches read mostly noise
             if (ms * 3 < 0.5f) ms = time_shape(std::min(50, (int)(0.5f / std::max(ms, 1e-3f)) + 1));
             if (tpi == shapes[0] || ms < best) {

@@ -93,11 +93,10 @@ public:
 private:
     struct GemmLaunch {
         GemmProblem* probs = nullptr;
-        GemmTile* tiles = nullptr;    // 64-row tiles
-        GemmTile* tiles128 = nullptr;  // 128-row tiles (plain form, when an operator has more than 64 rows)
+        GemmTile* tiles = nullptr;
         long long* xoff = nullptr;
         long long* yoff = nullptr;
-        int ntiles = 0, ntiles128 = 0;
+        int ntiles = 0;
         const double2* X = nullptr;
         double2* Y = nullptr;
         int mode = 0;
@@ -137,9 +136,7 @@ private:
         // that play the same part (phase, width, step type, occurrence): a Batch
         // merges the steps of its sessions that share a key into one launch.
         long long key;
-        // launch shape, set by autotune(): point interactions: threads per item
-        // (launch_pt; 0 = 32); plain-form GEMMs: tile rows (0 = 64, or 128)
-        int tpi;
+        int tpi;  // point interactions: launch shape (launch_pt; 0 = 32 threads per item), set by autotune()
         // mixed form: the step as a one-instance launch (device sub-launch array and
         // prefix sums) and the host copy of its sub-launch
         void* msubs;
