@@ -89,13 +89,39 @@ Batch::Batch(const std::vector<Session*>& sessions) : sessions_(sessions) {
             if (kind == 5) {
                 std::vector<UmmaSub> subs;
                 std::vector<int> n;
+                long long tiles = 0;
                 for (auto& e : kk.second) {
                     UmmaSub u = e.second->hu;
                     u.inst = e.first;
                     subs.push_back(u);
                     n.push_back(u.ntiles);
+                    tiles += u.ntiles;
                 }
                 add(GEMM, subs, n);
+                // Instances share packed operators (the process-wide cache): tiles that
+                // read one operator block run next to each other across instances, so
+                // the block comes from DRAM once while the blocks in flight share it in
+                // L2, instead of once per instance.  Within an operator, instance order
+                // and each instance's tile order are kept.
+                if (subs.size() > 1 && tiles > 0 && subs.size() < 256) {  // add() appended this launch
+                    std::vector<std::pair<const float*, int> > key;
+                    bool fits = true;
+                    for (size_t j = 0; j < kk.second.size(); ++j) {
+                        const std::vector<const float*>& op = kk.second[j].second->uop;
+                        if ((int)op.size() != n[j] || op.size() >= (1u << 24)) fits = false;
+                        for (size_t t = 0; fits && t < op.size(); ++t)
+                            key.push_back(std::make_pair(op[t], (int)((j << 24) | t)));
+                    }
+                    if (fits) {
+                        std::stable_sort(key.begin(), key.end(),
+                                         [](const std::pair<const float*, int>& a, const std::pair<const float*, int>& b) {
+                                             return a.first < b.first;
+                                         });
+                        std::vector<int> order(key.size());
+                        for (size_t i = 0; i < key.size(); ++i) order[i] = key[i].second;
+                        launches_.back().order = upload_bytes(order.data(), sizeof(int) * order.size());
+                    }
+                }
             } else if (kind == 1) {
                 std::vector<PtSub> subs;
                 std::vector<int> n;
@@ -208,7 +234,8 @@ void Batch::run(const int* active, cudaStream_t s) {
             case GEMM:
                 launch_umma_cgemm(static_cast<const UmmaSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub,
                                   (int)L.total, active, d_err_, s,
-                                  L.nsub == 1 ? reinterpret_cast<const UmmaSub*>(L.one) : nullptr);
+                                  L.nsub == 1 ? reinterpret_cast<const UmmaSub*>(L.one) : nullptr, 0, 0,
+                                  static_cast<const int*>(L.order));
                 break;
             case PT:
                 launch_pt32(static_cast<const PtSub*>(L.subs), static_cast<const int*>(L.prefix), L.nsub, (int)L.total,

@@ -52,6 +52,7 @@ private:
         long long total;
         int G;
         int tpi = 32;  // point interactions: threads per item
+        void* order = nullptr;  // tcgen05 GEMM: tiles by operator across the sub-launches (launch_umma_cgemm)
         alignas(16) unsigned char one[256];  // host copy of the first sub-launch
     };
     template <class Sub, class Pre>

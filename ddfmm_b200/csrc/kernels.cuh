@@ -235,9 +235,12 @@ void launch_umma_pack(const UmmaPackJob* jobs_dev, int njobs, cudaStream_t s);
 // nsub == 1: `one` is that sub-launch (host copy, sent as a kernel parameter).
 // wait_ns bounds every pipeline wait (0: 1 s); withhold != 0 is the failure-path
 // test hook: block 0 issues no operator copies, so its first wait runs out, the
-// block drains, frees its tensor memory and sets *err.
+// block drains, frees its tensor memory and sets *err.  order (nsub > 1,
+// optional): the launch's tiles in the order the blocks take them, entry
+// j << 24 | t for tile t of sub-launch j (j < 256, t < 2^24).
 void launch_umma_cgemm(const UmmaSub* subs, const int* prefix, int nsub, int ntiles, const int* active, int* err,
-                       cudaStream_t s, const UmmaSub* one, unsigned long long wait_ns = 0, int withhold = 0);
+                       cudaStream_t s, const UmmaSub* one, unsigned long long wait_ns = 0, int withhold = 0,
+                       const int* order = nullptr);
 
 // gather/scatter helpers
 void launch_gather_den(const double2* den, const int* perm, double2* out, int n, cudaStream_t s);

@@ -341,8 +341,9 @@ __device__ __forceinline__ void store_chunk(const float2* park, float2* Y, long 
     }
 }
 
-// Tile ti of a launch: its sub-launch (prefix[j] <= ti < prefix[j+1]), tile and
-// problem; `on` is false when the sub-launch's instance is inactive.
+// Tile ti of a launch: its sub-launch (prefix[j] <= ti < prefix[j+1], or
+// order[ti] = j << 24 | tile of sub-launch j where the launch gives an order),
+// tile and problem; `on` is false when the sub-launch's instance is inactive.
 struct TileInfo {
     UmmaTile t;
     UmmaProblem p;
@@ -358,22 +359,29 @@ struct TileInfo {
 // most) or the global arrays
 template <bool MULTI>
 __device__ __forceinline__ TileInfo tile_info(const UmmaSub& one, const UmmaSub* subs, const int* prefix, int nsub,
-                                              const int* __restrict__ active, int ti) {
-    int lo = 0;
+                                              const int* __restrict__ order, const int* __restrict__ active, int ti) {
+    int lo = 0, t = ti;
     if (MULTI) {
-        int hi = nsub - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (prefix[mid] <= ti)
-                lo = mid;
-            else
-                hi = mid - 1;
+        if (order) {
+            const unsigned e = (unsigned)__ldg(order + ti);
+            lo = (int)(e >> 24);
+            t = (int)(e & 0xFFFFFFu);
+        } else {
+            int hi = nsub - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (prefix[mid] <= ti)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            t = ti - prefix[lo];
         }
     }
     const UmmaSub& S = MULTI ? subs[lo] : one;
     TileInfo r;
     r.on = !active || active[S.inst];
-    r.t = S.tiles[MULTI ? ti - prefix[lo] : ti];
+    r.t = S.tiles[t];
     r.p = S.probs[r.t.prob];
     r.X = S.X;
     r.Y = S.Y;
@@ -390,9 +398,9 @@ template <bool MULTI>
 __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub one,
                                                                  const UmmaSub* __restrict__ gsubs,
                                                                  const int* __restrict__ gprefix, int nsub,
-                                                                 int ntiles, const int* __restrict__ active,
-                                                                 int* err, unsigned long long wait_ns,
-                                                                 int withhold) {
+                                                                 int ntiles, const int* __restrict__ order,
+                                                                 const int* __restrict__ active, int* err,
+                                                                 unsigned long long wait_ns, int withhold) {
     extern __shared__ __align__(1024) unsigned char usm_raw[];
     __shared__ UmmaSub ssubs[MULTI ? U_SUBS_SMEM : 1];
     __shared__ int sprefix[MULTI ? U_SUBS_SMEM + 1 : 1];
@@ -455,7 +463,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
         const float2* X = nullptr;
         auto load_tile = [&]() {  // the first active tile from ti_i on
             for (; ti_i < ntiles; ti_i += gridDim.x) {
-                const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, active, ti_i);
+                const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, order, active, ti_i);
                 if (!T.on) continue;
                 nkb_i = T.p.nkb;
                 k_i = T.p.k;
@@ -538,7 +546,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
         if (lane == 0 && !(withhold && blockIdx.x == 0)) {
             int g = 0;
             for (int ti = blockIdx.x; ti < ntiles && !*failed; ti += gridDim.x) {
-                const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, active, ti);
+                const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, order, active, ti);
                 if (!T.on) continue;
                 const char* Bt = reinterpret_cast<const char*>(T.p.B + (size_t)T.t.rtile * T.p.tile_stride);
                 const uint32_t blk = (uint32_t)tile_n(T.t.rows) * UBK * 4;
@@ -561,7 +569,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
         if (lane == 0) {
             int g = 0, it = 0, last = -1;
             for (int ti = blockIdx.x; ti < ntiles && !*failed; ti += gridDim.x) {
-                const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, active, ti);
+                const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, order, active, ti);
                 if (!T.on) continue;
                 const uint32_t idesc = idesc_tf32(tile_n(T.t.rows));
                 const int acc = it & 1;
@@ -615,7 +623,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
         };
         int it = 0;
         for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
-            const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, active, ti);
+            const TileInfo T = tile_info<MULTI>(one, subs, prefix, nsub, order, active, ti);
             if (!T.on) continue;
             const int ncol = min(UM, T.p.ncol - T.t.col0);
             const int rows = T.t.rows, N = tile_n(rows);
@@ -692,18 +700,18 @@ void umma_init() {
 }
 
 void launch_umma_cgemm(const UmmaSub* subs, const int* prefix, int nsub, int ntiles, const int* active, int* err,
-                       cudaStream_t s, const UmmaSub* one, unsigned long long wait_ns, int withhold) {
+                       cudaStream_t s, const UmmaSub* one, unsigned long long wait_ns, int withhold, const int* order) {
     if (ntiles == 0) return;
     const int sms = g_umma_sms > 0 ? g_umma_sms : 148;
     const int grid = ntiles < sms ? ntiles : sms;
     if (wait_ns == 0) wait_ns = U_WAIT_NS;
     if (nsub == 1) {
         if (!one) return;  // a single sub-launch is passed by value
-        umma_cgemm_kernel<false><<<grid, UTHREADS, UGEMM_SMEM, s>>>(*one, subs, prefix, nsub, ntiles, active, err,
-                                                                     wait_ns, withhold);
+        umma_cgemm_kernel<false><<<grid, UTHREADS, UGEMM_SMEM, s>>>(*one, subs, prefix, nsub, ntiles, nullptr, active,
+                                                                     err, wait_ns, withhold);
     } else {
-        umma_cgemm_kernel<true><<<grid, UTHREADS, UGEMM_SMEM, s>>>(UmmaSub{}, subs, prefix, nsub, ntiles, active, err,
-                                                                    wait_ns, withhold);
+        umma_cgemm_kernel<true><<<grid, UTHREADS, UGEMM_SMEM, s>>>(UmmaSub{}, subs, prefix, nsub, ntiles, order, active,
+                                                                    err, wait_ns, withhold);
     }
 }
 

@@ -238,8 +238,10 @@ void Session::add_umma(const std::vector<GemmProblem>& P, const std::vector<long
         const GemmProblem& q = P[i];
         U.push_back(UmmaProblem{packed_operator(q), umma_tile_stride(q.k), q.m, q.k, umma_nkb(q.k), q.col0, q.ncol});
         for (int rt = 0; rt * 128 < q.m; ++rt)
-            for (int c0 = 0; c0 < q.ncol; c0 += 128)
+            for (int c0 = 0; c0 < q.ncol; c0 += 128) {
                 tiles.push_back(UmmaTile{(int)i, rt, rt * 128, std::min(128, q.m - rt * 128), c0, 0});
+                st.uop.push_back(U.back().B + (size_t)rt * U.back().tile_stride);
+            }
     }
     st.kind = 5;
     st.hu = UmmaSub{upload(U), upload(tiles), upload(xs), upload(ys), reinterpret_cast<const float2*>(X),

@@ -143,6 +143,7 @@ private:
         int* mpre;
         int mtotal;
         UmmaSub hu;
+        std::vector<const float*> uop;  // tcgen05 GEMM: each tile's packed operator block (batch tile order)
         PtSub hp;
         VfSub hvf;
         VaSub hva;
