@@ -69,7 +69,10 @@ void launch_kmat(const KmatJob* jobs, int njobs, long long total, int kernel, cu
 // four-product form at the same FP64 accuracy (outputs agree to ~3e-15).
 // Slabs beyond the operator's rows are skipped (a tile carries
 // ceil(rows / 16) active slabs), so an 80-150-row translation operator
-// wastes at most 15 rows.  K is consumed in slices of BK (16) through a
+// wastes at most 15 rows; so are 8-column blocks past the tile's columns and
+// 8-wide K steps past k (warp-uniform), which the last, partial column tile of
+// a problem and a k of 77-111 rounded up to the 16-wide K slice would
+// otherwise spend on zeros.  K is consumed in slices of BK (16) through a
 // GSTAGES-deep (3) cp.async pipeline; rows, columns and k beyond the problem are zero-filled
 // by the copy (src-size 0).  128-bit shared loads are served in 8-lane
 // phases (lanes with g in {2p, 2p+1}, tig 0..3); both fragment layouts put
@@ -109,6 +112,48 @@ __device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[4], con
         : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
+// One K slice of a warp's 16 x 8NJ block (NJ 8-column blocks), its first KS
+// 8-wide K steps: the three real products cr = Ar Xr, ci = Ai Xi,
+// cs = (Ar + Ai)(Xr + Xi) into the accumulators of blocks 0 .. NJ-1.
+template <int NJ>
+__device__ __forceinline__ void zgemm_slice(const double2* As, const double2* Xs, int KS, double (&cr)[4][4],
+                                            double (&ci)[4][4], double (&cs)[4][4]) {
+#pragma unroll
+    for (int ks = 0; ks < BK / 8; ++ks) {
+        if (ks >= KS) break;
+        // m16n8k8 fragments: A rows g, g+8 at k = tig, tig + 4; B k = tig, tig + 4 at column g
+        double2 a[4], b[NJ][2];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a[q] = As[(ks * 8 + 4 * (q >> 1)) * BM + 8 * (q & 1)];
+#pragma unroll
+        for (int j = 0; j < NJ; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) b[j][h] = Xs[j * 8 * BKP + ks * 8 + 4 * h];
+        double ar[4], ai[4], as[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            ar[q] = a[q].x;
+            ai[q] = a[q].y;
+            as[q] = a[q].x + a[q].y;
+        }
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+            const double br[2] = {b[j][0].x, b[j][1].x};
+            dmma16(cr[j], ar, br);
+        }
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+            const double bi[2] = {b[j][0].y, b[j][1].y};
+            dmma16(ci[j], ai, bi);
+        }
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+            const double bs[2] = {b[j][0].x + b[j][0].y, b[j][1].x + b[j][1].y};
+            dmma16(cs[j], as, bs);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256, DDFMM_ZGEMM_MINB) zgemm_kernel(const GemmProblem* __restrict__ probs,
                                                        const GemmTile* __restrict__ tiles,
                                                        const long long* __restrict__ xoff,
@@ -123,7 +168,8 @@ __global__ void __launch_bounds__(256, DDFMM_ZGEMM_MINB) zgemm_kernel(const Gemm
     const int ncol = min(BN, p.ncol - t.col0);
     const int rows = min(BM, p.m - t.row0);
     const int nrow = ((rows + 15) >> 4) << 4;  // rows of the active slabs
-    const bool active = wm * 16 < rows;
+    const bool active = wm * 16 < rows && wn * 32 < ncol;
+    const int njb = min(4, (ncol - wn * 32 + 7) >> 3);  // 8-column blocks of this warp holding columns
     if (tid < BN) {
         xo[tid] = tid < ncol ? xoff[p.col0 + t.col0 + tid] : 0;
         yo[tid] = tid < ncol ? yoff[p.col0 + t.col0 + tid] : 0;
@@ -170,39 +216,12 @@ __global__ void __launch_bounds__(256, DDFMM_ZGEMM_MINB) zgemm_kernel(const Gemm
         if (active) {
             const double2* As = gsm + (it % GSTAGES) * GSTAGE + tig * BM + ((wm * 16 + g) ^ (tig << 1));
             const double2* Xs = gsm + (it % GSTAGES) * GSTAGE + BK * BM + (wn * 32 + g) * BKP + tig;
-#pragma unroll
-            for (int ks = 0; ks < BK / 8; ++ks) {
-                // m16n8k8 fragments: A rows g, g+8 at k = tig, tig + 4; B k = tig, tig + 4 at column g
-                double2 a[4], b[4][2];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) a[q] = As[(ks * 8 + 4 * (q >> 1)) * BM + 8 * (q & 1)];
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) b[j][h] = Xs[j * 8 * BKP + ks * 8 + 4 * h];
-                // three real products: cr = ArXr, ci = AiXi, cs = (Ar+Ai)(Xr+Xi)
-                double ar[4], ai[4], as[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    ar[q] = a[q].x;
-                    ai[q] = a[q].y;
-                    as[q] = a[q].x + a[q].y;
-                }
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const double br[2] = {b[j][0].x, b[j][1].x};
-                    dmma16(cr[j], ar, br);
-                }
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const double bi[2] = {b[j][0].y, b[j][1].y};
-                    dmma16(ci[j], ai, bi);
-                }
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const double bs[2] = {b[j][0].x + b[j][0].y, b[j][1].x + b[j][1].y};
-                    dmma16(cs[j], as, bs);
-                }
+            const int KS = min(BK / 8, (p.k - it * BK + 7) >> 3);  // 8-wide K steps holding k
+            switch (njb) {
+                case 4: zgemm_slice<4>(As, Xs, KS, cr, ci, cs); break;
+                case 3: zgemm_slice<3>(As, Xs, KS, cr, ci, cs); break;
+                case 2: zgemm_slice<2>(As, Xs, KS, cr, ci, cs); break;
+                default: zgemm_slice<1>(As, Xs, KS, cr, ci, cs); break;
             }
         }
     }

@@ -588,8 +588,10 @@ __global__ void __launch_bounds__(UTHREADS, 1) umma_cgemm_kernel(const UmmaSub o
                     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                     const uint32_t ahi = smem_u32(usm + s * U_STAGE_BYTES), alo = ahi + U_A_BYTES;
                     const uint32_t bhi = ahi + 2 * U_A_BYTES, blo = bhi + U_B_BYTES;
+                    const int KS = min(UBK / 8, (2 * T.p.k - kb * UBK + 7) >> 3);  // K steps holding k (zeros past it)
 #pragma unroll
                     for (int ks = 0; ks < UBK / 8; ++ks) {  // K = 8 per MMA
+                        if (ks >= KS) break;
                         const uint32_t o = ks * 256, oa = ks * 32;  // operator: two core matrices; columns: 32 B
                         const uint64_t dah = sdesc_a(ahi + oa), dal = sdesc_a(alo + oa);
                         umma_tf32(d, dah, sdesc(bhi + o), idesc, (kb > 0 || ks > 0) ? 1u : 0u);
