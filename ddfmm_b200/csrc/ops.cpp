@@ -3,22 +3,33 @@
 
 #include <cstring>
 #include <fstream>
-#include <iterator>
 #include <mutex>
 #include <sstream>
 #include <stdexcept>
 
+#include <fcntl.h>
+#include <sys/mman.h>
 #include <sys/stat.h>
+#include <unistd.h>
 
 namespace ddfmm {
 
 namespace {
+// A whole operator file mapped read-only; the matrices are copied out of the
+// mapping (no intermediate copy of the file).
 struct In {
-    std::vector<char> buf;
+    const char* buf = nullptr;
+    size_t size = 0;
     size_t o = 0;
     std::string name;
+    In() = default;
+    In(const In&) = delete;
+    In& operator=(const In&) = delete;
+    ~In() {
+        if (buf && size) munmap(const_cast<char*>(buf), size);
+    }
     void need(size_t n) {
-        if (o + n > buf.size())
+        if (o + n > size)
             throw std::runtime_error("operator file " + name + " is truncated");
     }
     int i32() {
@@ -74,20 +85,34 @@ struct In {
     }
 };
 
-In slurp(const std::string& path) {
-    std::ifstream f(path, std::ios::binary);
-    if (!f) throw std::runtime_error("cannot open operator file " + path);
-    In in;
+void slurp(const std::string& path, In& in) {
+    const int fd = open(path.c_str(), O_RDONLY);
+    if (fd < 0) throw std::runtime_error("cannot open operator file " + path);
+    struct stat st;
+    if (fstat(fd, &st) != 0) {
+        close(fd);
+        throw std::runtime_error("cannot size operator file " + path);
+    }
     in.name = path;
-    in.buf.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
-    return in;
+    in.size = (size_t)st.st_size;
+    if (in.size > 0) {
+        void* p = mmap(nullptr, in.size, PROT_READ, MAP_PRIVATE | MAP_POPULATE, fd, 0);
+        if (p == MAP_FAILED) {
+            close(fd);
+            in.size = 0;
+            throw std::runtime_error("cannot map operator file " + path);
+        }
+        in.buf = static_cast<const char*>(p);
+    }
+    close(fd);
 }
 }  // namespace
 
 void OperatorLib::load(const std::string& ld_path, const std::string& hd_path) {
     ld.clear();
     hd.clear();
-    In a = slurp(ld_path);
+    In a;
+    slurp(ld_path, a);
     int nw = a.dim();
     for (int w = 0; w < nw; ++w) {
         LowFreqOp op;
@@ -105,8 +130,9 @@ void OperatorLib::load(const std::string& ld_path, const std::string& hd_path) {
         for (int i = 0; i < 343; ++i) op.ue2dc[i] = a.ctns(op.tdim);
         ld[op.W] = std::move(op);
     }
-    if (a.o != a.buf.size()) throw std::runtime_error("ld file has trailing bytes");
-    In b = slurp(hd_path);
+    if (a.o != a.size) throw std::runtime_error("ld file has trailing bytes");
+    In b;
+    slurp(hd_path, b);
     nw = b.dim();
     for (int w = 0; w < nw; ++w) {
         double W = b.f64();
@@ -125,7 +151,7 @@ void OperatorLib::load(const std::string& ld_path, const std::string& hd_path) {
             lvl[key] = std::move(op);
         }
     }
-    if (b.o != b.buf.size()) throw std::runtime_error("hd file has trailing bytes");
+    if (b.o != b.size) throw std::runtime_error("hd file has trailing bytes");
 }
 
 std::shared_ptr<const OperatorLib> OperatorLib::shared(const std::string& ld_path, const std::string& hd_path) {

@@ -148,6 +148,11 @@ Session::~Session() {
 void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<long long> >& xo,
                        std::vector<std::vector<long long> >& yo, const double2* X, double2* Y, int mode,
                        const char* label) {
+    struct Clock {
+        double& acc;
+        std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+        ~Clock() { acc += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+    } clock{t_emit_gemm_};
     double flops = 0, bytes = 0;
     std::vector<GemmProblem> P;
     std::vector<GemmTile> tiles;
@@ -1096,6 +1101,7 @@ void Session::build() {
     std::vector<long long> lf_off(nb, -1);
     for (int l = 0; l < nLF; ++l) lf_off[lfbox[l]] = (long long)l * nE;
     HfColumns cols = hf_columns(T, up, dn, kids, lf_off, dirpts.size(), hfcanon.size());
+    phase("hf_columns");
     // ---------------------------------------------------------------- steps: HF upward
     // widths ascending = levels descending; hf_upeq holds w (upeqnden = E1 w)
     for (auto hit = hflevels.rbegin(); hit != hflevels.rend(); ++hit) {
@@ -1220,7 +1226,9 @@ void Session::build() {
         // pass over the union of their V-list sources; then one inverse transform
         // per target.
         {
+            const auto tv = std::chrono::steady_clock::now();
             VlistGroupPlan vg = vlist_groups(T, lfbox, lfidx, ids);
+            t_emit_vgroups_ += std::chrono::duration<double>(std::chrono::steady_clock::now() - tv).count();
             stats_.v_pairs += vg.pairs;
             const std::vector<int>& trg = vg.trg;
             if (!trg.empty()) {
@@ -1396,6 +1404,9 @@ void Session::build() {
             }
     }
     phase("steps_lf_down");
+    if (trace)
+        std::fprintf(stderr, "ddfmm setup   (host seconds in GEMM step emission %.3f, V-list grouping %.3f)\n",
+                     t_emit_gemm_, t_emit_vgroups_);
     flush_packs();
     if (mixed) {
         // the mixed eval reads only the FP32 copies (and, on tcgen05, only the packed

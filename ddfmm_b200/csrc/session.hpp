@@ -215,7 +215,8 @@ private:
     int* d_err_ = nullptr;  // set by a tensor-core GEMM that timed out
     unsigned long long stall_wait_ns_ = 0;  // armed failure-path hook (0: none)
     std::map<std::pair<const void*, long long>, const float*> packed_;  // (operator, m k) -> packed copy
-    std::vector<UmmaPackJob> pack_jobs_;                                 // packing still to launch
+    std::vector<UmmaPackJob> pack_jobs_;
+    double t_emit_gemm_ = 0, t_emit_vgroups_ = 0;  // setup trace: host seconds in add_gemm, vlist_groups                                 // packing still to launch
     // packed operators (tcgen05 form): the chunk being filled, the operators this
     // session uses (its own and shared ones), and those it created but has not yet
     // published to the process-wide cache (they are, once their packing completed)

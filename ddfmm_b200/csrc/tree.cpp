@@ -2,7 +2,9 @@
 #include "tree.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <deque>
 #include <exception>
@@ -32,18 +34,65 @@ Pt3 Tree::center(const Box& b) const {
     return t;
 }
 
-int Tree::find(int level, const Idx3& idx) const {
-    auto it = index_.find(pack(level, idx));
-    return it == index_.end() ? -1 : it->second;
+static inline uint64_t mix64(uint64_t k) {  // a 64-bit finalizer: every key bit reaches the slot bits
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdULL;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ULL;
+    k ^= k >> 33;
+    return k;
 }
 
-int Tree::child(int b, int ind) const {
-    const Box& p = boxes[b];
-    Idx3 c{{2 * p.idx[0] + ((ind & 4) >> 2), 2 * p.idx[1] + ((ind & 2) >> 1), 2 * p.idx[2] + (ind & 1)}};
-    return find(p.level + 1, c);
+void Tree::BoxIndex::clear() {
+    keys.assign(1024, ~0ull);
+    vals.assign(1024, -1);
+    used = 0;
 }
+
+bool Tree::BoxIndex::insert(uint64_t k, int v) {
+    if (2 * (used + 1) > keys.size()) {  // grow to keep the table at most half full
+        std::vector<uint64_t> ok;
+        std::vector<int> ov;
+        ok.swap(keys);
+        ov.swap(vals);
+        keys.assign(2 * ok.size(), ~0ull);
+        vals.assign(2 * ok.size(), -1);
+        used = 0;
+        for (size_t i = 0; i < ok.size(); ++i)
+            if (ok[i] != ~0ull) insert(ok[i], ov[i]);
+    }
+    const size_t mask = keys.size() - 1;
+    for (size_t s = mix64(k) & mask;; s = (s + 1) & mask) {
+        if (keys[s] == k) return false;
+        if (keys[s] == ~0ull) {
+            keys[s] = k;
+            vals[s] = v;
+            ++used;
+            return true;
+        }
+    }
+}
+
+int Tree::BoxIndex::find(uint64_t k) const {
+    const size_t mask = keys.size() - 1;
+    for (size_t s = mix64(k) & mask;; s = (s + 1) & mask) {
+        if (keys[s] == k) return vals[s];
+        if (keys[s] == ~0ull) return -1;
+    }
+}
+
+int Tree::find(int level, const Idx3& idx) const { return index_.find(pack(level, idx)); }
+
+// a box has all 8 children (some without points) or none
+int Tree::child(int b, int ind) const { return boxes[b].kid0 >= 0 ? boxes[b].kid0 + ind : -1; }
 
 // nml2dir, src/wave3d.cpp:43-71
+// Component d: t = floor(atan(n[d] / mval) / Ang) clamped to [-B, B-1], and
+// 2t + 1; the largest component becomes C round(atan(+-1)) = +-C.  Where the
+// tree holds the bin edges for C, t is found among them, and the arithmetic
+// above runs only for a ratio within 1e-9 of an edge (so t is the same as the
+// arithmetic's: away from an edge, rounding in atan and the division cannot
+// move the quotient across an integer).
 Idx3 Tree::nml2dir(const Pt3& n, double W) const {
     int C = prm.npq * (int)std::round(W);
     int B = C / 2;
@@ -54,16 +103,29 @@ Idx3 Tree::nml2dir(const Pt3& n, double W) const {
             midx = d;
             mval = std::fabs(n[d]);
         }
-    double val[3];
-    for (int d = 0; d < 3; ++d) val[d] = std::atan(n[d] / mval);
-    double Ang = (M_PI / 2) / C;
+    const double Ang = (M_PI / 2) / C;
+    const std::vector<double>* E = C < (int)edges_.size() && !edges_[C].empty() ? &edges_[C] : nullptr;
     Idx3 res;
     for (int d = 0; d < 3; ++d) {
-        int t = (int)std::floor(val[d] / Ang);
+        if (d == midx) continue;
+        const double x = n[d] / mval;
+        int t = 0;
+        bool exact = true;
+        if (E) {
+            // edges <= x: t = -B below every edge, edge j is tan((j + 1 - B) Ang)
+            const size_t i = std::upper_bound(E->begin(), E->end(), x) - E->begin();
+            const double lo = i > 0 ? (*E)[i - 1] : -2.0, hi = i < E->size() ? (*E)[i] : 2.0;
+            if (x - lo > 1e-9 && hi - x > 1e-9) {
+                t = (int)i - B;
+                exact = false;
+            }
+        }
+        if (exact) t = (int)std::floor(std::atan(x) / Ang);
         t = std::min(std::max(t, -B), B - 1);
         res[d] = 2 * t + 1;
     }
-    res[midx] = C * (int)std::round(val[midx]);
+    // n[midx] / mval is exactly +-1, and round(atan(+-1)) = +-1
+    res[midx] = n[midx] > 0 ? C : -C;
     return res;
 }
 
@@ -145,7 +207,9 @@ static double l2(const Pt3& a) {
 void Tree::lowlist(int bi) {
     Box& cur = boxes[bi];
     check(cur.level != cell_level(), "low-frequency box at the cell level");
-    std::set<uint64_t> U, V, Wl, X;
+    // key sets as vectors, sorted and deduplicated at the end (key order, as the
+    // reference's std::set<BoxKey>)
+    std::vector<uint64_t> U, V, Wl, X;
     Idx3 par{{cur.idx[0] / 2, cur.idx[1] / 2, cur.idx[2] / 2}};
     int L = 1 << cur.level;
     int lo[3], hi[3];
@@ -153,35 +217,50 @@ void Tree::lowlist(int bi) {
         lo[d] = std::max(2 * par[d] - 2, 0);
         hi[d] = std::min(2 * par[d] + 4, L);
     }
+    // find_or_ancestor(cur.level, tp) for the 6^3 block: tp's parent-level box
+    // tp / 2 is one of the parent's 27 neighbours; the box at tp exists exactly
+    // when that neighbour exists and is split (then it is child tp & 1),
+    // otherwise the answer is the neighbour's own nearest existing ancestor
+    int nb[27];
+    for (int a = 0; a < 27; ++a) {
+        const Idx3 q{{par[0] + a / 9 - 1, par[1] + (a / 3) % 3 - 1, par[2] + a % 3 - 1}};
+        const int half = L / 2;
+        nb[a] = (q[0] < 0 || q[1] < 0 || q[2] < 0 || q[0] >= half || q[1] >= half || q[2] >= half)
+                    ? -1
+                    : find_or_ancestor(cur.level - 1, q);
+    }
     for (int i = lo[0]; i < hi[0]; ++i)
         for (int j = lo[1]; j < hi[1]; ++j)
             for (int k = lo[2]; k < hi[2]; ++k) {
                 Idx3 tp{{i, j, k}};
                 if (tp == cur.idx) continue;
-                int ri = find_or_ancestor(cur.level, tp);
+                const int q = nb[(i / 2 - par[0] + 1) * 9 + (j / 2 - par[1] + 1) * 3 + (k / 2 - par[2] + 1)];
+                int ri = q;
+                if (q >= 0 && boxes[q].level == cur.level - 1 && boxes[q].kid0 >= 0)
+                    ri = boxes[q].kid0 + (i & 1) * 4 + (j & 1) * 2 + (k & 1);
                 if (ri < 0) continue;
                 const Box& res = boxes[ri];
                 bool adj = adjacent(res, cur);
                 if (res.level < cur.level && res.has_pts()) {
                     if (!adj)
-                        X.insert(pack(res.level, res.idx));
+                        X.push_back(pack(res.level, res.idx));
                     else if (cur.terminal())
-                        U.insert(pack(res.level, res.idx));
+                        U.push_back(pack(res.level, res.idx));
                 }
                 if (res.level == cur.level) {
                     if (!adj) {
                         Idx3 bb{{res.idx[0] - cur.idx[0], res.idx[1] - cur.idx[1], res.idx[2] - cur.idx[2]}};
                         check(linfty(bb) <= 3, "V-list offset beyond 3");
-                        if (res.has_pts()) V.insert(pack(res.level, res.idx));
+                        if (res.has_pts()) V.push_back(pack(res.level, res.idx));
                     } else if (cur.terminal()) {
-                        std::deque<int> rest(1, ri);
+                        std::vector<int> rest(1, ri);  // boxes still to visit (any order: the lists are sets)
                         while (!rest.empty()) {
-                            int fi = rest.front();
-                            rest.pop_front();
+                            int fi = rest.back();
+                            rest.pop_back();
                             const Box& fnt = boxes[fi];
                             bool a2 = adjacent(fnt, cur);
-                            if (!a2 && fnt.has_pts()) Wl.insert(pack(fnt.level, fnt.idx));
-                            if (a2 && fnt.terminal() && fnt.has_pts()) U.insert(pack(fnt.level, fnt.idx));
+                            if (!a2 && fnt.has_pts()) Wl.push_back(pack(fnt.level, fnt.idx));
+                            if (a2 && fnt.terminal() && fnt.has_pts()) U.push_back(pack(fnt.level, fnt.idx));
                             if (a2 && !fnt.terminal())
                                 for (int ind = 0; ind < 8; ++ind) {
                                     int c = child(fi, ind);
@@ -192,10 +271,17 @@ void Tree::lowlist(int bi) {
                     }
                 }
             }
-    if (cur.terminal() && cur.has_pts()) U.insert(pack(cur.level, cur.idx));
-    auto out = [&](const std::set<uint64_t>& s, std::vector<int>& v) {
+    if (cur.terminal() && cur.has_pts()) U.push_back(pack(cur.level, cur.idx));
+    auto out = [&](std::vector<uint64_t>& s, std::vector<int>& v) {
+        std::sort(s.begin(), s.end());
+        s.erase(std::unique(s.begin(), s.end()), s.end());
         v.clear();
-        for (uint64_t key : s) v.push_back(index_.at(key));
+        v.reserve(s.size());
+        for (uint64_t key : s) {
+            const int b = index_.find(key);
+            check(b >= 0, "listed box missing");
+            v.push_back(b);
+        }
     };
     out(U, cur.ulist);
     out(V, cur.vlist);
@@ -210,6 +296,33 @@ void Tree::highlist(int bi) {
     double W = width(cur.level);
     double D = W * W + W;
     double threshold = D - 1e-12;
+    // far boxes grouped by wedge in visiting order: a small open-addressing table
+    // from wedge to group (a box has tens of wedges), the groups moved into the
+    // map in wedge order at the end
+    std::vector<std::pair<Idx3, std::vector<int> > > groups;
+    std::vector<int> slot(256, -1);  // kept at most half full
+    auto hash = [](const Idx3& d) {
+        return (unsigned)(d[0] * 73856093) ^ (unsigned)(d[1] * 19349663) ^ (unsigned)(d[2] * 83492791);
+    };
+    auto group_of = [&](const Idx3& d) -> std::vector<int>& {
+        unsigned mask = (unsigned)slot.size() - 1;
+        unsigned s = hash(d) & mask;
+        for (; slot[s] >= 0; s = (s + 1) & mask)
+            if (groups[slot[s]].first == d) return groups[slot[s]].second;
+        groups.emplace_back(d, std::vector<int>());
+        if (2 * groups.size() <= slot.size()) {
+            slot[s] = (int)groups.size() - 1;
+        } else {  // grow, and place every group again
+            slot.assign(2 * slot.size(), -1);
+            mask = (unsigned)slot.size() - 1;
+            for (int g = 0; g < (int)groups.size(); ++g) {
+                unsigned t = hash(groups[g].first) & mask;
+                while (slot[t] >= 0) t = (t + 1) & mask;
+                slot[t] = g;
+            }
+        }
+        return groups.back().second;
+    };
     auto classify = [&](int oi) {
         const Box& oth = boxes[oi];
         if (!oth.has_pts()) return;
@@ -217,7 +330,7 @@ void Tree::highlist(int bi) {
         double n = l2(diff);
         if (n >= threshold) {
             Pt3 u{{diff[0] / n, diff[1] / n, diff[2] / n}};
-            cur.far[nml2dir(u, W)].push_back(oi);
+            group_of(nml2dir(u, W)).push_back(oi);
         } else {
             cur.nearlist.push_back(oi);
         }
@@ -238,6 +351,11 @@ void Tree::highlist(int bi) {
                 classify(oi);
             }
     }
+    std::sort(groups.begin(), groups.end(),
+              [](const std::pair<Idx3, std::vector<int> >& a, const std::pair<Idx3, std::vector<int> >& b) {
+                  return a.first < b.first;
+              });
+    for (auto& g : groups) cur.far.emplace_hint(cur.far.end(), g.first, std::move(g.second));
 }
 
 // Host threads for list construction: DDFMM_HOST_THREADS when set (> 0), else
@@ -281,7 +399,16 @@ void Tree::build(const double* p3n, int n, const TreeParams& p) {
     boxes.clear();
     order.clear();
     index_.clear();
+    edges_.clear();
     check(prm.ncell >= 1 && (prm.ncell & (prm.ncell - 1)) == 0, "ncell must be a power of two");
+    const bool trace = std::getenv("DDFMM_SETUP_TRACE") != nullptr;
+    auto tmark = std::chrono::steady_clock::now();
+    auto phase = [&](const char* what) {
+        if (!trace) return;
+        const auto t = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "ddfmm tree  %-16s %8.3f s\n", what, std::chrono::duration<double>(t - tmark).count());
+        tmark = t;
+    };
     const int numC = prm.ncell, lvlC = cell_level();
     const double K = prm.K;
     // cells (all of them, empty or not), points in id order
@@ -302,7 +429,7 @@ void Tree::build(const double* p3n, int n, const TreeParams& p) {
         b.pts = std::move(pts);
         boxes.push_back(std::move(b));
         int bi = (int)boxes.size() - 1;
-        check(index_.emplace(pack(level, idx), bi).second, "duplicate box");
+        check(index_.insert(pack(level, idx), bi), "duplicate box");
         q.push_back(bi);
     };
     for (int a = 0; a < numC; ++a)
@@ -326,6 +453,7 @@ void Tree::build(const double* p3n, int n, const TreeParams& p) {
             }
             Idx3 base = boxes[bi].idx;
             boxes[bi].pts.clear();
+            boxes[bi].kid0 = (int)boxes.size();  // add() appends the children in ind order
             for (int ind = 0; ind < 8; ++ind)
                 add(level + 1, Idx3{{2 * base[0] + ((ind & 4) >> 2), 2 * base[1] + ((ind & 2) >> 1), 2 * base[2] + (ind & 1)}},
                     std::move(cp[ind]));
@@ -333,6 +461,7 @@ void Tree::build(const double* p3n, int n, const TreeParams& p) {
             boxes[bi].tag |= TAG_TERMINAL;
         }
     }
+    phase("partition");
     order.resize(boxes.size());
     for (size_t i = 0; i < boxes.size(); ++i) order[i] = (int)i;
     std::sort(order.begin(), order.end(), [&](int x, int y) {
@@ -344,7 +473,20 @@ void Tree::build(const double* p3n, int n, const TreeParams& p) {
     // level by level (levels are contiguous in key order), the boxes of a level in
     // parallel.  Every box's lists come from the same sequential code, so the result
     // does not depend on the thread count.
+    phase("sort");
     const double eps = 1e-12;
+    // nml2dir's bin edges for every high-frequency width of the tree
+    for (size_t i = 0; i < order.size(); ++i) {
+        if (i > 0 && boxes[order[i]].level == boxes[order[i - 1]].level) continue;
+        const double W = width(boxes[order[i]].level);
+        if (W < 1 - eps) continue;
+        const int C = prm.npq * (int)std::round(W), B = C / 2;
+        if (C <= 0 || C > (1 << 16)) continue;
+        if ((int)edges_.size() <= C) edges_.resize(C + 1);
+        if (!edges_[C].empty()) continue;
+        const double Ang = (M_PI / 2) / C;
+        for (int t = 1 - B; t <= B - 1; ++t) edges_[C].push_back(std::tan(t * Ang));
+    }
     std::vector<size_t> lv(1, 0);
     for (size_t i = 1; i < order.size(); ++i)
         if (boxes[order[i]].level != boxes[order[i - 1]].level) lv.push_back(i);
@@ -358,30 +500,41 @@ void Tree::build(const double* p3n, int n, const TreeParams& p) {
             else
                 highlist(bi);
         });
+    phase("lists");
     for (size_t l = 0; l + 1 < lv.size(); ++l)
         parallel_for(lv[l + 1] - lv[l], [&](size_t i) {
             Box& cur = boxes[order[lv[l] + i]];
             double W = width(cur.level);
             if (!(W > 1 - eps && cur.has_pts())) return;
+            // the sets as sorted, deduplicated vectors first (most insertions repeat)
+            std::vector<Idx3> out, inc;
             if (cur.level != lvlC) {
                 int pi = find(cur.level - 1, Idx3{{cur.idx[0] / 2, cur.idx[1] / 2, cur.idx[2] / 2}});
                 check(pi >= 0, "missing parent");
-                for (const Idx3& d : boxes[pi].outdirs) cur.outdirs.insert(parent_dir(d));
-                for (const Idx3& d : boxes[pi].incdirs) cur.incdirs.insert(parent_dir(d));
+                for (const Idx3& d : boxes[pi].outdirs) out.push_back(parent_dir(d));
+                for (const Idx3& d : boxes[pi].incdirs) inc.push_back(parent_dir(d));
             }
             Pt3 cc = center(cur);
             for (auto& kv : cur.far) {
                 // the incoming direction of every far box is its key: highlist classified
                 // (cc - oc) / |cc - oc| with the same arithmetic
-                cur.incdirs.insert(kv.first);
+                inc.push_back(kv.first);
                 for (int oi : kv.second) {
                     Pt3 t = sub(center(boxes[oi]), cc);
                     double nt = l2(t);
                     for (int d = 0; d < 3; ++d) t[d] /= nt;
-                    cur.outdirs.insert(nml2dir(t, W));
+                    const Idx3 dir = nml2dir(t, W);
+                    if (out.empty() || out.back() != dir) out.push_back(dir);  // runs repeat a wedge
                 }
             }
+            for (std::vector<Idx3>* v : {&out, &inc}) {
+                std::sort(v->begin(), v->end());
+                v->erase(std::unique(v->begin(), v->end()), v->end());
+            }
+            cur.outdirs.insert(out.begin(), out.end());
+            cur.incdirs.insert(inc.begin(), inc.end());
         });
+    phase("directions");
 }
 
 // HighFetchIndex3Sort, src/mlib3d.cpp:328-357

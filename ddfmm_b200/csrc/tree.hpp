@@ -11,16 +11,15 @@
 //                           ChildDir, Dir2Width, BoxCenter)
 //   * canonical wedges      src/mlib3d.cpp:283-357 (predir, HighFetchShuffle,
 //                           HighFetchIndex3Sort)
-// Boxes live in one vector; a hash map from the packed key (level, i, j, k)
-// finds them, and "key order" (the order of the reference's std::map<BoxKey>)
-// is level first, then i, j, k lexicographically.
+// Boxes live in one vector; an open-addressing hash table from the packed key
+// (level, i, j, k) finds them, and "key order" (the order of the reference's
+// std::map<BoxKey>) is level first, then i, j, k lexicographically.
 #pragma once
 #include <array>
 #include <cstdint>
 #include <map>
 #include <set>
 #include <string>
-#include <unordered_map>
 #include <vector>
 
 namespace ddfmm {
@@ -34,6 +33,7 @@ struct Box {
     int level = 0;
     Idx3 idx{{0, 0, 0}};
     int tag = 0;
+    int kid0 = -1;                             // a split box's 8 children are boxes kid0 .. kid0 + 7
     std::vector<int> pts;                      // point ids of a terminal box
     std::vector<int> ulist, vlist, wlist, xlist;  // LF lists, key order
     std::vector<int> nearlist;                 // HF near boxes (endeidxvec)
@@ -77,7 +77,20 @@ public:
     double dir_width(const Idx3& d) const;
 
 private:
-    std::unordered_map<uint64_t, int> index_;
+    // packed key -> box index: linear probing in a power-of-two table kept at
+    // most half full (keys are never ~0, the empty mark)
+    struct BoxIndex {
+        std::vector<uint64_t> keys;
+        std::vector<int> vals;
+        size_t used = 0;
+        void clear();
+        bool insert(uint64_t k, int v);  // false if k is present
+        int find(uint64_t k) const;      // -1 if absent
+    };
+    BoxIndex index_;
+    // nml2dir's bin edges tan(t (pi/2) / C), t = 1-C/2 .. C/2-1, by C (filled by
+    // build() for the widths of the tree before the parallel list passes)
+    std::vector<std::vector<double> > edges_;
     static uint64_t pack(int level, const Idx3& idx);
     bool adjacent(const Box& a, const Box& b) const;
     int find_or_ancestor(int level, Idx3 idx) const;

@@ -5,11 +5,17 @@ boxes with points per level and the summed directional far-list sizes per
 level (src/wave3d_eval.cpp:345-372); the golden fixtures recorded them from
 the reference binary.  The native library's host-only tree builder must
 reproduce every number (no GPU needed)."""
+import os
+import subprocess
+
 import numpy as np
 import pytest
 
 import fixtures
-from ddfmm_b200 import _lib
+from ddfmm_b200 import _lib, geometry
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.join(ROOT, "ddfmm_b200")
 
 
 @pytest.mark.parametrize("name", fixtures.case_names())
@@ -57,3 +63,36 @@ def test_tree_rejects_point_outside_root_box():
 def test_tree_rejects_bad_cell_count():
     with pytest.raises(_lib.DDFMMError):
         _lib.tree_stats(np.zeros((4, 3)), 4.0, 100, 8, 3)
+
+
+@pytest.fixture(scope="module")
+def tree_hash(tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("treehash") / "tree_hash")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(LIBDIR, "csrc"), "-o", out,
+                    os.path.join(ROOT, "tests", "cpp", "tree_hash.cpp"), os.path.join(LIBDIR, "libddfmm_b200.so"),
+                    "-Wl,-rpath," + LIBDIR], check=True)
+    return out
+
+
+# Order-sensitive hashes of every list of these trees, recorded from the first
+# host implementation (hash-map box lookups, set-based lists, per-box atan
+# wedge classification); the faster list construction must reproduce them.
+TREE_HASHES = [
+    ("sphere", 16.0, None, 100, "boxes 11576 entries 432885 hash 2631c1902f959217"),
+    ("cluster", 4.0, 1500, 8, "boxes 1128 entries 31660 hash ec60cd5aa10d6ca2"),
+    ("ellipsoid", 8.0, 3000, 100, "boxes 1024 entries 22757 hash 5dc3f3fb33a49e6f"),
+    ("cluster", 16.0, 30000, 20, "boxes 10824 entries 631849 hash 9ff8f25a724161d5"),
+]
+
+
+@pytest.mark.parametrize("geom,K,N,ptsmax,want", TREE_HASHES)
+def test_tree_lists_unchanged(tree_hash, tmp_path, geom, K, N, ptsmax, want):
+    gen = {"sphere": geometry.sphere_points, "ellipsoid": geometry.ellipsoid_points,
+           "cluster": geometry.cluster_points}[geom]
+    pos = gen(N if N is not None else geometry.sphere_n_for(K), K)
+    path = tmp_path / "pos.bin"
+    pos.astype("<f8").tofile(path)
+    r = subprocess.run([tree_hash, str(path), str(len(pos)), repr(K), str(geometry.cells_for(K)),
+                        str(geometry.maxlevel_for(K)), str(ptsmax)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.strip() == want
