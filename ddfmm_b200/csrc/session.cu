@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <exception>
 #include <set>
 #include <stdexcept>
@@ -70,10 +71,27 @@ template <class T>
 T* Session::upload(const std::vector<T>& v) {
     const size_t bytes = v.size() * sizeof(T);
     if (bytes > kArenaMax) {
-        T* d = dalloc<T>(v.size());
-        CK(cudaMemcpyAsync(d, v.data(), bytes, cudaMemcpyHostToDevice, stream_));
-        // the caller's vector may die right after: make the copy complete
-        CK(cudaStreamSynchronize(stream_));
+        const auto t0 = std::chrono::steady_clock::now();
+        T* d = nullptr;
+        if (bytes <= kMidMax) {
+            const size_t need = (bytes + 255) & ~(size_t)255;
+            if (mid_used_ + need > mid_cap_) {  // chunks of 4 MiB doubling to 64 MiB: small sessions stay small
+                const size_t cap = std::max(need, std::min(kMidChunk, std::max((size_t)kMidMax, 2 * mid_cap_)));
+                void* chunk = nullptr;
+                CK(cudaMalloc(&chunk, cap));
+                allocs_.push_back(chunk);
+                stats_.device_bytes += cap;
+                mid_dev_ = static_cast<char*>(chunk);
+                mid_used_ = 0;
+                mid_cap_ = cap;
+            }
+            d = reinterpret_cast<T*>(mid_dev_ + mid_used_);
+            mid_used_ += need;
+        } else {
+            d = dalloc<T>(v.size());
+        }
+        stage_copy(d, v.data(), bytes);  // the caller's vector may die right after: the data is staged
+        t_big_uploads_ += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         return d;
     }
     const size_t need = (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;  // 256-byte aligned slots
@@ -102,9 +120,36 @@ T* Session::upload(const std::vector<T>& v) {
 
 void Session::flush_uploads() {
     if (arena_.used > arena_.sent)
-        CK(cudaMemcpyAsync(arena_.dev + arena_.sent, arena_.host.data() + arena_.sent, arena_.used - arena_.sent,
-                           cudaMemcpyHostToDevice, stream_));
+        stage_copy(arena_.dev + arena_.sent, arena_.host.data() + arena_.sent, arena_.used - arena_.sent);
     arena_.sent = arena_.used;
+}
+
+void Session::stage_copy(void* dst, const void* src, size_t bytes) {
+    if (!stage_[0])
+        for (int k = 0; k < 2; ++k) {
+            CK(cudaHostAlloc((void**)&stage_[k], kStage, cudaHostAllocDefault));
+            CK(cudaEventCreateWithFlags(&stage_ev_[k], cudaEventDisableTiming));
+            CK(cudaEventRecord(stage_ev_[k], stream_));
+        }
+    for (size_t off = 0; off < bytes;) {
+        const size_t n = std::min(kStage, bytes - off);
+        const int k = stage_next_;
+        stage_next_ ^= 1;
+        CK(cudaEventSynchronize(stage_ev_[k]));  // the device has read this buffer's previous contents
+        std::memcpy(stage_[k], static_cast<const char*>(src) + off, n);
+        CK(cudaMemcpyAsync(static_cast<char*>(dst) + off, stage_[k], n, cudaMemcpyHostToDevice, stream_));
+        CK(cudaEventRecord(stage_ev_[k], stream_));
+        off += n;
+    }
+}
+
+void Session::stage_release() {
+    for (int k = 0; k < 2; ++k) {
+        if (stage_ev_[k]) cudaEventDestroy(stage_ev_[k]);
+        if (stage_[k]) cudaFreeHost(stage_[k]);
+        stage_ev_[k] = nullptr;
+        stage_[k] = nullptr;
+    }
 }
 
 Session::Session(const double* pos3n, int n, const SessionParams& p, const std::string& ld_path,
@@ -140,6 +185,7 @@ Session::Session(const double* pos3n, int n, const SessionParams& p, const std::
 
 Session::~Session() {
     if (stream_) cudaStreamSynchronize(stream_);
+    stage_release();
     for (cudaEvent_t e : ev_) cudaEventDestroy(e);
     for (void* p : allocs_) cudaFree(p);
     if (stream_) cudaStreamDestroy(stream_);
@@ -400,11 +446,6 @@ struct GemmBatch {
     }
 };
 
-// (width, wedge) as one hash key: widths are powers of two, wedge components |d| < 1024
-uint64_t wedge_key(double W, const Idx3& d) {
-    const uint64_t wl = (uint64_t)(std::lround(std::log2(W)) + 32);
-    return (wl << 33) | ((uint64_t)(d[0] + 1024) << 22) | ((uint64_t)(d[1] + 1024) << 11) | (uint64_t)(d[2] + 1024);
-}
 Pt3 shifted_point(int ind, double W) {  // ShiftedPoint, src/mlib3d.cpp:21-30
     int a = (ind & 4) >> 2, b = (ind & 2) >> 1, c = ind & 1;
     return Pt3{{(a - 0.5) * W / 2, (b - 0.5) * W / 2, (c - 0.5) * W / 2}};
@@ -692,14 +733,41 @@ void Session::build() {
         int did;  // dense id, in order of first use
     };
     std::map<std::pair<double, Idx3>, DirPts> dirpts;
-    std::unordered_map<uint64_t, const DirPts*> dirfast;  // hash index into dirpts (node addresses are stable)
+    // dense index into dirpts (node addresses are stable): per width, the wedge's
+    // components (each in [-C, C], C = npq W) address a (2C+1)^3 table
+    struct DirTable {
+        double W;
+        int C;
+        std::vector<const DirPts*> t;
+    };
+    std::deque<DirTable> dirtabs;
+    DirTable* last_tab = nullptr;
+    auto dir_slot = [&](double W, const Idx3& d) -> const DirPts** {
+        if (!last_tab || last_tab->W != W) {
+            last_tab = nullptr;
+            for (DirTable& x : dirtabs)
+                if (x.W == W) last_tab = &x;
+            if (!last_tab) {
+                const int C = prm_.tree.npq * (int)std::round(W);
+                if (C <= 0 || C > 128) return nullptr;
+                dirtabs.push_back(DirTable{W, C, std::vector<const DirPts*>((size_t)(2 * C + 1) * (2 * C + 1) * (2 * C + 1), nullptr)});
+                last_tab = &dirtabs.back();
+            }
+        }
+        const int C = last_tab->C, E = 2 * C + 1;
+        for (int k = 0; k < 3; ++k)
+            if (d[k] < -C || d[k] > C) return nullptr;
+        return &last_tab->t[((size_t)(d[0] + C) * E + (d[1] + C)) * E + (d[2] + C)];
+    };
     auto get_dir = [&](double W, const Idx3& dir) -> const DirPts& {
-        const uint64_t fk = wedge_key(W, dir);
-        auto ft = dirfast.find(fk);
-        if (ft != dirfast.end()) return *ft->second;
+        const DirPts** slot = dir_slot(W, dir);
+        if (slot && *slot) return **slot;
         auto key = std::make_pair(W, dir);
         auto it = dirpts.find(key);
-        if (it != dirpts.end()) return *(dirfast[fk] = &it->second);
+        if (it != dirpts.end()) {
+            if (slot) *slot = &it->second;
+            return it->second;
+        }
         Idx3 sgn, pv;
         int c = get_canon(W, dir, sgn, pv);
         const HighFreqOp& op = *hfcanon[c].op;
@@ -713,7 +781,7 @@ void Session::build() {
         d.uep = upload(shuffle(op.uep, pv, sgn, 1.0));
         d.dcp = upload(shuffle(op.uep, pv, sgn, -1.0));
         DirPts& stored = dirpts[key] = d;
-        dirfast[fk] = &stored;
+        if (slot) *slot = &stored;
         return stored;
     };
 
@@ -824,12 +892,13 @@ void Session::build() {
         ccanon = cp.canon;
         return upward ? cp.uep : cp.dcp;
     };
-    std::unordered_set<uint64_t> m2m_seen, l2l_seen;  // wedges already in m2m_mats / l2l_mats
+    std::vector<char> m2m_seen(dirpts.size(), 0), l2l_seen(dirpts.size(), 0);  // by dense wedge id: already planned
     for (auto& kv : hflevels) {
         double W = T.width(kv.first);
         auto ur = up.range[kv.first], dr = dn.range[kv.first];
         for (int i = ur.first; i < ur.second; ++i) {
-            if (!m2m_seen.insert(wedge_key(W, up.v[i].dir)).second) continue;
+            if (m2m_seen[up.v[i].did]) continue;
+            m2m_seen[up.v[i].did] = 1;
             auto key = std::make_pair(W, up.v[i].dir);
             const DirPts& dp = get_dir(W, up.v[i].dir);
             DirMats M{};
@@ -848,7 +917,8 @@ void Session::build() {
             m2m_mats[key] = M;
         }
         for (int i = dr.first; i < dr.second; ++i) {
-            if (!l2l_seen.insert(wedge_key(W, dn.v[i].dir)).second) continue;
+            if (l2l_seen[dn.v[i].did]) continue;
+            l2l_seen[dn.v[i].did] = 1;
             auto key = std::make_pair(W, dn.v[i].dir);
             const DirPts& dp = get_dir(W, dn.v[i].dir);
             DirMats M{};
@@ -1405,8 +1475,10 @@ void Session::build() {
     }
     phase("steps_lf_down");
     if (trace)
-        std::fprintf(stderr, "ddfmm setup   (host seconds in GEMM step emission %.3f, V-list grouping %.3f)\n",
-                     t_emit_gemm_, t_emit_vgroups_);
+        std::fprintf(stderr,
+                     "ddfmm setup   (host seconds in GEMM step emission %.3f, V-list grouping %.3f, uploads above "
+                     "64 KB %.3f)\n",
+                     t_emit_gemm_, t_emit_vgroups_, t_big_uploads_);
     flush_packs();
     if (mixed) {
         // the mixed eval reads only the FP32 copies (and, on tcgen05, only the packed
@@ -1421,6 +1493,7 @@ void Session::build() {
     }
     flush_uploads();
     CK(cudaStreamSynchronize(stream_));
+    stage_release();
     std::vector<char>().swap(arena_.host);  // every chunk is on the device now
     arena_.retired.clear();
     arena_.used = arena_.sent = arena_.cap;

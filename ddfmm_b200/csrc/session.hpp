@@ -199,6 +199,23 @@ private:
         std::vector<std::vector<char> > retired;  // images of earlier chunks, kept until the plan's last sync
         size_t cap = 0, used = 0, sent = 0;
     } arena_;
+    // Host-to-device copies of the plan go through two pinned staging buffers
+    // (a pageable copy's speed varies several-fold between hosts): the source is
+    // copied into a free buffer, which the device then reads asynchronously, so
+    // the source may be released as soon as stage_copy returns.
+    static constexpr size_t kStage = 8 << 20;
+    // Arrays above kArenaMax and up to kMidMax bytes (most of them operators of a
+    // wedge) are placed in device chunks of 4 MiB doubling to 64 MiB, staged
+    // straight to the device: a few allocations instead of one cudaMalloc each.  Like the small arena's
+    // chunks they are released with the session, never by dfree().
+    static constexpr size_t kMidMax = 4 << 20, kMidChunk = 64 << 20;
+    char* mid_dev_ = nullptr;
+    size_t mid_used_ = 0, mid_cap_ = 0;
+    char* stage_[2] = {nullptr, nullptr};
+    cudaEvent_t stage_ev_[2] = {nullptr, nullptr};
+    int stage_next_ = 0;
+    void stage_copy(void* dst, const void* src, size_t bytes);
+    void stage_release();  // after a stream sync
     std::vector<Step> steps_;
     cudaStream_t stream_ = nullptr;
     SessionStats stats_;
@@ -216,7 +233,8 @@ private:
     unsigned long long stall_wait_ns_ = 0;  // armed failure-path hook (0: none)
     std::map<std::pair<const void*, long long>, const float*> packed_;  // (operator, m k) -> packed copy
     std::vector<UmmaPackJob> pack_jobs_;
-    double t_emit_gemm_ = 0, t_emit_vgroups_ = 0;  // setup trace: host seconds in add_gemm, vlist_groups                                 // packing still to launch
+    double t_emit_gemm_ = 0, t_emit_vgroups_ = 0, t_big_uploads_ = 0;  // setup trace: host seconds in add_gemm,
+                                                                       // vlist_groups, uploads above kArenaMax                                 // packing still to launch
     // packed operators (tcgen05 form): the chunk being filled, the operators this
     // session uses (its own and shared ones), and those it created but has not yet
     // published to the process-wide cache (they are, once their packing completed)
