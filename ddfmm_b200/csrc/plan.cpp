@@ -178,45 +178,54 @@ void ColLists::add(std::vector<int>& tab, int k, long long xv, long long yv) {
 HfColumns hf_columns(const Tree& T, const HfNodes& up, const HfNodes& dn, const std::vector<int>& kids,
                      const std::vector<long long>& lf_off, size_t ndirs, size_t ncanon) {
     HfColumns out;
-    std::vector<std::pair<int, int> > jobs;  // (level, pass)
+    // jobs (level, pass, child position): an M2M / L2L pass splits by child
+    // position, whose keys (wedge id * 8 + position) are disjoint, and the
+    // positions' lists are concatenated in position order afterwards -- the
+    // first-seen order of one loop over positions, then nodes
+    struct Job {
+        int level, pass, ind;
+    };
+    std::vector<Job> jobs;
     for (auto& kv : up.range)
         for (int pass = 0; pass < 4; ++pass) {
-            jobs.push_back(std::make_pair(kv.first, pass));
             (pass == 0 ? out.m2m : pass == 1 ? out.e2 : pass == 2 ? out.e2t : out.l2l)[kv.first];
+            if (pass == 0 || pass == 3)
+                for (int ind = 0; ind < 8; ++ind) jobs.push_back(Job{kv.first, pass, ind});
+            else
+                jobs.push_back(Job{kv.first, pass, -1});
         }
+    std::vector<ColLists> part(jobs.size());
     host_parallel_for(jobs.size(), [&](size_t j) {
-        const int level = jobs[j].first, pass = jobs[j].second;
+        const int level = jobs[j].level, pass = jobs[j].pass, ind = jobs[j].ind;
         const bool upward = pass == 0 || pass == 1;
         const HfNodes& N = upward ? up : dn;
         const auto r = N.range.at(level);
+        ColLists& L = part[j];
         if (pass == 0 || pass == 3) {
             // M2M: child w -> parent sum; L2L: parent t -> child u (a problem per (wedge, child position))
             const bool lf_children = T.width(level) == 1.0;
-            ColLists& L = (upward ? out.m2m : out.l2l).at(level);
             std::vector<int> tab(ndirs * 8, -1);
-            for (int ind = 0; ind < 8; ++ind)
-                for (int i = r.first; i < r.second; ++i) {
-                    const HfNode& u = N.v[i];
-                    const int c = kids[(size_t)u.box * 8 + ind];
-                    if (c < 0) continue;
-                    long long coff;
-                    if (lf_children) {
-                        coff = lf_off[c];
-                    } else {
-                        const int ci = N.find(c, predir(u.dir));
-                        if (ci < 0)
-                            throw std::runtime_error(upward ? "child has no directional equivalent density"
-                                                            : "child has no directional check value");
-                        coff = N.v[ci].off;
-                    }
-                    if (upward)
-                        L.add(tab, u.did * 8 + ind, coff, u.toff);
-                    else
-                        L.add(tab, u.did * 8 + ind, u.toff, coff);
+            for (int i = r.first; i < r.second; ++i) {
+                const HfNode& u = N.v[i];
+                const int c = kids[(size_t)u.box * 8 + ind];
+                if (c < 0) continue;
+                long long coff;
+                if (lf_children) {
+                    coff = lf_off[c];
+                } else {
+                    const int ci = N.find(c, predir(u.dir));
+                    if (ci < 0)
+                        throw std::runtime_error(upward ? "child has no directional equivalent density"
+                                                        : "child has no directional check value");
+                    coff = N.v[ci].off;
                 }
+                if (upward)
+                    L.add(tab, u.did * 8 + ind, coff, u.toff);
+                else
+                    L.add(tab, u.did * 8 + ind, u.toff, coff);
+            }
         } else {
             // E2 (upward: temporary -> outgoing vector) and E2^T (downward: incoming -> temporary)
-            ColLists& L = (upward ? out.e2 : out.e2t).at(level);
             std::vector<int> tab(ncanon, -1);
             for (int i = r.first; i < r.second; ++i) {
                 const HfNode& u = N.v[i];
@@ -227,6 +236,16 @@ HfColumns hf_columns(const Tree& T, const HfNodes& up, const HfNodes& dn, const 
             }
         }
     });
+    for (size_t j = 0; j < jobs.size(); ++j) {  // jobs of one (level, pass) are adjacent, positions ascending
+        const int pass = jobs[j].pass;
+        ColLists& L = (pass == 0 ? out.m2m : pass == 1 ? out.e2 : pass == 2 ? out.e2t : out.l2l).at(jobs[j].level);
+        ColLists& P = part[j];
+        for (size_t k = 0; k < P.key.size(); ++k) {
+            L.key.push_back(P.key[k]);
+            L.x.push_back(std::move(P.x[k]));
+            L.y.push_back(std::move(P.y[k]));
+        }
+    }
     return out;
 }
 

@@ -68,8 +68,8 @@ void Session::dfree(const void* p) {
 }
 
 template <class T>
-T* Session::upload(const std::vector<T>& v) {
-    const size_t bytes = v.size() * sizeof(T);
+T* Session::upload_n(const T* src, size_t count) {
+    const size_t bytes = count * sizeof(T);
     if (bytes > kArenaMax) {
         const auto t0 = std::chrono::steady_clock::now();
         T* d = nullptr;
@@ -88,9 +88,9 @@ T* Session::upload(const std::vector<T>& v) {
             d = reinterpret_cast<T*>(mid_dev_ + mid_used_);
             mid_used_ += need;
         } else {
-            d = dalloc<T>(v.size());
+            d = dalloc<T>(count);
         }
-        stage_copy(d, v.data(), bytes);  // the caller's vector may die right after: the data is staged
+        stage_copy(d, src, bytes);  // the caller's array may die right after: the data is staged
         t_big_uploads_ += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         return d;
     }
@@ -113,7 +113,7 @@ T* Session::upload(const std::vector<T>& v) {
         arena_.used = arena_.sent = 0;
     }
     char* d = arena_.dev + arena_.used;
-    if (bytes) std::memcpy(arena_.host.data() + arena_.used, v.data(), bytes);
+    if (bytes) std::memcpy(arena_.host.data() + arena_.used, src, bytes);
     arena_.used += need;
     return reinterpret_cast<T*>(d);
 }
@@ -201,22 +201,40 @@ void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<
     } clock{t_emit_gemm_};
     double flops = 0, bytes = 0;
     std::vector<GemmProblem> P;
+    std::vector<size_t> from;  // the caller's problem of each P
     std::vector<GemmTile> tiles;
-    std::vector<long long> xs, ys;
+    size_t ncols = 0;
     for (size_t i = 0; i < probs.size(); ++i) {
         if (xo[i].empty() || probs[i].m == 0 || probs[i].k == 0) continue;
         GemmProblem q = probs[i];
-        q.col0 = (int)xs.size();
+        q.col0 = (int)ncols;
         q.ncol = (int)xo[i].size();
+        if (yo[i].size() != xo[i].size()) throw std::logic_error("GEMM problem with unequal column lists");
         int pid = (int)P.size();
         P.push_back(q);
-        xs.insert(xs.end(), xo[i].begin(), xo[i].end());
-        ys.insert(ys.end(), yo[i].begin(), yo[i].end());
+        from.push_back(i);
+        ncols += (size_t)q.ncol;
         for (int r0 = 0; r0 < q.m; r0 += GEMM_TILE_M)
             for (int c0 = 0; c0 < q.ncol; c0 += GEMM_TILE_N) tiles.push_back(GemmTile{pid, r0, c0, 0});
         flops += 8.0 * q.m * q.k * (double)q.ncol;
         // operator once, each input and output column once (read-modify-write for += modes)
         bytes += 16.0 * ((double)q.m * q.k + (double)q.k * q.ncol + (mode == GEMM_SET ? 1.0 : 2.0) * q.m * q.ncol);
+    }
+    if (ncols > (size_t)INT_MAX) throw std::runtime_error("too many GEMM columns in one launch");
+    // the launch's column offsets, concatenated in problem order on all host cores
+    // (pieces of at most 64k columns); the arrays are not zeroed first
+    std::unique_ptr<long long[]> xs(new long long[std::max<size_t>(ncols, 1)]);
+    std::unique_ptr<long long[]> ys(new long long[std::max<size_t>(ncols, 1)]);
+    {
+        std::vector<std::array<size_t, 3> > pieces;  // (P index, first column, end column)
+        for (size_t j = 0; j < P.size(); ++j)
+            for (size_t c = 0; c < (size_t)P[j].ncol; c += 65536)
+                pieces.push_back({{j, c, std::min((size_t)P[j].ncol, c + 65536)}});
+        host_parallel_for(pieces.size(), [&](size_t e) {
+            const size_t j = pieces[e][0], c0 = pieces[e][1], n = pieces[e][2] - c0;
+            std::memcpy(xs.get() + P[j].col0 + c0, xo[from[j]].data() + c0, n * sizeof(long long));
+            std::memcpy(ys.get() + P[j].col0 + c0, yo[from[j]].data() + c0, n * sizeof(long long));
+        });
     }
     stats_.flops_gemm += flops;
     if (tiles.empty()) return;
@@ -226,15 +244,15 @@ void Session::add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<
     st.flops = flops;
     st.bytes = bytes;
     if (umma()) {
-        add_umma(P, xs, ys, X, Y, mode, st);
+        add_umma(P, xs.get(), ys.get(), ncols, X, Y, mode, st);
         push_step(st);
         stats_.gemm_launches++;
         return;
     }
     st.g.probs = upload(P);
     st.g.tiles = upload(tiles);
-    st.g.xoff = upload(xs);
-    st.g.yoff = upload(ys);
+    st.g.xoff = upload_n(xs.get(), ncols);
+    st.g.yoff = upload_n(ys.get(), ncols);
     st.g.ntiles = (int)tiles.size();
     st.g.X = X;
     st.g.Y = Y;
@@ -253,14 +271,23 @@ const float* Session::cached_op(const std::string& key) {
 
 const float* Session::packed_operator(const GemmProblem& q) {
     if (q.packed) return q.packed;  // shared copy from the cache
+    struct Clock {
+        double& acc;
+        std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+        ~Clock() { acc += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+    } clock{t_pack_};
     const auto key = std::make_pair((const void*)q.A, ((long long)q.m << 32) | (long long)q.k);
     auto it = packed_.find(key);
     if (it != packed_.end()) return it->second;
-    // packed operators are sub-allocated from 16 MiB chunks (256-byte aligned; cp.async.bulk
-    // needs 16); one larger than a chunk gets its own
+    // packed operators are sub-allocated from device chunks (256-byte aligned; cp.async.bulk
+    // needs 16), the unit the operator cache frees; one larger than a chunk gets its own
     const size_t nf = (umma_packed_floats(q.m, q.k) + 63) & ~(size_t)63;
     if (nf > chunk_left_) {
-        const size_t floats = std::max(nf, (size_t)4 << 20);
+        Clock ca{t_pack_alloc_};
+        // chunks of 16 MiB doubling to 128 MiB: small sessions stay small, large
+        // ones make few allocations
+        const size_t last = chunk_ ? chunk_->bytes() / sizeof(float) : 0;
+        const size_t floats = std::max(nf, std::min((size_t)32 << 20, std::max((size_t)4 << 20, 2 * last)));
         chunk_ = std::make_shared<DevChunk>(prm_.device, floats * sizeof(float));
         chunk_pos_ = chunk_->data();
         chunk_left_ = floats;
@@ -281,8 +308,8 @@ const float* Session::packed_operator(const GemmProblem& q) {
 // tcgen05 form of one grouped GEMM launch: tiles of 128 gathered columns x
 // 128 complex operator rows, the tiles of one problem adjacent so that blocks
 // in flight share its packed operator in L2.
-void Session::add_umma(const std::vector<GemmProblem>& P, const std::vector<long long>& xs,
-                       const std::vector<long long>& ys, const double2* X, double2* Y, int mode, Step& st) {
+void Session::add_umma(const std::vector<GemmProblem>& P, const long long* xs, const long long* ys, size_t ncols,
+                       const double2* X, double2* Y, int mode, Step& st) {
     std::vector<UmmaProblem> U;
     std::vector<UmmaTile> tiles;
     for (size_t i = 0; i < P.size(); ++i) {
@@ -295,7 +322,7 @@ void Session::add_umma(const std::vector<GemmProblem>& P, const std::vector<long
             }
     }
     st.kind = 5;
-    st.hu = UmmaSub{upload(U), upload(tiles), upload(xs), upload(ys), reinterpret_cast<const float2*>(X),
+    st.hu = UmmaSub{upload(U), upload(tiles), upload_n(xs, ncols), upload_n(ys, ncols), reinterpret_cast<const float2*>(X),
                     reinterpret_cast<float2*>(Y), (int)tiles.size(), mode, 0, 0};
     set_multi(st, st.hu, (int)tiles.size());
 }
@@ -1477,8 +1504,8 @@ void Session::build() {
     if (trace)
         std::fprintf(stderr,
                      "ddfmm setup   (host seconds in GEMM step emission %.3f, V-list grouping %.3f, uploads above "
-                     "64 KB %.3f)\n",
-                     t_emit_gemm_, t_emit_vgroups_, t_big_uploads_);
+                     "64 KB %.3f, operator packing %.3f of which chunk allocation %.3f)\n",
+                     t_emit_gemm_, t_emit_vgroups_, t_big_uploads_, t_pack_, t_pack_alloc_);
     flush_packs();
     if (mixed) {
         // the mixed eval reads only the FP32 copies (and, on tcgen05, only the packed

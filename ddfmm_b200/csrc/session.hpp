@@ -162,15 +162,19 @@ private:
     // device work reads those arrays.  Images stay alive until the plan's
     // last stream sync, as an asynchronous copy may still be reading them.
     template <class T>
-    T* upload(const std::vector<T>& v);
+    T* upload_n(const T* p, size_t n);
+    template <class T, class A>
+    T* upload(const std::vector<T, A>& v) {
+        return upload_n(v.data(), v.size());
+    }
     void flush_uploads();
     void dfree(const void* p);  // release one allocation made by dalloc / a large upload
     void add_gemm(std::vector<GemmProblem>& probs, std::vector<std::vector<long long> >& xo,
                   std::vector<std::vector<long long> >& yo, const double2* X, double2* Y, int mode,
                   const char* label);
     const float* packed_operator(const GemmProblem& q);
-    void add_umma(const std::vector<GemmProblem>& P, const std::vector<long long>& xs,
-                  const std::vector<long long>& ys, const double2* X, double2* Y, int mode, Step& st);
+    void add_umma(const std::vector<GemmProblem>& P, const long long* xs, const long long* ys, size_t ncols,
+                  const double2* X, double2* Y, int mode, Step& st);
     void flush_packs();
     void add_pt(const std::vector<PtItem>& items, const std::vector<PtSrc>& srcs, const char* label);
     template <class Sub>
@@ -233,8 +237,9 @@ private:
     unsigned long long stall_wait_ns_ = 0;  // armed failure-path hook (0: none)
     std::map<std::pair<const void*, long long>, const float*> packed_;  // (operator, m k) -> packed copy
     std::vector<UmmaPackJob> pack_jobs_;
-    double t_emit_gemm_ = 0, t_emit_vgroups_ = 0, t_big_uploads_ = 0;  // setup trace: host seconds in add_gemm,
-                                                                       // vlist_groups, uploads above kArenaMax                                 // packing still to launch
+    // setup trace: host seconds in add_gemm, vlist_groups, uploads above kArenaMax,
+    // packed_operator, and of that in packed-operator chunk allocations
+    double t_emit_gemm_ = 0, t_emit_vgroups_ = 0, t_big_uploads_ = 0, t_pack_ = 0, t_pack_alloc_ = 0;                                 // packing still to launch
     // packed operators (tcgen05 form): the chunk being filled, the operators this
     // session uses (its own and shared ones), and those it created but has not yet
     // published to the process-wide cache (they are, once their packing completed)
