@@ -32,20 +32,27 @@ VlistGroupPlan vlist_groups(const Tree& T, const std::vector<int>& lfbox, const 
     }
     std::sort(tlist.begin(), tlist.end());
     // one group per target parent: its children's rows and the union of their
-    // sources, each with the mask of the children that list it
-    std::vector<char> is_src(lfidx.empty() ? 0 : *std::max_element(lfidx.begin(), lfidx.end()) + 1, 0);
-    out.gptr.assign(1, 0);
+    // sources, each with the mask of the children that list it, in source-id
+    // order; groups are built on all host cores, then concatenated in order
+    std::vector<std::pair<size_t, size_t> > grp;  // [i, j) of tlist
     for (size_t i = 0; i < tlist.size();) {
         size_t j = i;
-        while (j < tlist.size() && tlist[j].first == tlist[i].first) ++j;  // one parent: [i, j)
-        const size_t g0 = out.gtrg.size();
-        out.gtrg.resize(g0 + 8, -1);
-        std::map<int, int> srcs;  // source lf id -> (tbase << 8) | mask
-        for (size_t k = i; k < j; ++k) {
+        while (j < tlist.size() && tlist[j].first == tlist[i].first) ++j;
+        grp.push_back(std::make_pair(i, j));
+        i = j;
+    }
+    const size_t ng = grp.size();
+    out.trg.resize(tlist.size());
+    out.gtrg.assign(ng * 8, -1);
+    std::vector<std::vector<VgEntry> > ent(ng);
+    std::vector<long long> gpairs(ng, 0);
+    host_parallel_for(ng, [&](size_t g) {
+        std::vector<std::pair<int, int> > e;  // (source lf id, (tbase << 8) | child bit)
+        for (size_t k = grp[g].first; k < grp[g].second; ++k) {
             const int ct = tlist[k].second.first, l = tlist[k].second.second;
             const Box& B = T.boxes[lfbox[l]];
-            out.gtrg[g0 + ct] = (int)out.trg.size();
-            out.trg.push_back(l);
+            out.gtrg[8 * g + ct] = (int)k;  // targets are numbered in tlist order
+            out.trg[k] = l;
             for (int s : B.vlist) {
                 const Box& SB = T.boxes[s];
                 int rel[3], o[3];
@@ -59,15 +66,27 @@ VlistGroupPlan vlist_groups(const Tree& T, const std::vector<int>& lfbox, const 
                 // the kernel's offset index for this pair: tbase + a + 7b + 49c
                 const int voff = (o[0] + 3) + 7 * ((o[1] + 3) + 7 * (o[2] + 3));
                 if (tbase + vlist_child_voff(ct) != voff) throw std::logic_error("V-list offset bookkeeping");
-                int& e = srcs[lfidx[s]];
-                e = (tbase << 8) | (e & 255) | (1 << ct);
-                is_src[lfidx[s]] = 1;
-                out.pairs++;
+                e.push_back(std::make_pair(lfidx[s], (tbase << 8) | (1 << ct)));
             }
         }
-        for (auto& kv : srcs) out.gsrc.push_back(VgEntry{kv.first, kv.second});
+        gpairs[g] = (long long)e.size();
+        std::sort(e.begin(), e.end());
+        std::vector<VgEntry>& v = ent[g];
+        for (size_t k = 0; k < e.size();) {  // a source's pairs share tbase (one parent): OR the bits
+            int m = 0;
+            size_t q = k;
+            for (; q < e.size() && e[q].first == e[k].first; ++q) m |= e[q].second & 255;
+            v.push_back(VgEntry{e[k].first, (e[k].second & ~255) | m});
+            k = q;
+        }
+    });
+    out.gptr.assign(1, 0);
+    std::vector<char> is_src(lfidx.empty() ? 0 : *std::max_element(lfidx.begin(), lfidx.end()) + 1, 0);
+    for (size_t g = 0; g < ng; ++g) {
+        out.gsrc.insert(out.gsrc.end(), ent[g].begin(), ent[g].end());
         out.gptr.push_back((int)out.gsrc.size());
-        i = j;
+        out.pairs += gpairs[g];
+        for (const VgEntry& v : ent[g]) is_src[v.row] = 1;
     }
     for (size_t l = 0; l < is_src.size(); ++l)
         if (is_src[l]) out.src.push_back((int)l);

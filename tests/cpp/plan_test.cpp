@@ -8,7 +8,9 @@
 //    node and the canonical offset of the pair;
 //  * M2M / E2 / E2^T / L2L column lists: every (node, child position with a
 //    child) pair and every node appears once, in the problem of its wedge and
-//    child position or of its canonical wedge, with the right columns.
+//    child position or of its canonical wedge, with the right columns;
+//  * an order-sensitive hash of the V-list groups and the column lists, so a
+//    faster construction can be held to the same problem and column order.
 //   plan_test <points.bin (3n doubles)> <n> <K> <ncell> <maxlevel> <ptsmax>
 #include <cstdio>
 #include <cstdlib>
@@ -45,9 +47,25 @@ int main(int argc, char** argv) {
         }
     std::map<int, std::vector<int> > levels;
     for (int l = 0; l < (int)lfbox.size(); ++l) levels[T.boxes[lfbox[l]].level].push_back(l);
+    // order-sensitive hash of the plan pieces (FNV-1a over 64-bit words): the
+    // test compares it with values recorded from the first implementation
+    unsigned long long H = 1469598103934665603ull;
+    auto mix = [&](long long v) {
+        H ^= (unsigned long long)v;
+        H *= 1099511628211ull;
+    };
     long long pairs = 0, groups = 0;
     for (auto& kv : levels) {
         const VlistGroupPlan g = vlist_groups(T, lfbox, lfidx, kv.second);
+        for (int x : g.trg) mix(x);
+        for (int x : g.gptr) mix(x);
+        for (const VgEntry& e : g.gsrc) {
+            mix(e.row);
+            mix(e.tbase_mask);
+        }
+        for (int x : g.gtrg) mix(x);
+        for (int x : g.src) mix(x);
+        mix(g.pairs);
         std::set<std::pair<int, int> > want, got;  // (target lf id, source lf id)
         for (int l : kv.second)
             for (int s : T.boxes[lfbox[l]].vlist) want.insert(std::make_pair(l, lfidx[s]));
@@ -204,8 +222,14 @@ int main(int argc, char** argv) {
             }
             if (got2 != want2) { std::printf("columns differ (level %d pass %d)\n", level, pass); return 1; }
             ncols += (long long)got2.size();
+            for (size_t k = 0; k < L.key.size(); ++k) {
+                mix(L.key[k]);
+                for (long long x : L.x[k]) mix(x);
+                for (long long y : L.y[k]) mix(y);
+            }
+            mix(-pass - 1);
         }
     }
-    std::printf("ok pairs %lld groups %lld far %lld columns %lld\n", pairs, groups, far, ncols);
+    std::printf("ok pairs %lld groups %lld far %lld columns %lld hash %016llx\n", pairs, groups, far, ncols, H);
     return 0;
 }
