@@ -836,27 +836,92 @@ void Session::build() {
     std::map<int, long long> tmp_up_level;  // level -> temporary elements of its M2M sums
     long long upeq_total = 0, dnchk_total = 0, tmp_max = 0;
     for (auto& kv : hflevels) {
-        double W = T.width(kv.first);
-        long long tmp_up = 0, tmp_dn = 0;
-        int u0 = (int)up.v.size(), d0 = (int)dn.v.size();
-        for (int b : kv.second) {
-            up.first[b] = (int)up.v.size();
-            up.cnt[b] = (int)T.boxes[b].outdirs.size();
-            for (const Idx3& d : T.boxes[b].outdirs) {
-                const DirPts& dp = get_dir(W, d);
-                up.v.push_back(HfNode{b, d, dp.canon, upeq_total, tmp_up, dp.did});
-                upeq_total += dp.r1;
-                tmp_up += std::max(dp.r1, dp.r2);
-            }
-            dn.first[b] = (int)dn.v.size();
-            dn.cnt[b] = (int)T.boxes[b].incdirs.size();
-            for (const Idx3& d : T.boxes[b].incdirs) {
-                const DirPts& dp = get_dir(W, d);
-                dn.v.push_back(HfNode{b, d, dp.canon, dnchk_total, tmp_dn, dp.did});
-                dnchk_total += dp.r1;
-                tmp_dn += std::max(dp.r1, dp.r2);
-            }
+        const double W = T.width(kv.first);
+        const std::vector<int>& bx = kv.second;
+        const size_t nbx = bx.size();
+        // the level's wedges, created in first-use order (their dense ids follow it):
+        // a box's outgoing wedges, then its incoming ones, box by box
+        for (int b : bx) {
+            for (const Idx3& d : T.boxes[b].outdirs) get_dir(W, d);
+            for (const Idx3& d : T.boxes[b].incdirs) get_dir(W, d);
         }
+        // every wedge of the level now has its point sets: the nodes are filled on
+        // all host cores from per-box prefix sums (a box's nodes are contiguous, in
+        // its sorted wedge order), read-only lookups through the level's table
+        const DirPts** tab = dir_slot(W, Idx3{{0, 0, 0}}) ? last_tab->t.data() : nullptr;
+        const int C = last_tab ? last_tab->C : 0, E = 2 * C + 1;
+        auto lookup = [&](const Idx3& d) -> const DirPts& {
+            if (tab && d[0] >= -C && d[0] <= C && d[1] >= -C && d[1] <= C && d[2] >= -C && d[2] <= C) {
+                const DirPts* q = tab[((size_t)(d[0] + C) * E + (d[1] + C)) * E + (d[2] + C)];
+                if (q) return *q;
+            }
+            return dirpts.at(std::make_pair(W, d));
+        };
+        std::vector<long long> uo(nbx + 1, 0), ut(nbx + 1, 0), dof(nbx + 1, 0), dt(nbx + 1, 0);
+        std::vector<int> un(nbx + 1, 0), dnn(nbx + 1, 0);
+        host_parallel_for(nbx, [&](size_t i) {
+            const Box& B = T.boxes[bx[i]];
+            long long a = 0, at = 0, c = 0, ct = 0;
+            for (const Idx3& d : B.outdirs) {
+                const DirPts& dp = lookup(d);
+                a += dp.r1;
+                at += std::max(dp.r1, dp.r2);
+            }
+            for (const Idx3& d : B.incdirs) {
+                const DirPts& dp = lookup(d);
+                c += dp.r1;
+                ct += std::max(dp.r1, dp.r2);
+            }
+            uo[i + 1] = a;
+            ut[i + 1] = at;
+            dof[i + 1] = c;
+            dt[i + 1] = ct;
+            un[i + 1] = (int)B.outdirs.size();
+            dnn[i + 1] = (int)B.incdirs.size();
+        });
+        const int u0 = (int)up.v.size(), d0 = (int)dn.v.size();
+        uo[0] = upeq_total;
+        dof[0] = dnchk_total;
+        un[0] = u0;
+        dnn[0] = d0;
+        for (size_t i = 0; i < nbx; ++i) {
+            uo[i + 1] += uo[i];
+            ut[i + 1] += ut[i];
+            dof[i + 1] += dof[i];
+            dt[i + 1] += dt[i];
+            un[i + 1] += un[i];
+            dnn[i + 1] += dnn[i];
+        }
+        up.v.resize((size_t)un[nbx]);
+        dn.v.resize((size_t)dnn[nbx]);
+        host_parallel_for(nbx, [&](size_t i) {
+            const int b = bx[i];
+            const Box& B = T.boxes[b];
+            up.first[b] = un[i];
+            up.cnt[b] = un[i + 1] - un[i];
+            long long o = uo[i], t = ut[i];
+            int k = un[i];
+            for (const Idx3& d : B.outdirs) {
+                const DirPts& dp = lookup(d);
+                up.v[k++] = HfNode{b, d, dp.canon, o, t, dp.did};
+                o += dp.r1;
+                t += std::max(dp.r1, dp.r2);
+            }
+            dn.first[b] = dnn[i];
+            dn.cnt[b] = dnn[i + 1] - dnn[i];
+            o = dof[i];
+            t = dt[i];
+            k = dnn[i];
+            for (const Idx3& d : B.incdirs) {
+                const DirPts& dp = lookup(d);
+                dn.v[k++] = HfNode{b, d, dp.canon, o, t, dp.did};
+                o += dp.r1;
+                t += std::max(dp.r1, dp.r2);
+            }
+        });
+        upeq_total = uo[nbx];
+        dnchk_total = dof[nbx];
+        const long long tmp_up = ut[nbx], tmp_dn = dt[nbx];
         up.range[kv.first] = std::make_pair(u0, (int)up.v.size());
         tmp_up_level[kv.first] = tmp_up;
         dn.range[kv.first] = std::make_pair(d0, (int)dn.v.size());
