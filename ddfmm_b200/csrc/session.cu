@@ -51,7 +51,10 @@ template <class T>
 T* Session::dalloc(size_t count) {
     if (count == 0) count = 1;
     void* p = nullptr;
+    const auto t0 = std::chrono::steady_clock::now();
     CK(cudaMalloc(&p, count * sizeof(T)));
+    t_malloc_ += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    ++n_malloc_;
     allocs_.push_back(p);
     alloc_bytes_[p] = count * sizeof(T);
     stats_.device_bytes += count * sizeof(T);
@@ -135,8 +138,13 @@ void Session::stage_copy(void* dst, const void* src, size_t bytes) {
         const size_t n = std::min(kStage, bytes - off);
         const int k = stage_next_;
         stage_next_ ^= 1;
+        const auto t0 = std::chrono::steady_clock::now();
         CK(cudaEventSynchronize(stage_ev_[k]));  // the device has read this buffer's previous contents
+        const auto t1 = std::chrono::steady_clock::now();
         std::memcpy(stage_[k], static_cast<const char*>(src) + off, n);
+        t_stage_wait_ += std::chrono::duration<double>(t1 - t0).count();
+        t_stage_copy_ += std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+        ++n_stage_;
         CK(cudaMemcpyAsync(static_cast<char*>(dst) + off, stage_[k], n, cudaMemcpyHostToDevice, stream_));
         CK(cudaEventRecord(stage_ev_[k], stream_));
         off += n;
@@ -1569,8 +1577,10 @@ void Session::build() {
     if (trace)
         std::fprintf(stderr,
                      "ddfmm setup   (host seconds in GEMM step emission %.3f, V-list grouping %.3f, uploads above "
-                     "64 KB %.3f, operator packing %.3f of which chunk allocation %.3f)\n",
-                     t_emit_gemm_, t_emit_vgroups_, t_big_uploads_, t_pack_, t_pack_alloc_);
+                     "64 KB %.3f, operator packing %.3f of which chunk allocation %.3f; %lld device allocations "
+                     "%.3f, %lld staged copies: waits %.3f, host copies %.3f)\n",
+                     t_emit_gemm_, t_emit_vgroups_, t_big_uploads_, t_pack_, t_pack_alloc_, n_malloc_, t_malloc_,
+                     n_stage_, t_stage_wait_, t_stage_copy_);
     flush_packs();
     if (mixed) {
         // the mixed eval reads only the FP32 copies (and, on tcgen05, only the packed

@@ -239,7 +239,10 @@ private:
     std::vector<UmmaPackJob> pack_jobs_;
     // setup trace: host seconds in add_gemm, vlist_groups, uploads above kArenaMax,
     // packed_operator, and of that in packed-operator chunk allocations
-    double t_emit_gemm_ = 0, t_emit_vgroups_ = 0, t_big_uploads_ = 0, t_pack_ = 0, t_pack_alloc_ = 0;                                 // packing still to launch
+    double t_emit_gemm_ = 0, t_emit_vgroups_ = 0, t_big_uploads_ = 0, t_pack_ = 0, t_pack_alloc_ = 0;
+    // and in device allocations, staging-buffer waits and copies into the staging buffers
+    double t_malloc_ = 0, t_stage_wait_ = 0, t_stage_copy_ = 0;
+    long long n_malloc_ = 0, n_stage_ = 0;                                 // packing still to launch
     // packed operators (tcgen05 form): the chunk being filled, the operators this
     // session uses (its own and shared ones), and those it created but has not yet
     // published to the process-wide cache (they are, once their packing completed)
