@@ -112,10 +112,22 @@ __device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[4], con
         : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
+// D (8 x 8) += A (8 x 4, row g at k = tig) * B (4 x 8, k = tig at column g);
+// D elements 0, 1: row g, columns 2 tig, 2 tig + 1 -- the first two elements
+// of dmma16's D, at the same rows and columns
+__device__ __forceinline__ void dmma8(double (&c)[4], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
 // One K slice of a warp's 16 x 8NJ block (NJ 8-column blocks), its first KS
 // 8-wide K steps: the three real products cr = Ar Xr, ci = Ai Xi,
-// cs = (Ar + Ai)(Xr + Xi) into the accumulators of blocks 0 .. NJ-1.
-template <int NJ>
+// cs = (Ar + Ai)(Xr + Xi) into the accumulators of blocks 0 .. NJ-1.  HALF:
+// the slab holds at most 8 of the operator's rows, so each 16-row product is
+// two 8-row m8n8k4 products over k = tig and tig + 4 (the same fragments'
+// first rows), half the tensor work of the m16n8k8 form, rows g + 8 left zero.
+template <int NJ, bool HALF>
 __device__ __forceinline__ void zgemm_slice(const double2* As, const double2* Xs, int KS, double (&cr)[4][4],
                                             double (&ci)[4][4], double (&cs)[4][4]) {
 #pragma unroll
@@ -124,11 +136,32 @@ __device__ __forceinline__ void zgemm_slice(const double2* As, const double2* Xs
         // m16n8k8 fragments: A rows g, g+8 at k = tig, tig + 4; B k = tig, tig + 4 at column g
         double2 a[4], b[NJ][2];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) a[q] = As[(ks * 8 + 4 * (q >> 1)) * BM + 8 * (q & 1)];
+        for (int q = 0; q < 4; ++q)
+            if (!HALF || (q & 1) == 0) a[q] = As[(ks * 8 + 4 * (q >> 1)) * BM + 8 * (q & 1)];
 #pragma unroll
         for (int j = 0; j < NJ; ++j)
 #pragma unroll
             for (int h = 0; h < 2; ++h) b[j][h] = Xs[j * 8 * BKP + ks * 8 + 4 * h];
+        if (HALF) {
+            const double ar0 = a[0].x, ar2 = a[2].x, ai0 = a[0].y, ai2 = a[2].y;
+            const double as0 = a[0].x + a[0].y, as2 = a[2].x + a[2].y;
+#pragma unroll
+            for (int j = 0; j < NJ; ++j) {
+                dmma8(cr[j], ar0, b[j][0].x);
+                dmma8(cr[j], ar2, b[j][1].x);
+            }
+#pragma unroll
+            for (int j = 0; j < NJ; ++j) {
+                dmma8(ci[j], ai0, b[j][0].y);
+                dmma8(ci[j], ai2, b[j][1].y);
+            }
+#pragma unroll
+            for (int j = 0; j < NJ; ++j) {
+                dmma8(cs[j], as0, b[j][0].x + b[j][0].y);
+                dmma8(cs[j], as2, b[j][1].x + b[j][1].y);
+            }
+            continue;
+        }
         double ar[4], ai[4], as[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -170,6 +203,7 @@ __global__ void __launch_bounds__(256, DDFMM_ZGEMM_MINB) zgemm_kernel(const Gemm
     const int nrow = ((rows + 15) >> 4) << 4;  // rows of the active slabs
     const bool active = wm * 16 < rows && wn * 32 < ncol;
     const int njb = min(4, (ncol - wn * 32 + 7) >> 3);  // 8-column blocks of this warp holding columns
+    const bool half = rows - wm * 16 <= 8;               // this warp's slab holds at most 8 operator rows
     if (tid < BN) {
         xo[tid] = tid < ncol ? xoff[p.col0 + t.col0 + tid] : 0;
         yo[tid] = tid < ncol ? yoff[p.col0 + t.col0 + tid] : 0;
@@ -217,11 +251,20 @@ __global__ void __launch_bounds__(256, DDFMM_ZGEMM_MINB) zgemm_kernel(const Gemm
             const double2* As = gsm + (it % GSTAGES) * GSTAGE + tig * BM + ((wm * 16 + g) ^ (tig << 1));
             const double2* Xs = gsm + (it % GSTAGES) * GSTAGE + BK * BM + (wn * 32 + g) * BKP + tig;
             const int KS = min(BK / 8, (p.k - it * BK + 7) >> 3);  // 8-wide K steps holding k
-            switch (njb) {
-                case 4: zgemm_slice<4>(As, Xs, KS, cr, ci, cs); break;
-                case 3: zgemm_slice<3>(As, Xs, KS, cr, ci, cs); break;
-                case 2: zgemm_slice<2>(As, Xs, KS, cr, ci, cs); break;
-                default: zgemm_slice<1>(As, Xs, KS, cr, ci, cs); break;
+            if (half) {
+                switch (njb) {
+                    case 4: zgemm_slice<4, true>(As, Xs, KS, cr, ci, cs); break;
+                    case 3: zgemm_slice<3, true>(As, Xs, KS, cr, ci, cs); break;
+                    case 2: zgemm_slice<2, true>(As, Xs, KS, cr, ci, cs); break;
+                    default: zgemm_slice<1, true>(As, Xs, KS, cr, ci, cs); break;
+                }
+            } else {
+                switch (njb) {
+                    case 4: zgemm_slice<4, false>(As, Xs, KS, cr, ci, cs); break;
+                    case 3: zgemm_slice<3, false>(As, Xs, KS, cr, ci, cs); break;
+                    case 2: zgemm_slice<2, false>(As, Xs, KS, cr, ci, cs); break;
+                    default: zgemm_slice<1, false>(As, Xs, KS, cr, ci, cs); break;
+                }
             }
         }
     }
