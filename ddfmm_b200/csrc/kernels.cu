@@ -197,12 +197,19 @@ __global__ void __launch_bounds__(256, DDFMM_ZGEMM_MINB) zgemm_kernel(const Gemm
     const GemmTile t = tiles[blockIdx.x];
     const GemmProblem p = probs[t.prob];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int g = lane >> 2, tig = lane & 3, wm = warp >> 1, wn = warp & 1;
+    const int g = lane >> 2, tig = lane & 3;
     const int ncol = min(BN, p.ncol - t.col0);
     const int rows = min(BM, p.m - t.row0);
     const int nrow = ((rows + 15) >> 4) << 4;  // rows of the active slabs
-    const bool active = wm * 16 < rows && wn * 32 < ncol;
-    const int njb = min(4, (ncol - wn * 32 + 7) >> 3);  // 8-column blocks of this warp holding columns
+    // warps over (slab, column group): 4 slabs x 2 groups of 32 columns; a tile
+    // of 1 or 2 slabs (an operator's last rows) splits the columns into 8 or 4
+    // groups instead, so all 8 warps share its work
+    const int nslab = nrow >> 4;
+    const int ngrp = nslab == 1 ? 8 : nslab == 2 ? 4 : 2;
+    const int cpg = BN / ngrp;  // columns per group: 8, 16 or 32
+    const int wm = warp / ngrp, wn = warp % ngrp;
+    const bool active = wm < nslab && wn * cpg < ncol;
+    const int njb = min(cpg / 8, (ncol - wn * cpg + 7) >> 3);  // 8-column blocks of this warp holding columns
     const bool half = rows - wm * 16 <= 8;               // this warp's slab holds at most 8 operator rows
     if (tid < BN) {
         xo[tid] = tid < ncol ? xoff[p.col0 + t.col0 + tid] : 0;
@@ -249,7 +256,7 @@ __global__ void __launch_bounds__(256, DDFMM_ZGEMM_MINB) zgemm_kernel(const Gemm
         }
         if (active) {
             const double2* As = gsm + (it % GSTAGES) * GSTAGE + tig * BM + ((wm * 16 + g) ^ (tig << 1));
-            const double2* Xs = gsm + (it % GSTAGES) * GSTAGE + BK * BM + (wn * 32 + g) * BKP + tig;
+            const double2* Xs = gsm + (it % GSTAGES) * GSTAGE + BK * BM + (wn * cpg + g) * BKP + tig;
             const int KS = min(BK / 8, (p.k - it * BK + 7) >> 3);  // 8-wide K steps holding k
             if (half) {
                 switch (njb) {
@@ -274,7 +281,8 @@ __global__ void __launch_bounds__(256, DDFMM_ZGEMM_MINB) zgemm_kernel(const Gemm
     for (int j = 0; j < 4; ++j)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-            int col = wn * 32 + j * 8 + 2 * tig + e;
+            if (j * 8 >= cpg) break;  // the group's own 8-column blocks only
+            int col = wn * cpg + j * 8 + 2 * tig + e;
             if (col >= ncol) continue;
             double2* y = Y + yo[col] + t.row0;
 #pragma unroll
