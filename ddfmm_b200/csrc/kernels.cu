@@ -201,12 +201,13 @@ __global__ void __launch_bounds__(256, DDFMM_ZGEMM_MINB) zgemm_kernel(const Gemm
     const int ncol = min(BN, p.ncol - t.col0);
     const int rows = min(BM, p.m - t.row0);
     const int nrow = ((rows + 15) >> 4) << 4;  // rows of the active slabs
-    // warps over (slab, column group): 4 slabs x 2 groups of 32 columns; a tile
-    // of 1 or 2 slabs (an operator's last rows) splits the columns into 8 or 4
-    // groups instead, so all 8 warps share its work
+    // warps over (slab, column group): 4 slabs x 2 groups of up to 32 columns; a
+    // tile of 1 or 2 slabs (an operator's last rows) splits the columns into 8 or
+    // 4 groups instead, and the groups share the tile's columns evenly (in
+    // multiples of 8), so all 8 warps share its work when it has few columns too
     const int nslab = nrow >> 4;
     const int ngrp = nslab == 1 ? 8 : nslab == 2 ? 4 : 2;
-    const int cpg = BN / ngrp;  // columns per group: 8, 16 or 32
+    const int cpg = min(BN / ngrp, max(8, ((ncol + ngrp - 1) / ngrp + 7) / 8 * 8));  // columns per group
     const int wm = warp / ngrp, wn = warp % ngrp;
     const bool active = wm < nslab && wn * cpg < ncol;
     const int njb = min(cpg / 8, (ncol - wn * cpg + 7) >> 3);  // 8-column blocks of this warp holding columns
