@@ -91,7 +91,7 @@ void launch_kmat(const KmatJob* jobs, int njobs, long long total, int kernel, cu
 #define DDFMM_ZGEMM_MINB 2
 #endif
 constexpr int BM = 64, BN = 64, BK = DDFMM_ZGEMM_BK, BKP = BK + 4, GSTAGES = DDFMM_ZGEMM_STAGES;
-static_assert(BK == 16 || BK == 32, "K slice of 16 or 32");
+static_assert(BK == 8 || BK == 16 || BK == 32, "K slice of 8, 16 or 32");
 constexpr int GSTAGE = BK * BM + BN * BKP;  // double2 per stage
 constexpr int GEMM_SMEM = GSTAGES * GSTAGE * (int)sizeof(double2);
 
@@ -160,29 +160,29 @@ __device__ __forceinline__ void zgemm_slice(const double2* As, const double2* Xs
                 dmma8(cs[j], as0, b[j][0].x + b[j][0].y);
                 dmma8(cs[j], as2, b[j][1].x + b[j][1].y);
             }
-            continue;
-        }
-        double ar[4], ai[4], as[4];
+        } else {
+            double ar[4], ai[4], as[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            ar[q] = a[q].x;
-            ai[q] = a[q].y;
-            as[q] = a[q].x + a[q].y;
-        }
+            for (int q = 0; q < 4; ++q) {
+                ar[q] = a[q].x;
+                ai[q] = a[q].y;
+                as[q] = a[q].x + a[q].y;
+            }
 #pragma unroll
-        for (int j = 0; j < NJ; ++j) {
-            const double br[2] = {b[j][0].x, b[j][1].x};
-            dmma16(cr[j], ar, br);
-        }
+            for (int j = 0; j < NJ; ++j) {
+                const double br[2] = {b[j][0].x, b[j][1].x};
+                dmma16(cr[j], ar, br);
+            }
 #pragma unroll
-        for (int j = 0; j < NJ; ++j) {
-            const double bi[2] = {b[j][0].y, b[j][1].y};
-            dmma16(ci[j], ai, bi);
-        }
+            for (int j = 0; j < NJ; ++j) {
+                const double bi[2] = {b[j][0].y, b[j][1].y};
+                dmma16(ci[j], ai, bi);
+            }
 #pragma unroll
-        for (int j = 0; j < NJ; ++j) {
-            const double bs[2] = {b[j][0].x + b[j][0].y, b[j][1].x + b[j][1].y};
-            dmma16(cs[j], as, bs);
+            for (int j = 0; j < NJ; ++j) {
+                const double bs[2] = {b[j][0].x + b[j][0].y, b[j][1].x + b[j][1].y};
+                dmma16(cs[j], as, bs);
+            }
         }
     }
 }
