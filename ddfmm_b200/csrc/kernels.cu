@@ -90,7 +90,8 @@ void launch_kmat(const KmatJob* jobs, int njobs, long long total, int kernel, cu
 #ifndef DDFMM_ZGEMM_MINB
 #define DDFMM_ZGEMM_MINB 2
 #endif
-constexpr int BM = 64, BN = 64, BK = DDFMM_ZGEMM_BK, BKP = BK + 4, GSTAGES = DDFMM_ZGEMM_STAGES;
+constexpr int BM = GEMM_TILE_M, BN = GEMM_TILE_N, BK = DDFMM_ZGEMM_BK, BKP = BK + 4, GSTAGES = DDFMM_ZGEMM_STAGES;
+static_assert(BN * BK % 256 == 0, "whole column loads per thread");
 static_assert(BK == 8 || BK == 16 || BK == 32, "K slice of 8, 16 or 32");
 constexpr int GSTAGE = BK * BM + BN * BKP;  // double2 per stage
 constexpr int GEMM_SMEM = GSTAGES * GSTAGE * (int)sizeof(double2);
@@ -206,7 +207,7 @@ __global__ void __launch_bounds__(256, DDFMM_ZGEMM_MINB) zgemm_kernel(const Gemm
     // 4 groups instead, and the groups share the tile's columns evenly (in
     // multiples of 8), so all 8 warps share its work when it has few columns too
     const int nslab = nrow >> 4;
-    const int ngrp = nslab == 1 ? 8 : nslab == 2 ? 4 : 2;
+    const int ngrp = min(BN / 8, nslab == 1 ? 8 : nslab == 2 ? 4 : 2);
     const int cpg = min(BN / ngrp, max(8, ((ncol + ngrp - 1) / ngrp + 7) / 8 * 8));  // columns per group
     const int wm = warp / ngrp, wn = warp % ngrp;
     const bool active = wm < nslab && wn * cpg < ncol;
